@@ -1,0 +1,1125 @@
+// Engine: ownership of one network's device memory, ingest, the run loop and the
+// property surface.  The run loop is the reference's per-iteration body
+// (tools/dist_simulator.cpp:2072-2315) with the MPI exchange replaced by in-HBM
+// delivery and every per-step host synchronisation removed.
+#include "dtb_engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+
+namespace dtb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error() { return g_last_error.c_str(); }
+
+int fail(int status, const std::string& msg) {
+    g_last_error = msg;
+    return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    cudaGetLastError();
+    const int st = (e == cudaErrorMemoryAllocation) ? DTB_OUT_OF_MEMORY
+                 : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? DTB_NO_DEVICE : DTB_CUDA_ERROR;
+    return fail(st, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+__global__ void set_u64_kernel(unsigned long long* p, unsigned long long v) { *p = v; }
+__global__ void set_clock_kernel(Clock* c, float t, unsigned long long n) {
+    c->t = t;
+    c->n = n;
+    c->err = 0u;
+}
+__global__ void fill_range_kernel(float* p, uint32_t begin, uint32_t end, float v) {
+    for (uint32_t i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+static uint32_t round_up(uint32_t x, uint32_t m) { return (x + m - 1) / m * m; }
+
+Engine::~Engine() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (void* p : allocs) cudaFree(p);
+    if (h_cnt) cudaFreeHost(h_cnt);
+    if (h_vsum) cudaFreeHost(h_vsum);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+void Engine::dfree(void* p) {
+    if (!p) return;
+    auto it = std::find(allocs.begin(), allocs.end(), p);
+    if (it != allocs.end()) allocs.erase(it);
+    cudaFree(p);
+}
+
+int Engine::weight_bytes() const {
+    switch (wtype) {
+        case W_F32: return 8;
+        case W_BF16: case W_F16: return 4;
+        default: return 2;
+    }
+}
+
+int Engine::init_common(const dtb_options& opt, uint32_t n_neurons) {
+    if (!(opt.dt > 0.0f) || !std::isfinite(opt.dt)) return fail(DTB_INVALID_PARAMETER, "dt must be positive");
+    if (opt.weight_type > DTB_W_U8) return fail(DTB_UNSUPPORTED, "device weight type must be F32, BF16, F16 or U8");
+    if (n_neurons == 0) return fail(DTB_INVALID_NETWORK, "network has no neurons");
+    if (n_neurons >= 0x7FFFFFFFu - kPad) return fail(DTB_UNSUPPORTED, "more than 2^31 neurons");
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
+        cudaGetLastError();
+        return fail(DTB_NO_DEVICE, "no CUDA device");
+    }
+    DTB_CU(cudaGetDevice(&device));
+    DTB_CU(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
+    DTB_CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    DTB_CU(cudaEventCreate(&ev0));
+    DTB_CU(cudaEventCreate(&ev1));
+    dt = opt.dt;
+    wtype = opt.weight_type;
+    seed = opt.seed;
+    n = n_neurons;
+    n_pad = round_up(n, kPad);
+    n_words = n_pad / 32;
+    return DTB_OK;
+}
+
+int Engine::setup_populations_from_property(const float* prop) {
+    // Populations are runs of equal column-3 values (src/configuration.cpp:1902-1930).
+    pop_ids.clear();
+    pop_off.clear();
+    for (uint32_t i = 0; i < n; ++i) {
+        const float v = prop[static_cast<size_t>(i) * 22 + 3];
+        if (i == 0 || v != prop[static_cast<size_t>(i - 1) * 22 + 3]) {
+            if (!(v >= 0.0f) || v > 4294967040.0f) return fail(DTB_INVALID_NETWORK, "population id must be a non-negative integer");
+            pop_ids.push_back(static_cast<uint32_t>(v));
+            pop_off.push_back(i);
+        }
+    }
+    pop_off.push_back(n);
+    P = static_cast<uint32_t>(pop_ids.size());
+    return DTB_OK;
+}
+
+int Engine::upload_params() {
+    std::vector<PopParams> pp(P);
+    for (uint32_t p = 0; p < P; ++p) pp[p] = derive(pop_raw[p], dt);
+    DTB_CU(cudaMemcpyAsync(pop_dev, pp.data(), sizeof(PopParams) * P, cudaMemcpyHostToDevice, stream));
+    if (per_neuron) {
+        if (!np_dev) DTB_TRY(dalloc(np_dev, static_cast<size_t>(kParamFloats) * n_pad));
+        std::vector<float> soa(static_cast<size_t>(kParamFloats) * n_pad, 0.0f);
+        for (uint32_t i = 0; i < n; ++i) {
+            const PopParams d = derive(neuron_raw[i], dt);
+            const float* f = reinterpret_cast<const float*>(&d);
+            for (int k = 0; k < kParamFloats; ++k) soa[static_cast<size_t>(k) * n_pad + i] = f[k];
+        }
+        DTB_CU(cudaMemcpyAsync(np_dev, soa.data(), soa.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
+        DTB_CU(cudaStreamSynchronize(stream));
+    } else {
+        DTB_CU(cudaStreamSynchronize(stream));
+    }
+    return refresh_view();
+}
+
+int Engine::init_state() {
+    // block_new.py:57-62: V = (V_th + V_reset) / 2, t_last = -T_ref, J = 0, i_bg = OU mean
+    std::vector<float> v(n_pad, 0.0f), tl(n_pad, 0.0f), io(n_pad, 0.0f);
+    for (uint32_t p = 0; p < P; ++p) {
+        for (uint32_t i = pop_off[p]; i < pop_off[p + 1]; ++i) {
+            const RawParams& r = per_neuron ? neuron_raw[i] : pop_raw[p];
+            volatile float s = r.V_th + r.V_reset;
+            v[i] = s / 2.0f;
+            tl[i] = -r.T_ref;
+            io[i] = r.ou_mean;
+        }
+    }
+    DTB_CU(cudaMemcpyAsync(V, v.data(), sizeof(float) * n_pad, cudaMemcpyHostToDevice, stream));
+    DTB_CU(cudaMemcpyAsync(tlast, tl.data(), sizeof(float) * n_pad, cudaMemcpyHostToDevice, stream));
+    DTB_CU(cudaMemcpyAsync(iou, io.data(), sizeof(float) * n_pad, cudaMemcpyHostToDevice, stream));
+    DTB_CU(cudaMemsetAsync(J, 0, sizeof(float4) * n_pad, stream));
+    DTB_CU(cudaMemsetAsync(bits0, 0, sizeof(uint32_t) * n_words, stream));
+    DTB_CU(cudaMemsetAsync(bits1, 0, sizeof(uint32_t) * n_words, stream));
+    set_clock_kernel<<<1, 1, 0, stream>>>(clock, 0.0f, 0ull);
+    DTB_CU(cudaGetLastError());
+    DTB_CU(cudaStreamSynchronize(stream));
+    steps = 0;
+    t = 0.0f;
+    return DTB_OK;
+}
+
+int Engine::refresh_view() {
+    NetView v{};
+    v.n = n;
+    v.n_pad = n_pad;
+    v.n_words = n_words;
+    v.n_pops = P;
+    v.dt = dt;
+    v.per_neuron = per_neuron ? 1u : 0u;
+    v.weight_type = wtype;
+    v.hist_cap = hist_cap;
+    v.V = V;
+    v.iou = iou;
+    v.tlast = tlast;
+    v.J = J;
+    v.dJ = dJ;
+    v.pop = pop_dev;
+    v.pop_off = pop_off_dev;
+    v.np_params = np_dev;
+    v.out_ptr = out_ptr;
+    v.out_col = out_col;
+    v.out_w = out_w;
+    v.out_deg = out_deg;
+    v.in_ptr = in_ptr;
+    v.in_col = in_col;
+    v.in_w = in_w;
+    v.bits0 = bits0;
+    v.bits1 = bits1;
+    v.rec_bits = rec_bits;
+    v.stat_excl = excl;
+    v.clock = clock;
+    v.seed = seed;
+    v.inj_z = inj_z;
+    v.inj_u = inj_u;
+    v.inj_rows = inj_rows;
+    v.hist_cnt = hist_cnt;
+    v.hist_vsum = hist_vsum;
+    v.events = events;
+    v.ticket = ticket;
+    v.lif_tiles = n_pad / kLifTile;
+    view = v;
+    DTB_CU(cudaMemcpyAsync(view_dev, &view, sizeof(NetView), cudaMemcpyHostToDevice, stream));
+    DTB_CU(cudaStreamSynchronize(stream));
+    return DTB_OK;
+}
+
+LaunchBatch Engine::single_batch() const {
+    LaunchBatch b{};
+    b.nets = view_dev;
+    b.lif_prefix = prefix_dev;
+    b.pull_prefix = prefix_dev + 2;
+    b.vbase = prefix_dev + 4;
+    b.n_nets = 1;
+    b.lif_tiles_total = n_pad / kLifTile;
+    b.pull_tiles_total = n_pad / kPullTile;
+    b.push_ctas = static_cast<uint32_t>(sm_count) * 8u;
+    b.spikes = SpikeList{list, list_count, list_ticket, n_pad};
+    return b;
+}
+
+// Allocations every network needs, independent of its connectivity.
+static int alloc_core(Engine& e) {
+    DTB_TRY(e.dalloc(e.V, e.n_pad));
+    DTB_TRY(e.dalloc(e.iou, e.n_pad));
+    DTB_TRY(e.dalloc(e.tlast, e.n_pad));
+    DTB_TRY(e.dalloc(e.J, e.n_pad));
+    DTB_TRY(e.dalloc(e.pop_dev, e.P));
+    DTB_TRY(e.dalloc(e.pop_off_dev, e.P + 1));
+    DTB_TRY(e.dalloc(e.out_deg, e.n_pad));
+    DTB_TRY(e.dalloc(e.bits0, e.n_words));
+    DTB_TRY(e.dalloc(e.bits1, e.n_words));
+    DTB_TRY(e.dalloc(e.clock, 1));
+    DTB_TRY(e.dalloc(e.events, 1));
+    DTB_TRY(e.dalloc(e.ticket, 1));
+    DTB_TRY(e.dalloc(e.view_dev, 1));
+    DTB_TRY(e.dalloc(e.prefix_dev, 6));
+    DTB_TRY(e.dalloc(e.list, e.n_pad, false));
+    DTB_TRY(e.dalloc(e.list_count, 1));
+    DTB_TRY(e.dalloc(e.list_ticket, 1));
+    const uint32_t pre[6] = {0u, e.n_pad / kLifTile, 0u, e.n_pad / kPullTile, 0u, e.n_pad};
+    DTB_CU(cudaMemcpyAsync(e.prefix_dev, pre, sizeof(pre), cudaMemcpyHostToDevice, e.stream));
+    DTB_CU(cudaMemcpyAsync(e.pop_off_dev, e.pop_off.data(), sizeof(uint32_t) * (e.P + 1), cudaMemcpyHostToDevice, e.stream));
+    DTB_CU(cudaStreamSynchronize(e.stream));
+    e.ou_set.assign(e.P, 0);
+    return DTB_OK;
+}
+
+// Convert one input weight pair to float32.
+static void weight_to_f32(const void* w, uint32_t type, uint64_t e, float& a, float& b) {
+    switch (type) {
+        case DTB_W_F32: { const float* f = static_cast<const float*>(w) + 2 * e; a = f[0]; b = f[1]; break; }
+        case DTB_W_F64: { const double* f = static_cast<const double*>(w) + 2 * e; a = static_cast<float>(f[0]); b = static_cast<float>(f[1]); break; }
+        case DTB_W_F16: { const __half* f = static_cast<const __half*>(w) + 2 * e; a = __half2float(f[0]); b = __half2float(f[1]); break; }
+        case DTB_W_BF16: { const __nv_bfloat16* f = static_cast<const __nv_bfloat16*>(w) + 2 * e; a = __bfloat162float(f[0]); b = __bfloat162float(f[1]); break; }
+        default: { const uint8_t* f = static_cast<const uint8_t*>(w) + 2 * e; a = static_cast<float>(f[0]) / 255.f; b = static_cast<float>(f[1]) / 255.f; break; }
+    }
+}
+
+// Write weight pair e of the input in the device encoding at slot `dst_index`.
+static void encode_weight(const void* w, uint32_t in_type, uint64_t e, uint32_t dev_type, uint8_t* dst, uint64_t dst_index) {
+    if (dev_type == W_U8 && in_type == DTB_W_U8) {
+        std::memcpy(dst + 2 * dst_index, static_cast<const uint8_t*>(w) + 2 * e, 2);
+        return;
+    }
+    if (dev_type == W_F16 && in_type == DTB_W_F16) {
+        std::memcpy(dst + 4 * dst_index, static_cast<const uint8_t*>(w) + 4 * e, 4);
+        return;
+    }
+    float a, b;
+    weight_to_f32(w, in_type, e, a, b);
+    switch (dev_type) {
+        case W_F32: { float* f = reinterpret_cast<float*>(dst) + 2 * dst_index; f[0] = a; f[1] = b; break; }
+        case W_BF16: { __nv_bfloat16* f = reinterpret_cast<__nv_bfloat16*>(dst) + 2 * dst_index; f[0] = __float2bfloat16_rn(a); f[1] = __float2bfloat16_rn(b); break; }
+        case W_F16: { __half* f = reinterpret_cast<__half*>(dst) + 2 * dst_index; f[0] = __float2half_rn(a); f[1] = __float2half_rn(b); break; }
+        default: {
+            uint8_t* f = dst + 2 * dst_index;
+            f[0] = static_cast<uint8_t>(std::lrint(std::min(std::max(a, 0.f), 1.f) * 255.f));
+            f[1] = static_cast<uint8_t>(std::lrint(std::min(std::max(b, 0.f), 1.f) * 255.f));
+            break;
+        }
+    }
+}
+
+int Engine::upload_csr_host(const uint32_t* pre, const uint32_t* post, const uint8_t* kind_in, const void* w,
+                            uint32_t in_type, bool build_push, bool build_pull) {
+    const int wb = weight_bytes();
+    std::vector<uint64_t> ptr, perm;
+    std::vector<uint32_t> deg(n_pad, 0);
+    for (uint64_t e = 0; e < n_edges; ++e) deg[pre[e]]++;
+    DTB_CU(cudaMemcpyAsync(out_deg, deg.data(), sizeof(uint32_t) * n_pad, cudaMemcpyHostToDevice, stream));
+    DTB_CU(cudaStreamSynchronize(stream));
+    auto build = [&](const uint32_t* key, const uint32_t* other, unsigned long long*& d_ptr, uint32_t*& d_col, void*& d_w) -> int {
+        counting_sort(key, n_edges, n, ptr, perm);
+        std::vector<uint32_t> col(n_edges);
+        std::vector<uint8_t> wt(static_cast<size_t>(n_edges) * wb);
+        for (uint64_t q = 0; q < n_edges; ++q) {
+            const uint64_t e = perm[q];
+            col[q] = other[e] | ((kind_in[e] != 0 ? 1u : 0u) << 31);
+            encode_weight(w, in_type, e, wtype, wt.data(), q);
+        }
+        DTB_TRY(dalloc(d_ptr, static_cast<size_t>(n) + 1, false));
+        DTB_TRY(dalloc(d_col, n_edges, false));
+        uint8_t* wdev = nullptr;
+        DTB_TRY(dalloc(wdev, static_cast<size_t>(n_edges) * wb, false));
+        d_w = wdev;
+        DTB_CU(cudaMemcpyAsync(d_ptr, ptr.data(), sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, stream));
+        DTB_CU(cudaMemcpyAsync(d_col, col.data(), sizeof(uint32_t) * n_edges, cudaMemcpyHostToDevice, stream));
+        DTB_CU(cudaMemcpyAsync(wdev, wt.data(), wt.size(), cudaMemcpyHostToDevice, stream));
+        DTB_CU(cudaStreamSynchronize(stream));
+        return DTB_OK;
+    };
+    if (build_push) {
+        DTB_TRY(build(pre, post, out_ptr, out_col, out_w));
+        has_push = true;
+    }
+    if (build_pull) {
+        DTB_TRY(build(post, pre, in_ptr, in_col, in_w));
+        has_pull = true;
+    }
+    return DTB_OK;
+}
+
+int Engine::create_from_arrays(const dtb_network_arrays& a, const dtb_options& opt) {
+    if (!a.property) return fail(DTB_INVALID_PARAMETER, "property is NULL");
+    if (a.n_edges && (!a.input_neuron_idx || !a.output_neuron_idx || !a.input_channel_offset || !a.weight))
+        return fail(DTB_INVALID_PARAMETER, "edge arrays missing");
+    if (a.weight_type > DTB_W_F64) return fail(DTB_UNSUPPORTED, "unknown input weight type");
+    if (!opt.build_push && !opt.build_pull) return fail(DTB_INVALID_PARAMETER, "neither push nor pull CSR requested");
+    DTB_TRY(init_common(opt, a.n_neurons));
+    n_edges = a.n_edges;
+    for (uint64_t e = 0; e < n_edges; ++e) {
+        if (a.input_neuron_idx[e] >= n || a.output_neuron_idx[e] >= n)
+            return fail(DTB_INVALID_NETWORK, "edge " + std::to_string(e) + " references a neuron outside the block");
+        if (a.input_block_idx && a.input_block_idx[e] != 0)
+            return fail(DTB_UNSUPPORTED, "edges from other blocks (input_block_idx != 0): one network per GPU");
+    }
+    DTB_TRY(setup_populations_from_property(a.property));
+    // per-population parameters; per-neuron mode if any population is not uniform
+    pop_raw.resize(P);
+    for (uint32_t p = 0; p < P; ++p) {
+        const float* row0 = a.property + static_cast<size_t>(pop_off[p]) * 22;
+        pop_raw[p] = raw_from_property(row0, opt.ou_mean, opt.ou_sigma, opt.ou_tau);
+        for (uint32_t i = pop_off[p] + 1; i < pop_off[p + 1] && !per_neuron; ++i)
+            if (!same_params(row0, a.property + static_cast<size_t>(i) * 22)) per_neuron = true;
+    }
+    if (per_neuron) {
+        neuron_raw.resize(n);
+        for (uint32_t i = 0; i < n; ++i)
+            neuron_raw[i] = raw_from_property(a.property + static_cast<size_t>(i) * 22, opt.ou_mean, opt.ou_sigma, opt.ou_tau);
+    }
+    DTB_TRY(alloc_core(*this));
+    // statistics exclusion (column 1, blocked_in_stat)
+    excl_count.assign(P, 0);
+    std::vector<uint32_t> ex(n_words, 0);
+    bool any_ex = false;
+    for (uint32_t p = 0; p < P; ++p)
+        for (uint32_t i = pop_off[p]; i < pop_off[p + 1]; ++i)
+            if (a.property[static_cast<size_t>(i) * 22 + 1] != 0.0f) {
+                ex[i >> 5] |= 1u << (i & 31);
+                excl_count[p]++;
+                any_ex = true;
+            }
+    if (any_ex) {
+        DTB_TRY(dalloc(excl, n_words));
+        DTB_CU(cudaMemcpyAsync(excl, ex.data(), sizeof(uint32_t) * n_words, cudaMemcpyHostToDevice, stream));
+    }
+    DTB_TRY(upload_csr_host(a.input_neuron_idx, a.output_neuron_idx, a.input_channel_offset, a.weight, a.weight_type,
+                            opt.build_push != 0, opt.build_pull != 0));
+    DTB_TRY(upload_params());
+    DTB_TRY(init_state());
+    return refresh_view();
+}
+
+int Engine::create_structured(const dtb_structured_spec& s, const dtb_options& opt) {
+    if (s.n_pops == 0 || !s.pop_sizes || !s.pop_exc || !s.src_cdf || !s.pop_property)
+        return fail(DTB_INVALID_PARAMETER, "structured spec incomplete");
+    if (s.in_degree == 0) return fail(DTB_INVALID_PARAMETER, "in_degree must be positive");
+    if (!opt.build_push && !opt.build_pull) return fail(DTB_INVALID_PARAMETER, "neither push nor pull CSR requested");
+    uint64_t total = 0;
+    for (uint32_t b = 0; b < s.n_pops; ++b) {
+        if (s.pop_sizes[b] < 2) return fail(DTB_INVALID_PARAMETER, "every population needs at least 2 neurons");
+        if (s.pop_exc[b] > s.pop_sizes[b]) return fail(DTB_INVALID_PARAMETER, "pop_exc larger than the population");
+        total += s.pop_sizes[b];
+        const uint64_t* row = s.src_cdf + static_cast<size_t>(b) * s.n_pops;
+        if (row[s.n_pops - 1] != (1ull << 32)) return fail(DTB_INVALID_PARAMETER, "src_cdf rows must end at 2^32");
+        for (uint32_t c = 1; c < s.n_pops; ++c)
+            if (row[c] < row[c - 1]) return fail(DTB_INVALID_PARAMETER, "src_cdf rows must be non-decreasing");
+    }
+    if (total >= 0x7FFFFFFFull - kPad) return fail(DTB_UNSUPPORTED, "more than 2^31 neurons");
+    DTB_TRY(init_common(opt, static_cast<uint32_t>(total)));
+    n_edges = static_cast<uint64_t>(n) * s.in_degree;
+    P = s.n_pops;
+    pop_ids.resize(P);
+    pop_off.resize(P + 1);
+    pop_raw.resize(P);
+    pop_off[0] = 0;
+    for (uint32_t b = 0; b < P; ++b) {
+        pop_ids[b] = s.pop_id_base + b;
+        pop_off[b + 1] = pop_off[b] + s.pop_sizes[b];
+        pop_raw[b] = raw_from_property(s.pop_property + static_cast<size_t>(b) * 22, opt.ou_mean, opt.ou_sigma, opt.ou_tau);
+    }
+    excl_count.assign(P, 0);
+    DTB_TRY(alloc_core(*this));
+    // device tables for the generator
+    uint32_t* d_exc = nullptr;
+    unsigned long long* d_cdf = nullptr;
+    DTB_TRY(dalloc(d_exc, P));
+    DTB_TRY(dalloc(d_cdf, static_cast<size_t>(P) * P));
+    DTB_CU(cudaMemcpyAsync(d_exc, s.pop_exc, sizeof(uint32_t) * P, cudaMemcpyHostToDevice, stream));
+    DTB_CU(cudaMemcpyAsync(d_cdf, s.src_cdf, sizeof(uint64_t) * P * P, cudaMemcpyHostToDevice, stream));
+    const int wb = weight_bytes();
+    if (opt.build_push) {
+        DTB_TRY(dalloc(out_ptr, static_cast<size_t>(n) + 1, false));
+        DTB_TRY(dalloc(out_col, n_edges, false));
+        uint8_t* w = nullptr;
+        DTB_TRY(dalloc(w, static_cast<size_t>(n_edges) * wb, false));
+        out_w = w;
+        has_push = true;
+    }
+    if (opt.build_pull) {
+        DTB_TRY(dalloc(in_ptr, static_cast<size_t>(n) + 1, false));
+        DTB_TRY(dalloc(in_col, n_edges, false));
+        uint8_t* w = nullptr;
+        DTB_TRY(dalloc(w, static_cast<size_t>(n_edges) * wb, false));
+        in_w = w;
+        has_pull = true;
+    }
+    GenSpec g{};
+    g.n = n;
+    g.n_pops = P;
+    g.in_degree = s.in_degree;
+    g.dyadic = s.dyadic_weights;
+    g.seed = s.seed;
+    g.pop_off = pop_off_dev;
+    g.pop_exc = d_exc;
+    g.cdf = d_cdf;
+    const cudaError_t ge = build_structured(g, static_cast<int>(wtype), out_ptr, out_col, out_w, in_ptr, in_col, in_w, out_deg, stream);
+    if (ge == cudaErrorUnknown) return fail(DTB_DEVICE_FAULT, "device CSR build: placement check failed");
+    if (ge != cudaSuccess) return cuda_fail(ge, "build_structured");
+    dfree(d_exc);
+    dfree(d_cdf);
+    dev_bytes -= sizeof(uint32_t) * P + sizeof(unsigned long long) * P * P;
+    DTB_TRY(upload_params());
+    DTB_TRY(init_state());
+    return refresh_view();
+}
+
+int Engine::create_from_npz(const std::string& path, const dtb_options& opt) {
+    std::vector<std::string> names = {"property", "input_block_idx", "input_neuron_idx", "output_neuron_idx",
+                                      "input_channel_offset", "weight", "src_timestamp"};
+    std::vector<NpyArray> arr;
+    std::vector<bool> found;
+    const std::string err = npz_load(path, names, arr, found);
+    if (!err.empty()) return fail(DTB_IO_ERROR, err);
+    if (found[6]) return fail(DTB_UNSUPPORTED, "input (spike replay) blocks are not supported");
+    for (int k : {0, 2, 3, 4, 5})
+        if (!found[k]) return fail(DTB_IO_ERROR, "npz member missing: " + names[k]);
+    for (const auto& a : arr)
+        if (a.fortran) return fail(DTB_UNSUPPORTED, "Fortran-ordered arrays");
+    const NpyArray& prop = arr[0];
+    if (prop.dtype != "<f4" || prop.shape.size() != 2 || prop.shape[1] != 22)
+        return fail(DTB_INVALID_NETWORK, "property must be float32 [N, 22]");
+    const uint64_t S = arr[2].count();
+    if (arr[2].dtype != "<u4" || arr[3].dtype != "<u4" || arr[3].count() != S)
+        return fail(DTB_INVALID_NETWORK, "input/output_neuron_idx must be uint32 [S]");
+    if (arr[4].word() != 1 || arr[4].count() != S) return fail(DTB_INVALID_NETWORK, "input_channel_offset must be uint8 [S]");
+    const NpyArray& w = arr[5];
+    if (w.shape.size() != 2 || w.shape[0] != S || w.shape[1] != 2) return fail(DTB_INVALID_NETWORK, "weight must be [S, 2]");
+    uint32_t wt;
+    if (w.dtype == "<f4") wt = DTB_W_F32;
+    else if (w.dtype == "<f8") wt = DTB_W_F64;
+    else if (w.dtype == "<f2") wt = DTB_W_F16;
+    else if (w.dtype == "|u1" || w.dtype == "|i1") wt = DTB_W_U8;
+    else return fail(DTB_UNSUPPORTED, "weight dtype " + w.dtype);
+    std::vector<int16_t> blk;
+    if (found[1]) {
+        const NpyArray& b = arr[1];
+        if (b.count() != S || b.word() != 2) return fail(DTB_INVALID_NETWORK, "input_block_idx must be int16/uint16 [S]");
+        blk.resize(S);
+        std::memcpy(blk.data(), b.data.data(), S * 2);
+    }
+    dtb_network_arrays a{};
+    a.n_neurons = static_cast<uint32_t>(prop.shape[0]);
+    a.property = reinterpret_cast<const float*>(prop.data.data());
+    a.n_edges = S;
+    a.input_block_idx = found[1] ? blk.data() : nullptr;
+    a.input_neuron_idx = reinterpret_cast<const uint32_t*>(arr[2].data.data());
+    a.output_neuron_idx = reinterpret_cast<const uint32_t*>(arr[3].data.data());
+    a.input_channel_offset = arr[4].data.data();
+    a.weight = w.data.data();
+    a.weight_type = wt;
+    return create_from_arrays(a, opt);
+}
+
+int Engine::ensure_dj() {
+    if (dJ) return DTB_OK;
+    DTB_TRY(dalloc(dJ, static_cast<size_t>(n_pad) * 4));
+    DTB_CU(cudaStreamSynchronize(stream));
+    return refresh_view();
+}
+
+int Engine::ensure_hist(uint32_t rows, bool record) {
+    bool changed = false;
+    if (rows > hist_cap) {
+        dfree(hist_cnt);
+        dfree(hist_vsum);
+        hist_cnt = nullptr;
+        hist_vsum = nullptr;
+        DTB_TRY(dalloc(hist_cnt, static_cast<size_t>(rows) * P));
+        DTB_TRY(dalloc(hist_vsum, static_cast<size_t>(rows) * P));
+        hist_cap = rows;
+        changed = true;
+        if (h_cnt) cudaFreeHost(h_cnt);
+        if (h_vsum) cudaFreeHost(h_vsum);
+        h_cnt = nullptr;
+        h_vsum = nullptr;
+        DTB_CU(cudaMallocHost(&h_cnt, sizeof(int) * rows * P));
+        DTB_CU(cudaMallocHost(&h_vsum, sizeof(long long) * rows * P));
+        h_cap = rows;
+    }
+    if (record && rec_cap < hist_cap) {
+        dfree(rec_bits);
+        rec_bits = nullptr;
+        DTB_TRY(dalloc(rec_bits, static_cast<size_t>(hist_cap) * n_words));
+        rec_cap = hist_cap;
+        changed = true;
+    }
+    if (changed) return refresh_view();
+    return DTB_OK;
+}
+
+int Engine::begin_run_chunk(uint64_t run_base, uint32_t rows, bool stats) {
+    set_u64_kernel<<<1, 1, 0, stream>>>(&clock->run_base, run_base);
+    DTB_CU(cudaGetLastError());
+    if (stats) {
+        DTB_CU(cudaMemsetAsync(hist_cnt, 0, sizeof(int) * rows * P, stream));
+        DTB_CU(cudaMemsetAsync(hist_vsum, 0, sizeof(long long) * rows * P, stream));
+    }
+    return DTB_OK;
+}
+
+int Engine::finish_hist(uint32_t rows, uint32_t out_row0, const dtb_run_output& out, bool freq, bool vmean, bool record) {
+    if (freq || vmean) {
+        DTB_CU(cudaMemcpyAsync(h_cnt, hist_cnt, sizeof(int) * rows * P, cudaMemcpyDeviceToHost, stream));
+        DTB_CU(cudaMemcpyAsync(h_vsum, hist_vsum, sizeof(long long) * rows * P, cudaMemcpyDeviceToHost, stream));
+    }
+    if (record) {
+        const size_t out_words = (n + 31) / 32;
+        DTB_CU(cudaMemcpy2DAsync(out.spike_bits + static_cast<size_t>(out_row0) * out_words, out_words * 4, rec_bits,
+                                 static_cast<size_t>(n_words) * 4, out_words * 4, rows, cudaMemcpyDeviceToHost, stream));
+    }
+    DTB_CU(cudaStreamSynchronize(stream));
+    for (uint32_t r = 0; r < rows && (freq || vmean); ++r) {
+        for (uint32_t p = 0; p < P; ++p) {
+            const size_t src = static_cast<size_t>(r) * P + p;
+            const size_t dst = static_cast<size_t>(out_row0 + r) * P + p;
+            if (freq) out.freqs[dst] = h_cnt[src];
+            if (vmean) {
+                const uint32_t cnt = pop_off[p + 1] - pop_off[p] - excl_count[p];
+                out.vmeans[dst] = cnt ? static_cast<float>(static_cast<double>(h_vsum[src]) / kVsumScale / static_cast<double>(cnt)) : 0.0f;
+            }
+        }
+    }
+    return DTB_OK;
+}
+
+int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
+    if (rq.iters == 0) return fail(DTB_INVALID_PARAMETER, "iter must be positive");
+    if (rq.prop_mode > DTB_PROP_OR) return fail(DTB_INVALID_PARAMETER, "unknown prop_mode");
+    if (rq.syn_mode > DTB_SYN_PULL) return fail(DTB_INVALID_PARAMETER, "unknown syn_mode");
+    if (rq.syn_mode != DTB_SYN_PULL && !has_push) return fail(DTB_UNSUPPORTED, "network was built without the out-degree CSR");
+    if (rq.syn_mode == DTB_SYN_PULL && !has_pull) return fail(DTB_UNSUPPORTED, "network was built without the in-degree CSR");
+    const bool freq = (rq.flags & DTB_RUN_FREQ) != 0;
+    const bool vmean = (rq.flags & DTB_RUN_VMEAN) != 0;
+    const bool record = (rq.flags & DTB_RUN_RECORD_SPIKES) != 0;
+    if ((freq && !out.freqs) || (vmean && !out.vmeans) || (record && !out.spike_bits))
+        return fail(DTB_INVALID_PARAMETER, "requested output buffer is NULL");
+    const bool injected = noise_src == DTB_NOISE_INJECTED;
+    if (injected) {
+        const uint64_t used = steps - inj_first;
+        if (used + rq.iters > inj_rows) return fail(DTB_INVALID_PARAMETER, "not enough injected noise rows for this run");
+        if (rq.prop_mode != DTB_PROP_THRESHOLD && !inj_u) return fail(DTB_INVALID_PARAMETER, "noise train needs injected uniforms");
+    }
+    if (rq.syn_mode == DTB_SYN_PUSH_EXACT) DTB_TRY(ensure_dj());
+    uint32_t cap = std::min<uint32_t>(rq.iters, 4096u);
+    if (record) cap = std::min<uint32_t>(cap, std::max<uint32_t>(1u, static_cast<uint32_t>((512ull << 20) / (4ull * n_words))));
+    DTB_TRY(ensure_hist(cap, record));
+    uint32_t kflags = 0;
+    if (rq.flags & DTB_RUN_USE_OU) kflags |= kFlagUseOU;
+    if (freq || vmean) kflags |= kFlagStats;
+    if (record) kflags |= kFlagRecord;
+    if (rq.syn_mode != DTB_SYN_PULL) kflags |= kFlagList;
+    if (injected) kflags |= kFlagInjected;
+    const LaunchBatch b = single_batch();
+    const int pm = static_cast<int>(rq.prop_mode);
+    set_u64_kernel<<<1, 1, 0, stream>>>(events, 0ull);
+    DTB_CU(cudaGetLastError());
+    double ms_total = 0.0;
+    uint32_t done = 0;
+    while (done < rq.iters) {
+        const uint32_t rows = std::min(cap, rq.iters - done);
+        DTB_TRY(begin_run_chunk(steps, rows, freq || vmean));
+        DTB_CU(cudaEventRecord(ev0, stream));
+        for (uint32_t s = 0; s < rows; ++s) {
+            const bool first = (done + s) == 0;
+            switch (rq.syn_mode) {
+                case DTB_SYN_PUSH:
+                    DTB_CU(launch_lif(b, J_DIRECT, kflags, pm, stream));
+                    DTB_CU(launch_push(b, 0, static_cast<int>(wtype), stream));
+                    break;
+                case DTB_SYN_PUSH_EXACT:
+                    DTB_CU(launch_lif(b, first ? J_ASIS : J_FOLD, kflags, pm, stream));
+                    DTB_CU(launch_push(b, 1, static_cast<int>(wtype), stream));
+                    break;
+                default:
+                    DTB_CU(launch_pull(b, first ? 0 : 1, static_cast<int>(wtype), kflags, pm, stream));
+                    break;
+            }
+        }
+        if (done + rows == rq.iters) {
+            if (rq.syn_mode == DTB_SYN_PUSH_EXACT) DTB_CU(launch_fold_finish(b, stream));
+            if (rq.syn_mode == DTB_SYN_PULL) DTB_CU(launch_gather_finish(b, static_cast<int>(wtype), stream));
+        }
+        DTB_CU(cudaEventRecord(ev1, stream));
+        DTB_CU(cudaEventSynchronize(ev1));
+        float ms = 0.f;
+        DTB_CU(cudaEventElapsedTime(&ms, ev0, ev1));
+        ms_total += ms;
+        for (uint32_t s = 0; s < rows; ++s) {
+            volatile float tt = t + dt;
+            t = tt;
+        }
+        steps += rows;
+        DTB_TRY(finish_hist(rows, done, out, freq, vmean, record));
+        done += rows;
+    }
+    Clock ck;
+    unsigned long long ev = 0;
+    DTB_CU(cudaMemcpyAsync(&ck, clock, sizeof(Clock), cudaMemcpyDeviceToHost, stream));
+    DTB_CU(cudaMemcpyAsync(&ev, events, sizeof(ev), cudaMemcpyDeviceToHost, stream));
+    DTB_CU(cudaStreamSynchronize(stream));
+    out.events = ev;
+    out.device_ms = ms_total;
+    if (ck.n != steps) return fail(DTB_DEVICE_FAULT, "device clock out of step with the host");
+    if (ck.err) {
+        set_clock_kernel<<<1, 1, 0, stream>>>(clock, ck.t, ck.n);
+        cudaStreamSynchronize(stream);
+        return fail(DTB_DEVICE_FAULT, "kernel check failed, error bits " + std::to_string(ck.err));
+    }
+    return DTB_OK;
+}
+
+int Engine::info(dtb_engine_info& inf) const {
+    inf.n_neurons = n;
+    inf.n_pops = P;
+    inf.n_edges = n_edges;
+    inf.device_bytes = dev_bytes;
+    inf.step = steps;
+    inf.t = t;
+    inf.weight_type = wtype;
+    inf.has_push = has_push;
+    inf.has_pull = has_pull;
+    inf.per_neuron_params = per_neuron;
+    return DTB_OK;
+}
+
+int Engine::populations(uint32_t* ids, uint32_t* counts) const {
+    for (uint32_t p = 0; p < P; ++p) {
+        if (ids) ids[p] = pop_ids[p];
+        if (counts) counts[p] = pop_off[p + 1] - pop_off[p];
+    }
+    return DTB_OK;
+}
+
+static void to_per_neuron(Engine& e) {
+    if (e.per_neuron) return;
+    e.neuron_raw.resize(e.n);
+    for (uint32_t p = 0; p < e.P; ++p)
+        for (uint32_t i = e.pop_off[p]; i < e.pop_off[p + 1]; ++i) e.neuron_raw[i] = e.pop_raw[p];
+    e.per_neuron = true;
+}
+
+int Engine::update_props(uint32_t cnt, const uint32_t* nid, const uint32_t* pid, const float* val) {
+    if (cnt == 0) return DTB_OK;
+    if (!nid || !pid || !val) return fail(DTB_INVALID_PARAMETER, "NULL array");
+    to_per_neuron(*this);
+    for (uint32_t k = 0; k < cnt; ++k) {
+        if (nid[k] >= n) continue;   // the reference ignores out-of-range neurons (property.cpp:72)
+        float* f = nullptr;
+        if (!raw_field(neuron_raw[nid[k]], pid[k], &f)) continue;
+        *f = val[k];
+    }
+    return upload_params();
+}
+
+int Engine::update_prop_cols(uint32_t cnt, const uint32_t* pid, const uint32_t* pop, const float* val, int assign) {
+    if (cnt == 0) return DTB_OK;
+    if (!pid || !pop || !val) return fail(DTB_INVALID_PARAMETER, "NULL array");
+    for (uint32_t k = 0; k < cnt; ++k) {
+        for (uint32_t p = 0; p < P; ++p) {
+            if (pop_ids[p] != pop[k]) continue;
+            float* f = nullptr;
+            if (!raw_field(pop_raw[p], pid[k], &f)) continue;
+            *f = assign ? val[k] : *f * val[k];
+            if (per_neuron) {
+                for (uint32_t i = pop_off[p]; i < pop_off[p + 1]; ++i) {
+                    float* g = nullptr;
+                    raw_field(neuron_raw[i], pid[k], &g);
+                    *g = assign ? val[k] : *g * val[k];
+                }
+            }
+        }
+    }
+    return upload_params();
+}
+
+// Gamma(alpha, 1) by Marsaglia & Tsang (2000), "A simple method for generating
+// gamma variables", with the alpha < 1 boost U^(1/alpha) * Gamma(alpha + 1).
+static double sample_gamma(double alpha, std::mt19937_64& rng) {
+    std::uniform_real_distribution<double> uni(0.0, 1.0);
+    std::normal_distribution<double> nrm(0.0, 1.0);
+    if (alpha <= 0.0) return 0.0;
+    double scale = 1.0;
+    if (alpha < 1.0) {
+        scale = std::pow(1.0 - uni(rng), 1.0 / alpha);
+        alpha += 1.0;
+    }
+    const double d = alpha - 1.0 / 3.0, c = 1.0 / std::sqrt(9.0 * d);
+    for (;;) {
+        double x, v;
+        do { x = nrm(rng); v = 1.0 + c * x; } while (v <= 0.0);
+        v = v * v * v;
+        const double u = 1.0 - uni(rng);
+        const double xx = x * x;
+        if (u < 1.0 - 0.0331 * xx * xx) return scale * d * v;
+        if (std::log(u) < 0.5 * xx + d * (1.0 - v + std::log(v))) return scale * d * v;
+    }
+}
+
+int Engine::update_gamma(uint32_t cnt, const uint32_t* pid, const uint32_t* pop, const float* alpha, const float* beta) {
+    if (cnt == 0) return DTB_OK;
+    if (!pid || !pop || !alpha || !beta) return fail(DTB_INVALID_PARAMETER, "NULL array");
+    for (uint32_t k = 0; k < cnt; ++k)
+        if (!(alpha[k] >= 0.0f) || !(beta[k] > 0.0f)) return fail(DTB_INVALID_PARAMETER, "gamma needs alpha >= 0 and beta > 0");
+    to_per_neuron(*this);
+    std::mt19937_64 rng(seed ^ (0x9E3779B97F4A7C15ull * (++gamma_calls)));
+    for (uint32_t k = 0; k < cnt; ++k) {
+        for (uint32_t p = 0; p < P; ++p) {
+            if (pop_ids[p] != pop[k]) continue;
+            for (uint32_t i = pop_off[p]; i < pop_off[p + 1]; ++i) {
+                float* f = nullptr;
+                if (!raw_field(neuron_raw[i], pid[k], &f)) break;
+                *f = static_cast<float>(sample_gamma(alpha[k], rng) / beta[k]);
+            }
+        }
+    }
+    return upload_params();
+}
+
+int Engine::set_ou(uint32_t cnt, const uint32_t* pop, const float* mean, const float* sigma, const float* tau) {
+    if (cnt == 0) return DTB_OK;
+    if (!pop || !mean || !sigma || !tau) return fail(DTB_INVALID_PARAMETER, "NULL array");
+    for (uint32_t k = 0; k < cnt; ++k)
+        if (!(tau[k] > 0.0f) || !(sigma[k] >= 0.0f)) return fail(DTB_INVALID_PARAMETER, "OU needs tau > 0 and sigma >= 0");
+    for (uint32_t k = 0; k < cnt; ++k) {
+        for (uint32_t p = 0; p < P; ++p) {
+            if (pop_ids[p] != pop[k]) continue;
+            pop_raw[p].ou_mean = mean[k];
+            pop_raw[p].ou_sigma = sigma[k];
+            pop_raw[p].ou_tau = tau[k];
+            if (per_neuron)
+                for (uint32_t i = pop_off[p]; i < pop_off[p + 1]; ++i) {
+                    neuron_raw[i].ou_mean = mean[k];
+                    neuron_raw[i].ou_sigma = sigma[k];
+                    neuron_raw[i].ou_tau = tau[k];
+                }
+            if (!ou_set[p]) {
+                // first configuration resets the population's OU current to its mean (src/block.cpp:244-266)
+                fill_range_kernel<<<64, 256, 0, stream>>>(iou, pop_off[p], pop_off[p + 1], mean[k]);
+                DTB_CU(cudaGetLastError());
+                ou_set[p] = 1;
+            }
+        }
+    }
+    return upload_params();
+}
+
+int Engine::set_noise(uint32_t source, uint32_t rows, const float* z, const float* u) {
+    if (source > DTB_NOISE_INJECTED) return fail(DTB_INVALID_PARAMETER, "unknown noise source");
+    dfree(inj_z);
+    dfree(inj_u);
+    inj_z = inj_u = nullptr;
+    inj_rows = 0;
+    noise_src = static_cast<int>(source);
+    if (source == DTB_NOISE_INJECTED) {
+        if (rows == 0 || !z) return fail(DTB_INVALID_PARAMETER, "injected noise needs rows and z");
+        DTB_TRY(dalloc(inj_z, static_cast<size_t>(rows) * n_pad));
+        DTB_CU(cudaMemcpy2DAsync(inj_z, sizeof(float) * n_pad, z, sizeof(float) * n, sizeof(float) * n, rows,
+                                 cudaMemcpyHostToDevice, stream));
+        if (u) {
+            DTB_TRY(dalloc(inj_u, static_cast<size_t>(rows) * n_pad));
+            DTB_CU(cudaMemcpy2DAsync(inj_u, sizeof(float) * n_pad, u, sizeof(float) * n, sizeof(float) * n, rows,
+                                     cudaMemcpyHostToDevice, stream));
+        }
+        inj_rows = rows;
+        inj_first = steps;
+        set_u64_kernel<<<1, 1, 0, stream>>>(&clock->inj_base, steps);
+        DTB_CU(cudaGetLastError());
+    }
+    DTB_CU(cudaStreamSynchronize(stream));
+    return refresh_view();
+}
+
+int Engine::read_state(int which, void* dst) {
+    if (!dst) return fail(DTB_INVALID_PARAMETER, "NULL destination");
+    switch (which) {
+        case DTB_STATE_V: DTB_CU(cudaMemcpyAsync(dst, V, sizeof(float) * n, cudaMemcpyDeviceToHost, stream)); break;
+        case DTB_STATE_J: DTB_CU(cudaMemcpyAsync(dst, J, sizeof(float4) * n, cudaMemcpyDeviceToHost, stream)); break;
+        case DTB_STATE_I_OU: DTB_CU(cudaMemcpyAsync(dst, iou, sizeof(float) * n, cudaMemcpyDeviceToHost, stream)); break;
+        case DTB_STATE_T_LAST: DTB_CU(cudaMemcpyAsync(dst, tlast, sizeof(float) * n, cudaMemcpyDeviceToHost, stream)); break;
+        default: return fail(DTB_INVALID_PARAMETER, "unknown state id");
+    }
+    DTB_CU(cudaStreamSynchronize(stream));
+    return DTB_OK;
+}
+
+int Engine::write_state(int which, const void* src) {
+    if (!src) return fail(DTB_INVALID_PARAMETER, "NULL source");
+    switch (which) {
+        case DTB_STATE_V: DTB_CU(cudaMemcpyAsync(V, src, sizeof(float) * n, cudaMemcpyHostToDevice, stream)); break;
+        case DTB_STATE_J: DTB_CU(cudaMemcpyAsync(J, src, sizeof(float4) * n, cudaMemcpyHostToDevice, stream)); break;
+        case DTB_STATE_I_OU: DTB_CU(cudaMemcpyAsync(iou, src, sizeof(float) * n, cudaMemcpyHostToDevice, stream)); break;
+        case DTB_STATE_T_LAST: DTB_CU(cudaMemcpyAsync(tlast, src, sizeof(float) * n, cudaMemcpyHostToDevice, stream)); break;
+        default: return fail(DTB_INVALID_PARAMETER, "unknown state id");
+    }
+    DTB_CU(cudaStreamSynchronize(stream));
+    return DTB_OK;
+}
+
+int Engine::read_out_csr(uint32_t* n_rows, uint64_t* n_edges_out, uint32_t* rows, uint64_t* row_ptr, uint32_t* post,
+                         uint8_t* kind, float* weight) {
+    if (!has_push) return fail(DTB_UNSUPPORTED, "network was built without the out-degree CSR");
+    std::vector<unsigned long long> ptr(static_cast<size_t>(n) + 1);
+    DTB_CU(cudaMemcpyAsync(ptr.data(), out_ptr, sizeof(unsigned long long) * (n + 1), cudaMemcpyDeviceToHost, stream));
+    DTB_CU(cudaStreamSynchronize(stream));
+    uint32_t nr = 0;
+    for (uint32_t j = 0; j < n; ++j) {
+        if (ptr[j + 1] > ptr[j]) {
+            if (rows) rows[nr] = j;
+            if (row_ptr) row_ptr[nr] = ptr[j];
+            ++nr;
+        }
+    }
+    if (row_ptr) row_ptr[nr] = ptr[n];
+    *n_rows = nr;
+    *n_edges_out = n_edges;
+    if (post || kind) {
+        std::vector<uint32_t> col(n_edges);
+        DTB_CU(cudaMemcpyAsync(col.data(), out_col, sizeof(uint32_t) * n_edges, cudaMemcpyDeviceToHost, stream));
+        DTB_CU(cudaStreamSynchronize(stream));
+        for (uint64_t e = 0; e < n_edges; ++e) {
+            if (post) post[e] = col[e] & kIndexMask;
+            if (kind) kind[e] = static_cast<uint8_t>(col[e] >> 31);
+        }
+    }
+    if (weight) {
+        const int wb = weight_bytes();
+        std::vector<uint8_t> w(static_cast<size_t>(n_edges) * wb);
+        DTB_CU(cudaMemcpyAsync(w.data(), out_w, w.size(), cudaMemcpyDeviceToHost, stream));
+        DTB_CU(cudaStreamSynchronize(stream));
+        const uint32_t as_in = wtype == W_F32 ? DTB_W_F32 : wtype == W_BF16 ? DTB_W_BF16 : wtype == W_F16 ? DTB_W_F16 : DTB_W_U8;
+        for (uint64_t e = 0; e < n_edges; ++e) weight_to_f32(w.data(), as_in, e, weight[2 * e], weight[2 * e + 1]);
+    }
+    return DTB_OK;
+}
+
+// State blob: header, V, i_ou, t_last, J, both spike-bit buffers.
+struct BlobHeader {
+    uint64_t magic, n, n_words, steps;
+    float t;
+    uint32_t pad;
+};
+static constexpr uint64_t kBlobMagic = 0x44544242'53544154ull;
+
+uint64_t Engine::state_size() const {
+    return sizeof(BlobHeader) + sizeof(float) * 3ull * n + sizeof(float4) * static_cast<uint64_t>(n) + 8ull * n_words;
+}
+
+int Engine::save_state(void* blob, uint64_t bytes) {
+    if (!blob || bytes < state_size()) return fail(DTB_INVALID_PARAMETER, "state blob too small");
+    uint8_t* p = static_cast<uint8_t*>(blob);
+    BlobHeader h{kBlobMagic, n, n_words, steps, t, 0};
+    std::memcpy(p, &h, sizeof(h));
+    p += sizeof(h);
+    DTB_CU(cudaMemcpyAsync(p, V, sizeof(float) * n, cudaMemcpyDeviceToHost, stream)); p += sizeof(float) * n;
+    DTB_CU(cudaMemcpyAsync(p, iou, sizeof(float) * n, cudaMemcpyDeviceToHost, stream)); p += sizeof(float) * n;
+    DTB_CU(cudaMemcpyAsync(p, tlast, sizeof(float) * n, cudaMemcpyDeviceToHost, stream)); p += sizeof(float) * n;
+    DTB_CU(cudaMemcpyAsync(p, J, sizeof(float4) * n, cudaMemcpyDeviceToHost, stream)); p += sizeof(float4) * n;
+    DTB_CU(cudaMemcpyAsync(p, bits0, 4ull * n_words, cudaMemcpyDeviceToHost, stream)); p += 4ull * n_words;
+    DTB_CU(cudaMemcpyAsync(p, bits1, 4ull * n_words, cudaMemcpyDeviceToHost, stream));
+    DTB_CU(cudaStreamSynchronize(stream));
+    return DTB_OK;
+}
+
+int Engine::load_state(const void* blob, uint64_t bytes) {
+    if (!blob || bytes < state_size()) return fail(DTB_INVALID_PARAMETER, "state blob too small");
+    const uint8_t* p = static_cast<const uint8_t*>(blob);
+    BlobHeader h;
+    std::memcpy(&h, p, sizeof(h));
+    if (h.magic != kBlobMagic || h.n != n || h.n_words != n_words) return fail(DTB_INVALID_PARAMETER, "state blob is for another network");
+    p += sizeof(h);
+    DTB_CU(cudaMemcpyAsync(V, p, sizeof(float) * n, cudaMemcpyHostToDevice, stream)); p += sizeof(float) * n;
+    DTB_CU(cudaMemcpyAsync(iou, p, sizeof(float) * n, cudaMemcpyHostToDevice, stream)); p += sizeof(float) * n;
+    DTB_CU(cudaMemcpyAsync(tlast, p, sizeof(float) * n, cudaMemcpyHostToDevice, stream)); p += sizeof(float) * n;
+    DTB_CU(cudaMemcpyAsync(J, p, sizeof(float4) * n, cudaMemcpyHostToDevice, stream)); p += sizeof(float4) * n;
+    DTB_CU(cudaMemcpyAsync(bits0, p, 4ull * n_words, cudaMemcpyHostToDevice, stream)); p += 4ull * n_words;
+    DTB_CU(cudaMemcpyAsync(bits1, p, 4ull * n_words, cudaMemcpyHostToDevice, stream));
+    if (dJ) DTB_CU(cudaMemsetAsync(dJ, 0, sizeof(long long) * 4 * n_pad, stream));
+    set_clock_kernel<<<1, 1, 0, stream>>>(clock, h.t, h.steps);
+    DTB_CU(cudaGetLastError());
+    DTB_CU(cudaStreamSynchronize(stream));
+    steps = h.steps;
+    t = h.t;
+    return DTB_OK;
+}
+
+}  // namespace dtb
+
+// ===========================================================================
+// C-ABI
+// ===========================================================================
+using dtb::Engine;
+
+namespace {
+
+template <class F>
+int32_t guarded(F&& f) {
+    try {
+        return static_cast<int32_t>(f());
+    } catch (const std::bad_alloc&) {
+        return dtb::fail(DTB_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception& e) {
+        return dtb::fail(DTB_INVALID_PARAMETER, e.what());
+    }
+}
+
+Engine* as_engine(void* p) { return static_cast<Engine*>(p); }
+
+}  // namespace
+
+extern "C" {
+
+int32_t dtb_abi_version(void) { return DTB_ABI_VERSION; }
+
+int32_t dtb_engine_version(void) { return 1 * 1000 + 0 * 100 + 0; }
+
+const char* dtb_status_string(int32_t s) {
+    switch (s) {
+        case DTB_OK: return "SNN_OK";
+        case DTB_INVALID_PARAMETER: return "SNN_INVALID_PARAMETER";
+        case DTB_UNSET_SAMPLE_FAILURE: return "SNN_UNSET_SAMPLE_FAILURE";
+        case DTB_UNSUPPORTED: return "SNN_UNSUPPORTED";
+        case DTB_NOT_ENABLE_METRIC: return "SNN_NOT_ENABLE_METRIC";
+        case DTB_INVALID_NETWORK: return "SNN_INVALID_NETWORK";
+        case DTB_OUT_OF_MEMORY: return "DTB_OUT_OF_MEMORY";
+        case DTB_CUDA_ERROR: return "DTB_CUDA_ERROR";
+        case DTB_DEVICE_FAULT: return "DTB_DEVICE_FAULT";
+        case DTB_IO_ERROR: return "DTB_IO_ERROR";
+        case DTB_NO_DEVICE: return "DTB_NO_DEVICE";
+        default: return "DTB_UNKNOWN_STATUS";
+    }
+}
+
+const char* dtb_last_error(void) { return dtb::last_error(); }
+
+void dtb_default_options(dtb_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->dt = 0.1f;
+    o->weight_type = DTB_W_F32;
+    o->seed = 0;
+    o->build_push = 1;
+    o->build_pull = 0;
+    o->ou_mean = 0.6f;
+    o->ou_sigma = 0.2f;
+    o->ou_tau = 10.0f;
+}
+
+int32_t dtb_create(const dtb_network_arrays* net, const dtb_options* opt, void** engine) {
+    if (!net || !opt || !engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
+    *engine = nullptr;
+    return guarded([&]() -> int {
+        auto* e = new Engine();
+        const int s = e->create_from_arrays(*net, *opt);
+        if (s != DTB_OK) { delete e; return s; }
+        *engine = e;
+        return DTB_OK;
+    });
+}
+
+int32_t dtb_create_structured(const dtb_structured_spec* spec, const dtb_options* opt, void** engine) {
+    if (!spec || !opt || !engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
+    *engine = nullptr;
+    return guarded([&]() -> int {
+        auto* e = new Engine();
+        const int s = e->create_structured(*spec, *opt);
+        if (s != DTB_OK) { delete e; return s; }
+        *engine = e;
+        return DTB_OK;
+    });
+}
+
+int32_t dtb_create_from_npz(const char* path, const dtb_options* opt, void** engine) {
+    if (!path || !opt || !engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
+    if (!*path) return dtb::fail(DTB_INVALID_PARAMETER, "empty file path");
+    *engine = nullptr;
+    return guarded([&]() -> int {
+        auto* e = new Engine();
+        const int s = e->create_from_npz(path, *opt);
+        if (s != DTB_OK) { delete e; return s; }
+        *engine = e;
+        return DTB_OK;
+    });
+}
+
+int32_t dtb_destroy(void* engine) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    delete as_engine(engine);
+    return DTB_OK;
+}
+
+int32_t dtb_info(void* engine, dtb_engine_info* info) {
+    if (!engine || !info) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
+    return as_engine(engine)->info(*info);
+}
+
+int32_t dtb_populations(void* engine, uint32_t* ids, uint32_t* counts) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    return as_engine(engine)->populations(ids, counts);
+}
+
+int32_t dtb_update_props(void* engine, uint32_t n, const uint32_t* nid, const uint32_t* pid, const float* val) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    return guarded([&] { return as_engine(engine)->update_props(n, nid, pid, val); });
+}
+
+int32_t dtb_update_prop_cols(void* engine, uint32_t n, const uint32_t* pid, const uint32_t* pop, const float* val, int32_t assign) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    return guarded([&] { return as_engine(engine)->update_prop_cols(n, pid, pop, val, assign); });
+}
+
+int32_t dtb_update_gamma(void* engine, uint32_t n, const uint32_t* pid, const uint32_t* pop, const float* alpha, const float* beta) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    return guarded([&] { return as_engine(engine)->update_gamma(n, pid, pop, alpha, beta); });
+}
+
+int32_t dtb_set_ou(void* engine, uint32_t n, const uint32_t* pop, const float* mean, const float* sigma, const float* tau) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    return guarded([&] { return as_engine(engine)->set_ou(n, pop, mean, sigma, tau); });
+}
+
+int32_t dtb_set_noise(void* engine, uint32_t source, uint32_t steps, const float* z, const float* u) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    return guarded([&] { return as_engine(engine)->set_noise(source, steps, z, u); });
+}
+
+int32_t dtb_run(void* engine, const dtb_run_request* req, dtb_run_output* out) {
+    if (!engine || !req || !out) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
+    return guarded([&] { return as_engine(engine)->run(*req, *out); });
+}
+
+int32_t dtb_read_state(void* engine, int32_t which, void* dst) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    return as_engine(engine)->read_state(which, dst);
+}
+
+int32_t dtb_write_state(void* engine, int32_t which, const void* src) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    return as_engine(engine)->write_state(which, src);
+}
+
+int32_t dtb_read_out_csr(void* engine, uint32_t* n_rows, uint64_t* n_edges, uint32_t* rows, uint64_t* row_ptr,
+                         uint32_t* post, uint8_t* kind, float* weight) {
+    if (!engine || !n_rows || !n_edges) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
+    return guarded([&] { return as_engine(engine)->read_out_csr(n_rows, n_edges, rows, row_ptr, post, kind, weight); });
+}
+
+int32_t dtb_build_out_csr_host(uint32_t n_neurons, uint64_t n_edges, const uint32_t* pre, const uint32_t* post,
+                               const uint8_t* kind, uint32_t* n_rows, uint32_t* rows, uint64_t* row_ptr,
+                               uint32_t* post_out, uint8_t* kind_out, uint64_t* perm) {
+    if (!n_rows || (n_edges && (!pre || !post || !kind))) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
+    return guarded([&]() -> int {
+        for (uint64_t e = 0; e < n_edges; ++e)
+            if (pre[e] >= n_neurons || post[e] >= n_neurons) return dtb::fail(DTB_INVALID_NETWORK, "edge index out of range");
+        std::vector<uint64_t> ptr, p;
+        dtb::counting_sort(pre, n_edges, n_neurons, ptr, p);
+        uint32_t nr = 0;
+        for (uint32_t j = 0; j < n_neurons; ++j) {
+            if (ptr[j + 1] > ptr[j]) {
+                if (rows) rows[nr] = j;
+                if (row_ptr) row_ptr[nr] = ptr[j];
+                ++nr;
+            }
+        }
+        if (row_ptr) row_ptr[nr] = n_edges;
+        *n_rows = nr;
+        for (uint64_t q = 0; q < n_edges; ++q) {
+            if (post_out) post_out[q] = post[p[q]];
+            if (kind_out) kind_out[q] = kind[p[q]] != 0 ? 1 : 0;
+            if (perm) perm[q] = p[q];
+        }
+        return DTB_OK;
+    });
+}
+
+int32_t dtb_state_size(void* engine, uint64_t* bytes) {
+    if (!engine || !bytes) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
+    *bytes = as_engine(engine)->state_size();
+    return DTB_OK;
+}
+
+int32_t dtb_save_state(void* engine, void* blob, uint64_t bytes) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    return as_engine(engine)->save_state(blob, bytes);
+}
+
+int32_t dtb_load_state(void* engine, const void* blob, uint64_t bytes) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    return as_engine(engine)->load_state(blob, bytes);
+}
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+// The engine object behind the C-ABI: one network resident in one GPU's HBM.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "dtb_b200.h"
+#include "dtb_device.cuh"
+#include "dtb_host.h"
+#include "dtb_kernels.h"
+
+namespace dtb {
+
+void set_error(const std::string& msg);
+int fail(int status, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define DTB_CU(x) do { cudaError_t e__ = (x); if (e__ != cudaSuccess) return ::dtb::cuda_fail(e__, #x); } while (0)
+#define DTB_TRY(x) do { int s__ = (x); if (s__ != DTB_OK) return s__; } while (0)
+
+class Engine {
+public:
+    ~Engine();
+
+    int init_common(const dtb_options& opt, uint32_t n);
+    int create_from_arrays(const dtb_network_arrays& a, const dtb_options& opt);
+    int create_structured(const dtb_structured_spec& s, const dtb_options& opt);
+    int create_from_npz(const std::string& path, const dtb_options& opt);
+
+    int run(const dtb_run_request& rq, dtb_run_output& out);
+    int info(dtb_engine_info& info) const;
+    int populations(uint32_t* ids, uint32_t* counts) const;
+    int update_props(uint32_t n, const uint32_t* nid, const uint32_t* pid, const float* val);
+    int update_prop_cols(uint32_t n, const uint32_t* pid, const uint32_t* pop, const float* val, int assign);
+    int update_gamma(uint32_t n, const uint32_t* pid, const uint32_t* pop, const float* alpha, const float* beta);
+    int set_ou(uint32_t n, const uint32_t* pop, const float* mean, const float* sigma, const float* tau);
+    int set_noise(uint32_t source, uint32_t steps, const float* z, const float* u);
+    int read_state(int which, void* dst);
+    int write_state(int which, const void* src);
+    int read_out_csr(uint32_t* n_rows, uint64_t* n_edges, uint32_t* rows, uint64_t* row_ptr, uint32_t* post,
+                     uint8_t* kind, float* weight);
+    uint64_t state_size() const;
+    int save_state(void* blob, uint64_t bytes);
+    int load_state(const void* blob, uint64_t bytes);
+
+    // ---- pieces shared with the batch / serving layers
+    LaunchBatch single_batch() const;
+    int refresh_view();
+    int ensure_dj();
+    int ensure_hist(uint32_t rows, bool record);
+    int begin_run_chunk(uint64_t run_base, uint32_t rows, bool stats);
+    int finish_hist(uint32_t rows, uint32_t out_row0, const dtb_run_output& out, bool freq, bool vmean, bool record);
+
+    // identity
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float dt = 0.1f;
+    uint32_t wtype = W_F32;
+    uint64_t seed = 0;
+    uint32_t n = 0, n_pad = 0, n_words = 0, P = 0;
+    uint64_t n_edges = 0;
+    bool has_push = false, has_pull = false;
+    int sm_count = 148;
+
+    // populations and parameters (host copies)
+    std::vector<uint32_t> pop_ids, pop_off, excl_count;
+    std::vector<RawParams> pop_raw;
+    std::vector<RawParams> neuron_raw;  // only in per-neuron mode
+    bool per_neuron = false;
+    std::vector<uint8_t> ou_set;
+    uint64_t gamma_calls = 0;
+
+    // host mirror of the clock
+    uint64_t steps = 0;
+    float t = 0.0f;
+    int noise_src = DTB_NOISE_PHILOX;
+    uint64_t inj_rows = 0, inj_first = 0;
+
+    // device memory
+    std::vector<void*> allocs;
+    uint64_t dev_bytes = 0;
+    float* V = nullptr;
+    float* iou = nullptr;
+    float* tlast = nullptr;
+    float4* J = nullptr;
+    long long* dJ = nullptr;
+    PopParams* pop_dev = nullptr;
+    uint32_t* pop_off_dev = nullptr;
+    float* np_dev = nullptr;
+    unsigned long long* out_ptr = nullptr;
+    uint32_t* out_col = nullptr;
+    void* out_w = nullptr;
+    unsigned long long* in_ptr = nullptr;
+    uint32_t* in_col = nullptr;
+    void* in_w = nullptr;
+    uint32_t* out_deg = nullptr;
+    uint32_t* bits0 = nullptr;
+    uint32_t* bits1 = nullptr;
+    uint32_t* excl = nullptr;
+    Clock* clock = nullptr;
+    unsigned long long* events = nullptr;
+    uint32_t* ticket = nullptr;
+    int* hist_cnt = nullptr;
+    long long* hist_vsum = nullptr;
+    uint32_t* rec_bits = nullptr;
+    uint32_t hist_cap = 0, rec_cap = 0;
+    float* inj_z = nullptr;
+    float* inj_u = nullptr;
+    NetView* view_dev = nullptr;
+    uint32_t* prefix_dev = nullptr;   // [lif 2][pull 2][vbase 2]
+    uint32_t* list = nullptr;
+    uint32_t* list_count = nullptr;
+    uint32_t* list_ticket = nullptr;
+    NetView view{};
+
+    // pinned staging for the statistics
+    int* h_cnt = nullptr;
+    long long* h_vsum = nullptr;
+    size_t h_cap = 0;
+
+    template <class T> int dalloc(T*& p, size_t count, bool zero = true) {
+        void* q = nullptr;
+        const size_t bytes = count * sizeof(T) > 0 ? count * sizeof(T) : 16;
+        DTB_CU(cudaMalloc(&q, bytes));
+        allocs.push_back(q);
+        dev_bytes += bytes;
+        if (zero) DTB_CU(cudaMemsetAsync(q, 0, bytes, stream));
+        p = static_cast<T*>(q);
+        return DTB_OK;
+    }
+    void dfree(void* p);
+
+private:
+    int setup_populations_from_property(const float* prop);
+    int upload_params();
+    int init_state();
+    int upload_csr_host(const uint32_t* pre, const uint32_t* post, const uint8_t* kind_in, const void* w, uint32_t in_type,
+                        bool build_push, bool build_pull);
+    int weight_bytes() const;
+};
+
+}  // namespace dtb

@@ -1,0 +1,735 @@
+// Per-step kernels of the engine.
+//
+//   lif_kernel<JM>        fused OU + LIF + threshold + receptor decay + spike
+//                         compaction + per-population statistics, 4 neurons/thread
+//                         with 128-bit loads (replaces the reference's OU, membrane,
+//                         spike, compaction, J-decay, synaptic-current and stat kernels:
+//                         src/stage/extern_stimuli.cpp:39-112, membrane_voltage.cpp:114-235,
+//                         spike.cpp:42-68, 244-762, presynaptic_voltage.cpp:46-120,
+//                         synaptic_current.cpp:7-71, stat_result.cpp:161-327)
+//   push_kernel<ACC,WT>   out-degree CSR propagation of the compacted spikes: one warp per
+//                         spiking row, 4 synapses in flight per lane, one vector reduction
+//                         (or two 64-bit fixed-point atomics) per synapse
+//                         (src/stage/presynaptic_voltage.cpp:122-225)
+//   lif_pull_kernel<G,WT> deterministic in-degree gather fused into the LIF step: one warp
+//                         gathers 32 neurons, then each lane steps one neuron
+//   fold_finish_kernel / gather_finish_kernel: bring J back to "complete" at the end of a run
+//
+// A launch covers a batch of networks (one for the plain path).  CTA -> network is
+// a binary search over the batch's tile prefix; every network keeps its own clock,
+// and the last CTA of a network to finish (ticket counter) advances that clock.
+#include "dtb_device.cuh"
+#include "dtb_kernels.h"
+
+namespace dtb {
+
+constexpr int kStatSlots = 32;
+constexpr int kPushThreads = 256;
+
+__device__ inline uint32_t find_net(const uint32_t* __restrict__ prefix, uint32_t n_nets, uint32_t x) {
+    uint32_t lo = 0, hi = n_nets - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= x) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ inline void load_netview(NetView& dst, const NetView* __restrict__ src) {
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+    uint32_t* d = reinterpret_cast<uint32_t*>(&dst);
+    for (int w = threadIdx.x; w < static_cast<int>(sizeof(NetView) / 4); w += blockDim.x) d[w] = s[w];
+}
+
+// 4-bit nibble of lane l covers neurons 4l..4l+3 of the warp's 128; gather the
+// 32-bit word of neurons 32w..32w+31 (lanes 8w..8w+7) into every lane of the group.
+__device__ inline uint32_t nibbles_to_word(uint32_t nib, int lane) {
+    uint32_t x = nib << (4 * (lane & 7));
+    x |= __shfl_xor_sync(0xffffffffu, x, 1);
+    x |= __shfl_xor_sync(0xffffffffu, x, 2);
+    x |= __shfl_xor_sync(0xffffffffu, x, 4);
+    return x;
+}
+
+__device__ inline long long warp_sum_ll(long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ inline unsigned long long warp_sum_ull(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Normal draws (OU) and uniforms (noise train) for 4 consecutive neurons.
+__device__ inline void draw_noise(const NetView& nv, uint32_t i0, unsigned long long n, unsigned long long inj_base,
+                                  bool injected, bool need_u, float z[4], float u[4], uint32_t& err) {
+    if (injected) {
+        const unsigned long long row = n - inj_base - 1;
+        if (row < nv.inj_rows && nv.inj_z != nullptr) {
+            const float4 zz = __ldcs(reinterpret_cast<const float4*>(nv.inj_z + row * nv.n_pad + i0));
+            z[0] = zz.x; z[1] = zz.y; z[2] = zz.z; z[3] = zz.w;
+            if (need_u) {
+                if (nv.inj_u != nullptr) {
+                    const float4 uu = __ldcs(reinterpret_cast<const float4*>(nv.inj_u + row * nv.n_pad + i0));
+                    u[0] = uu.x; u[1] = uu.y; u[2] = uu.z; u[3] = uu.w;
+                } else {
+                    u[0] = u[1] = u[2] = u[3] = 1.0f;
+                    err |= kErrNoiseExhausted;
+                }
+            }
+        } else {
+            z[0] = z[1] = z[2] = z[3] = 0.0f;
+            u[0] = u[1] = u[2] = u[3] = 1.0f;
+            err |= kErrNoiseExhausted;
+        }
+    } else {
+        const uint32_t k0 = static_cast<uint32_t>(nv.seed), k1 = static_cast<uint32_t>(nv.seed >> 32);
+        const U4 r = philox4x32_10(U4{i0 >> 2, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamOU}, k0, k1);
+        box_muller(r.x, r.y, z[0], z[1]);
+        box_muller(r.z, r.w, z[2], z[3]);
+        if (need_u) {
+            const U4 q = philox4x32_10(U4{i0 >> 2, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamNoise}, k0, k1);
+            u[0] = u01(q.x); u[1] = u01(q.y); u[2] = u01(q.z); u[3] = u01(q.w);
+        }
+    }
+}
+
+__device__ inline void draw_noise1(const NetView& nv, uint32_t i, unsigned long long n, unsigned long long inj_base,
+                                   bool injected, bool need_u, float& z, float& u, uint32_t& err) {
+    // one neuron: same streams as draw_noise (the neuron's slot of its quad)
+    if (injected) {
+        const unsigned long long row = n - inj_base - 1;
+        if (row < nv.inj_rows && nv.inj_z != nullptr) {
+            z = __ldcs(nv.inj_z + row * nv.n_pad + i);
+            if (need_u) {
+                if (nv.inj_u != nullptr) u = __ldcs(nv.inj_u + row * nv.n_pad + i);
+                else { u = 1.0f; err |= kErrNoiseExhausted; }
+            }
+        } else {
+            z = 0.0f; u = 1.0f; err |= kErrNoiseExhausted;
+        }
+    } else {
+        const uint32_t k0 = static_cast<uint32_t>(nv.seed), k1 = static_cast<uint32_t>(nv.seed >> 32);
+        const U4 r = philox4x32_10(U4{i >> 2, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamOU}, k0, k1);
+        float z4[4];
+        box_muller(r.x, r.y, z4[0], z4[1]);
+        box_muller(r.z, r.w, z4[2], z4[3]);
+        z = z4[i & 3];
+        if (need_u) {
+            const U4 q = philox4x32_10(U4{i >> 2, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamNoise}, k0, k1);
+            const uint32_t qq[4] = {q.x, q.y, q.z, q.w};
+            u = u01(qq[i & 3]);
+        }
+    }
+}
+
+__device__ inline bool propagated(int prop_mode, bool active, float u, float rate) {
+    if (prop_mode == PROP_THRESHOLD) return active;
+    const bool noise = u < rate;
+    return prop_mode == PROP_NOISE ? noise : (noise || active);
+}
+
+__device__ inline bool excluded(const NetView& nv, uint32_t i) {
+    return nv.stat_excl != nullptr && ((__ldg(nv.stat_excl + (i >> 5)) >> (i & 31)) & 1u);
+}
+
+// Shared per-CTA statistics accumulator: population slots relative to the
+// CTA's first population; populations beyond the window go straight to global.
+struct StatAcc {
+    int* cnt;
+    long long* vs;
+    uint32_t p0;
+};
+
+__device__ inline void stat_add(const NetView& nv, const StatAcc& sa, long long row, uint32_t p, int c, long long v) {
+    const uint32_t slot = p - sa.p0;
+    if (slot < static_cast<uint32_t>(kStatSlots)) {
+        if (c) atomicAdd(sa.cnt + slot, c);
+        atomicAdd(reinterpret_cast<unsigned long long*>(sa.vs + slot), static_cast<unsigned long long>(v));
+    } else {
+        const size_t o = static_cast<size_t>(row) * nv.n_pops + p;
+        if (c) atomicAdd(nv.hist_cnt + o, c);
+        atomicAdd(reinterpret_cast<unsigned long long*>(nv.hist_vsum + o), static_cast<unsigned long long>(v));
+    }
+}
+
+__device__ inline long long v_fix(float v) {
+    return __float2ll_rn(__fmul_rn(v, static_cast<float>(kVsumScale)));
+}
+
+__device__ inline void advance_clock(const NetView& nv, uint32_t tiles, float t, unsigned long long n, uint32_t err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (err) atomicOr(&nv.clock->err, err);
+        __threadfence();
+        const uint32_t k = atomicAdd(nv.ticket, 1u);
+        if (k == tiles - 1) {
+            nv.clock->t = t;
+            nv.clock->n = n;
+            *nv.ticket = 0u;
+            __threadfence();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused LIF step (push and exact-push modes)
+// ---------------------------------------------------------------------------
+template <int JM>
+__global__ void __launch_bounds__(kLifThreads)
+lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_prefix,
+           const uint32_t* __restrict__ vbase, uint32_t n_nets, SpikeList sl, uint32_t flags, int prop_mode) {
+    __shared__ NetView s_nv;
+    __shared__ uint32_t s_net, s_tile, s_p0, s_base;
+    __shared__ uint32_t s_warp[kLifThreads / 32];
+    __shared__ unsigned long long s_events;
+    __shared__ int s_cnt[kStatSlots];
+    __shared__ long long s_vs[kStatSlots];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        const uint32_t k = n_nets > 1 ? find_net(tile_prefix, n_nets, blockIdx.x) : 0u;
+        s_net = k;
+        s_tile = blockIdx.x - __ldg(tile_prefix + k);
+        s_events = 0ull;
+    }
+    if (tid < kStatSlots) { s_cnt[tid] = 0; s_vs[tid] = 0; }
+    __syncthreads();
+    load_netview(s_nv, nets + s_net);
+    __syncthreads();
+    const NetView& nv = s_nv;
+
+    const float t_prev = nv.clock->t;
+    const unsigned long long n_prev = nv.clock->n;
+    const unsigned long long run_base = nv.clock->run_base;
+    const unsigned long long inj_base = nv.clock->inj_base;
+    const unsigned long long n = n_prev + 1;
+    const float t = __fadd_rn(t_prev, nv.dt);
+    const uint32_t parity = static_cast<uint32_t>(n & 1ull);
+    const uint32_t tile_first = s_tile * kLifTile;
+    const uint32_t i0 = tile_first + tid * 4;
+    uint32_t err = 0;
+
+    const long long row = static_cast<long long>(n - run_base - 1);
+    bool stats = (flags & kFlagStats) != 0;
+    bool record = (flags & kFlagRecord) != 0 && nv.rec_bits != nullptr;
+    if ((stats || record) && (row < 0 || row >= static_cast<long long>(nv.hist_cap))) {
+        stats = false; record = false; err |= kErrHistOverflow;
+    }
+    if (tid == 0) s_p0 = find_pop(nv.pop_off, nv.n_pops, min(tile_first, nv.n - 1));
+    __syncthreads();
+    StatAcc sa{s_cnt, s_vs, s_p0};
+
+    // ---- state loads: 128-bit per array, 4 neurons per thread
+    float4 V4 = *reinterpret_cast<const float4*>(nv.V + i0);
+    float4 I4 = *reinterpret_cast<const float4*>(nv.iou + i0);
+    float4 T4 = *reinterpret_cast<const float4*>(nv.tlast + i0);
+    float4 J4[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) J4[k] = nv.J[i0 + k];
+    longlong2 D[8];
+    if constexpr (JM == J_FOLD) {
+        const longlong2* dsrc = reinterpret_cast<const longlong2*>(nv.dJ + static_cast<size_t>(i0) * 4);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) D[k] = dsrc[k];
+    }
+    const bool use_ou = (flags & kFlagUseOU) != 0;
+    const bool need_u = prop_mode != PROP_THRESHOLD;
+    float z[4], u[4] = {1.f, 1.f, 1.f, 1.f};
+    draw_noise(nv, i0, n, inj_base, (flags & kFlagInjected) != 0, need_u, z, u, err);
+
+    float* Vv = reinterpret_cast<float*>(&V4);
+    float* Iv = reinterpret_cast<float*>(&I4);
+    float* Tv = reinterpret_cast<float*>(&T4);
+    uint32_t nib_prop = 0, nib_act = 0;
+    unsigned long long ev = 0;
+
+    uint32_t p = find_pop(nv.pop_off, nv.n_pops, min(i0, nv.n - 1));
+    uint32_t p_first = p;
+    bool uniform = true;
+    int cnt_acc = 0;
+    long long vs_acc = 0;
+    PopParams pp;
+    load_pop_params(nv, p, i0, pp);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t i = i0 + k;
+        if (i >= nv.n) { uniform = false; continue; }
+        if (!nv.per_neuron) {
+            if (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) {
+                while (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) ++p;
+                load_pop_params(nv, p, i, pp);
+                uniform = false;
+            }
+        } else {
+            if (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) {
+                while (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) ++p;
+                uniform = false;
+            }
+            if (k > 0) load_pop_params(nv, p, i, pp);
+        }
+        float* Jk = reinterpret_cast<float*>(&J4[k]);
+        NeuronIn in;
+        in.V = Vv[k];
+        in.iou = Iv[k];
+        in.tlast = Tv[k];
+        if constexpr (JM == J_FOLD) {
+            const long long* dk = reinterpret_cast<const long long*>(&D[2 * k]);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) in.J[c] = decay_add(Jk[c], pp.decay[c], fix_to_float(dk[c]));
+        } else {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) in.J[c] = Jk[c];
+        }
+        const NeuronOut o = lif_update(pp, in, t, z[k], use_ou);
+        Vv[k] = o.V;
+        Iv[k] = o.iou;
+        Tv[k] = o.tlast;
+        if constexpr (JM == J_DIRECT) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) Jk[c] = __fmul_rn(in.J[c], pp.decay[c]);
+        } else if constexpr (JM == J_FOLD) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) Jk[c] = in.J[c];
+        }
+        const bool sp = propagated(prop_mode, o.active, u[k], pp.noise_rate);
+        nib_prop |= static_cast<uint32_t>(sp) << k;
+        nib_act |= static_cast<uint32_t>(o.active) << k;
+        if (sp) ev += __ldg(nv.out_deg + i);
+        if (stats) {
+            if (excluded(nv, i)) { uniform = false; continue; }
+            if (p == p_first) {
+                cnt_acc += o.active;
+                vs_acc += v_fix(o.V);
+            } else {
+                stat_add(nv, sa, row, p, o.active, v_fix(o.V));
+            }
+        }
+    }
+
+    // ---- state stores
+    *reinterpret_cast<float4*>(nv.V + i0) = V4;
+    *reinterpret_cast<float4*>(nv.iou + i0) = I4;
+    *reinterpret_cast<float4*>(nv.tlast + i0) = T4;
+    if constexpr (JM != J_ASIS) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) nv.J[i0 + k] = J4[k];
+    }
+    if constexpr (JM == J_FOLD) {
+        longlong2* ddst = reinterpret_cast<longlong2*>(nv.dJ + static_cast<size_t>(i0) * 4);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) ddst[k] = make_longlong2(0, 0);
+    }
+
+    // ---- spike bitmaps (propagated: parity buffer; threshold: history row)
+    {
+        const uint32_t wprop = nibbles_to_word(nib_prop, lane);
+        const uint32_t wact = nibbles_to_word(nib_act, lane);
+        if ((lane & 7) == 0) {
+            const uint32_t word = (i0 >> 5);   // lane 8w holds neurons 32w.. of this warp
+            uint32_t* bits = parity ? nv.bits1 : nv.bits0;
+            bits[word] = wprop;
+            if (record) nv.rec_bits[static_cast<size_t>(row) * nv.n_words + word] = wact;
+        }
+    }
+
+    // ---- population statistics: warp-uniform fast path, else per-thread slots
+    if (stats) {
+        const uint32_t pl = __shfl_sync(0xffffffffu, p_first, 0);
+        const bool wuni = __all_sync(0xffffffffu, uniform && p_first == pl);
+        if (wuni) {
+            const int c = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(cnt_acc));
+            const long long v = warp_sum_ll(vs_acc);
+            if (lane == 0) stat_add(nv, sa, row, pl, c, v);
+        } else if (i0 < nv.n) {
+            stat_add(nv, sa, row, p_first, cnt_acc, vs_acc);
+        }
+    }
+
+    // ---- spike list (push modes): CTA-aggregated, ascending within the CTA
+    const uint32_t my_cnt = __popc(nib_prop);
+    uint32_t incl = my_cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    const unsigned long long wev = warp_sum_ull(ev);
+    if (lane == 0 && wev) atomicAdd(&s_events, wev);
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t total = 0;
+#pragma unroll
+        for (int w = 0; w < kLifThreads / 32; ++w) { const uint32_t c = s_warp[w]; s_warp[w] = total; total += c; }
+        s_base = ((flags & kFlagList) && total) ? atomicAdd(sl.count, total) : 0u;
+        if (s_events) atomicAdd(nv.events, s_events);
+    }
+    __syncthreads();
+    if ((flags & kFlagList) && my_cnt) {
+        uint32_t pos = s_base + s_warp[warp] + incl - my_cnt;
+        const uint32_t vb = __ldg(vbase + s_net);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if ((nib_prop >> k) & 1u) sl.list[pos++] = vb + i0 + k;
+    }
+    if (stats && tid < kStatSlots) {
+        const int c = s_cnt[tid];
+        const long long v = s_vs[tid];
+        if (c || v) {
+            const size_t o = static_cast<size_t>(row) * nv.n_pops + (s_p0 + tid);
+            if (c) atomicAdd(nv.hist_cnt + o, c);
+            atomicAdd(reinterpret_cast<unsigned long long*>(nv.hist_vsum + o), static_cast<unsigned long long>(v));
+        }
+    }
+    advance_clock(nv, nv.lif_tiles, t, n, err);
+}
+
+// ---------------------------------------------------------------------------
+// Push propagation: one warp per spiking row of the out-degree CSR
+// ---------------------------------------------------------------------------
+template <int ACC, int WT>
+__global__ void __launch_bounds__(kPushThreads)
+push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase, uint32_t n_nets, SpikeList sl) {
+    const uint32_t count = *sl.count;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const unsigned long long* ptr = nets[0].out_ptr;
+    const uint32_t* col = nets[0].out_col;
+    const void* wts = nets[0].out_w;
+    float4* J = nets[0].J;
+    long long* dJ = nets[0].dJ;
+    uint32_t vb = 0;
+    for (uint32_t r = gw; r < count; r += nw) {
+        const uint32_t v = __ldg(sl.list + r);
+        if (n_nets > 1) {
+            const uint32_t k = find_net(vbase, n_nets, v);
+            vb = __ldg(vbase + k);
+            ptr = nets[k].out_ptr;
+            col = nets[k].out_col;
+            wts = nets[k].out_w;
+            J = nets[k].J;
+            dJ = nets[k].dJ;
+        }
+        const uint32_t j = v - vb;
+        const unsigned long long beg = __ldg(ptr + j), end = __ldg(ptr + j + 1);
+        for (unsigned long long e = beg + lane; e < end; e += 128) {
+            uint32_t c[4];
+            float2 w[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const unsigned long long idx = e + 32ull * q;
+                if (idx < end) {
+                    c[q] = __ldcs(col + idx);
+                    w[q] = load_weight<WT>(wts, idx);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const unsigned long long idx = e + 32ull * q;
+                if (idx < end) {
+                    const uint32_t target = c[q] & kIndexMask;
+                    const uint32_t kind = c[q] >> 31;
+                    if constexpr (ACC == 0) {
+                        atomicAdd(reinterpret_cast<float2*>(J + target) + kind, w[q]);
+                    } else {
+                        unsigned long long* d = reinterpret_cast<unsigned long long*>(dJ) + static_cast<size_t>(target) * 4 + 2 * kind;
+                        atomicAdd(d, static_cast<unsigned long long>(float_to_fix(w[q].x)));
+                        atomicAdd(d + 1, static_cast<unsigned long long>(float_to_fix(w[q].y)));
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(sl.ticket, 1u) == gridDim.x - 1) {
+            *sl.count = 0u;
+            *sl.ticket = 0u;
+            __threadfence();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic in-degree gather of 32 neurons by one warp: lane k returns the
+// exact fixed-point input of neuron base + k (sum over in-edges whose source
+// spiked in `prev_bits`).
+// ---------------------------------------------------------------------------
+template <int WT>
+__device__ inline void gather32(const NetView& nv, uint32_t base, const uint32_t* __restrict__ prev_bits,
+                                int lane, long long acc_out[4]) {
+    acc_out[0] = acc_out[1] = acc_out[2] = acc_out[3] = 0;
+    const uint32_t last = min(base + 32u, nv.n);
+    for (uint32_t j = base; j < last; ++j) {
+        const unsigned long long beg = __ldg(nv.in_ptr + j), end = __ldg(nv.in_ptr + j + 1);
+        long long a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        for (unsigned long long e = beg + lane; e < end; e += 128) {
+            uint32_t c[4];
+            uint32_t hit = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const unsigned long long idx = e + 32ull * q;
+                c[q] = idx < end ? __ldcs(nv.in_col + idx) : 0u;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const unsigned long long idx = e + 32ull * q;
+                if (idx < end) {
+                    const uint32_t src = c[q] & kIndexMask;
+                    hit |= ((__ldg(prev_bits + (src >> 5)) >> (src & 31u)) & 1u) << q;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if ((hit >> q) & 1u) {
+                    const float2 w = load_weight<WT>(nv.in_w, e + 32ull * q);
+                    const long long f0 = float_to_fix(w.x), f1 = float_to_fix(w.y);
+                    if (c[q] >> 31) { a2 += f0; a3 += f1; } else { a0 += f0; a1 += f1; }
+                }
+            }
+        }
+        a0 = warp_sum_ll(a0);
+        a1 = warp_sum_ll(a1);
+        a2 = warp_sum_ll(a2);
+        a3 = warp_sum_ll(a3);
+        if (static_cast<uint32_t>(lane) == j - base) {
+            acc_out[0] = a0; acc_out[1] = a1; acc_out[2] = a2; acc_out[3] = a3;
+        }
+    }
+}
+
+// Pull-fused LIF step: GATHER=1 folds last step's spikes into J first; GATHER=0
+// (first step of a run) takes J as complete.
+template <int GATHER, int WT>
+__global__ void __launch_bounds__(kPullThreads)
+lif_pull_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_prefix, uint32_t n_nets,
+                uint32_t flags, int prop_mode) {
+    __shared__ NetView s_nv;
+    __shared__ uint32_t s_net, s_tile, s_p0;
+    __shared__ unsigned long long s_events;
+    __shared__ int s_cnt[kStatSlots];
+    __shared__ long long s_vs[kStatSlots];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        const uint32_t k = n_nets > 1 ? find_net(tile_prefix, n_nets, blockIdx.x) : 0u;
+        s_net = k;
+        s_tile = blockIdx.x - __ldg(tile_prefix + k);
+        s_events = 0ull;
+    }
+    if (tid < kStatSlots) { s_cnt[tid] = 0; s_vs[tid] = 0; }
+    __syncthreads();
+    load_netview(s_nv, nets + s_net);
+    __syncthreads();
+    const NetView& nv = s_nv;
+    const float t_prev = nv.clock->t;
+    const unsigned long long n_prev = nv.clock->n;
+    const unsigned long long run_base = nv.clock->run_base;
+    const unsigned long long inj_base = nv.clock->inj_base;
+    const unsigned long long n = n_prev + 1;
+    const float t = __fadd_rn(t_prev, nv.dt);
+    const uint32_t parity = static_cast<uint32_t>(n & 1ull);
+    const uint32_t tile_first = s_tile * kPullTile;
+    const uint32_t base = tile_first + warp * 32;
+    const uint32_t i = base + lane;
+    uint32_t err = 0;
+    const long long row = static_cast<long long>(n - run_base - 1);
+    bool stats = (flags & kFlagStats) != 0;
+    bool record = (flags & kFlagRecord) != 0 && nv.rec_bits != nullptr;
+    if ((stats || record) && (row < 0 || row >= static_cast<long long>(nv.hist_cap))) {
+        stats = false; record = false; err |= kErrHistOverflow;
+    }
+    if (tid == 0) s_p0 = find_pop(nv.pop_off, nv.n_pops, min(tile_first, nv.n - 1));
+    __syncthreads();
+    StatAcc sa{s_cnt, s_vs, s_p0};
+
+    long long acc[4] = {0, 0, 0, 0};
+    if constexpr (GATHER) {
+        const uint32_t* prev = parity ? nv.bits0 : nv.bits1;
+        gather32<WT>(nv, base, prev, lane, acc);
+    }
+    const bool valid = i < nv.n;
+    bool active = false, sp = false;
+    float vnew = 0.f;
+    uint32_t p = 0;
+    if (valid) {
+        p = find_pop(nv.pop_off, nv.n_pops, i);
+        PopParams pp;
+        load_pop_params(nv, p, i, pp);
+        float4 Jv = nv.J[i];
+        float* Jc = reinterpret_cast<float*>(&Jv);
+        NeuronIn in;
+        in.V = nv.V[i];
+        in.iou = nv.iou[i];
+        in.tlast = nv.tlast[i];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) in.J[c] = GATHER ? decay_add(Jc[c], pp.decay[c], fix_to_float(acc[c])) : Jc[c];
+        float z, u = 1.f;
+        draw_noise1(nv, i, n, inj_base, (flags & kFlagInjected) != 0, prop_mode != PROP_THRESHOLD, z, u, err);
+        const NeuronOut o = lif_update(pp, in, t, z, (flags & kFlagUseOU) != 0);
+        nv.V[i] = o.V;
+        nv.iou[i] = o.iou;
+        nv.tlast[i] = o.tlast;
+        if constexpr (GATHER) nv.J[i] = make_float4(in.J[0], in.J[1], in.J[2], in.J[3]);
+        active = o.active;
+        vnew = o.V;
+        sp = propagated(prop_mode, o.active, u, pp.noise_rate);
+    }
+    const uint32_t wprop = __ballot_sync(0xffffffffu, sp);
+    const uint32_t wact = __ballot_sync(0xffffffffu, active);
+    if (lane == 0) {
+        uint32_t* bits = parity ? nv.bits1 : nv.bits0;
+        bits[base >> 5] = wprop;
+        if (record) nv.rec_bits[static_cast<size_t>(row) * nv.n_words + (base >> 5)] = wact;
+    }
+    const unsigned long long ev = warp_sum_ull(sp ? static_cast<unsigned long long>(__ldg(nv.out_deg + i)) : 0ull);
+    if (lane == 0 && ev) atomicAdd(&s_events, ev);
+    if (stats) {
+        const bool inc = valid && !excluded(nv, i);
+        const uint32_t pl = __shfl_sync(0xffffffffu, p, 0);
+        const bool wuni = __all_sync(0xffffffffu, !valid || (inc && p == pl)) && __any_sync(0xffffffffu, valid);
+        const int c = inc && active ? 1 : 0;
+        const long long v = inc ? v_fix(vnew) : 0;
+        if (wuni) {
+            const int cs = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(c));
+            const long long vs = warp_sum_ll(v);
+            if (lane == 0) stat_add(nv, sa, row, pl, cs, vs);
+        } else if (inc) {
+            stat_add(nv, sa, row, p, c, v);
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && s_events) atomicAdd(nv.events, s_events);
+    if (stats && tid < kStatSlots) {
+        const int c = s_cnt[tid];
+        const long long v = s_vs[tid];
+        if (c || v) {
+            const size_t o = static_cast<size_t>(row) * nv.n_pops + (s_p0 + tid);
+            if (c) atomicAdd(nv.hist_cnt + o, c);
+            atomicAdd(reinterpret_cast<unsigned long long*>(nv.hist_vsum + o), static_cast<unsigned long long>(v));
+        }
+    }
+    advance_clock(nv, nv.n_pad / kPullTile, t, n, err);
+}
+
+// End of an exact-push run: J <- J*decay + dJ, dJ <- 0 (J becomes complete).
+__global__ void __launch_bounds__(kLifThreads)
+fold_finish_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_prefix, uint32_t n_nets) {
+    const uint32_t k = n_nets > 1 ? find_net(tile_prefix, n_nets, blockIdx.x) : 0u;
+    const NetView& nv = nets[k];
+    const uint32_t tile = blockIdx.x - __ldg(tile_prefix + k);
+    const uint32_t i0 = tile * kLifTile + threadIdx.x * 4;
+    const uint32_t n = nv.n;
+    uint32_t p = find_pop(nv.pop_off, nv.n_pops, min(i0, n - 1));
+    for (int q = 0; q < 4; ++q) {
+        const uint32_t i = i0 + q;
+        if (i >= n) break;
+        while (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) ++p;
+        PopParams pp;
+        load_pop_params(nv, p, i, pp);
+        float4 Jv = nv.J[i];
+        float* Jc = reinterpret_cast<float*>(&Jv);
+        long long* d = nv.dJ + static_cast<size_t>(i) * 4;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) { Jc[c] = decay_add(Jc[c], pp.decay[c], fix_to_float(d[c])); d[c] = 0; }
+        nv.J[i] = Jv;
+    }
+}
+
+// End of a pull run: J <- J*decay + gather(last step's spikes).
+template <int WT>
+__global__ void __launch_bounds__(kPullThreads)
+gather_finish_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_prefix, uint32_t n_nets) {
+    const uint32_t k = n_nets > 1 ? find_net(tile_prefix, n_nets, blockIdx.x) : 0u;
+    const NetView& nv = nets[k];
+    const uint32_t tile = blockIdx.x - __ldg(tile_prefix + k);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t base = tile * kPullTile + warp * 32;
+    const unsigned long long n = nv.clock->n;
+    const uint32_t* last = (n & 1ull) ? nv.bits1 : nv.bits0;
+    long long acc[4];
+    gather32<WT>(nv, base, last, lane, acc);
+    const uint32_t i = base + lane;
+    if (i < nv.n) {
+        const uint32_t p = find_pop(nv.pop_off, nv.n_pops, i);
+        PopParams pp;
+        load_pop_params(nv, p, i, pp);
+        float4 Jv = nv.J[i];
+        float* Jc = reinterpret_cast<float*>(&Jv);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) Jc[c] = decay_add(Jc[c], pp.decay[c], fix_to_float(acc[c]));
+        nv.J[i] = Jv;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launchers
+// ---------------------------------------------------------------------------
+cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop_mode, cudaStream_t s) {
+    if (b.lif_tiles_total == 0) return cudaSuccess;
+    const dim3 grid(b.lif_tiles_total), block(kLifThreads);
+    switch (jmode) {
+        case J_DIRECT: lif_kernel<J_DIRECT><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, b.spikes, flags, prop_mode); break;
+        case J_FOLD: lif_kernel<J_FOLD><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, b.spikes, flags, prop_mode); break;
+        default: lif_kernel<J_ASIS><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, b.spikes, flags, prop_mode); break;
+    }
+    return cudaGetLastError();
+}
+
+template <int ACC>
+static void push_dispatch(const LaunchBatch& b, int wt, cudaStream_t s) {
+    const dim3 grid(b.push_ctas), block(kPushThreads);
+    switch (wt) {
+        case W_F32: push_kernel<ACC, W_F32><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
+        case W_BF16: push_kernel<ACC, W_BF16><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
+        case W_F16: push_kernel<ACC, W_F16><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
+        default: push_kernel<ACC, W_U8><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
+    }
+}
+
+cudaError_t launch_push(const LaunchBatch& b, int exact, int wt, cudaStream_t s) {
+    if (exact) push_dispatch<1>(b, wt, s); else push_dispatch<0>(b, wt, s);
+    return cudaGetLastError();
+}
+
+template <int G>
+static void pull_dispatch(const LaunchBatch& b, int wt, uint32_t flags, int prop_mode, cudaStream_t s) {
+    const dim3 grid(b.pull_tiles_total), block(kPullThreads);
+    switch (wt) {
+        case W_F32: lif_pull_kernel<G, W_F32><<<grid, block, 0, s>>>(b.nets, b.pull_prefix, b.n_nets, flags, prop_mode); break;
+        case W_BF16: lif_pull_kernel<G, W_BF16><<<grid, block, 0, s>>>(b.nets, b.pull_prefix, b.n_nets, flags, prop_mode); break;
+        case W_F16: lif_pull_kernel<G, W_F16><<<grid, block, 0, s>>>(b.nets, b.pull_prefix, b.n_nets, flags, prop_mode); break;
+        default: lif_pull_kernel<G, W_U8><<<grid, block, 0, s>>>(b.nets, b.pull_prefix, b.n_nets, flags, prop_mode); break;
+    }
+}
+
+cudaError_t launch_pull(const LaunchBatch& b, int gather, int wt, uint32_t flags, int prop_mode, cudaStream_t s) {
+    if (b.pull_tiles_total == 0) return cudaSuccess;
+    if (gather) pull_dispatch<1>(b, wt, flags, prop_mode, s); else pull_dispatch<0>(b, wt, flags, prop_mode, s);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold_finish(const LaunchBatch& b, cudaStream_t s) {
+    if (b.lif_tiles_total == 0) return cudaSuccess;
+    fold_finish_kernel<<<b.lif_tiles_total, kLifThreads, 0, s>>>(b.nets, b.lif_prefix, b.n_nets);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_finish(const LaunchBatch& b, int wt, cudaStream_t s) {
+    if (b.pull_tiles_total == 0) return cudaSuccess;
+    const dim3 grid(b.pull_tiles_total), block(kPullThreads);
+    switch (wt) {
+        case W_F32: gather_finish_kernel<W_F32><<<grid, block, 0, s>>>(b.nets, b.pull_prefix, b.n_nets); break;
+        case W_BF16: gather_finish_kernel<W_BF16><<<grid, block, 0, s>>>(b.nets, b.pull_prefix, b.n_nets); break;
+        case W_F16: gather_finish_kernel<W_F16><<<grid, block, 0, s>>>(b.nets, b.pull_prefix, b.n_nets); break;
+        default: gather_finish_kernel<W_U8><<<grid, block, 0, s>>>(b.nets, b.pull_prefix, b.n_nets); break;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace dtb

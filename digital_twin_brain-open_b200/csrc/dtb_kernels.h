@@ -1,0 +1,53 @@
+// Host-side launch interface of the per-step kernels and the device network builder.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dtb_device.cuh"
+
+namespace dtb {
+
+// One launch group: a batch of networks advanced together.
+struct LaunchBatch {
+    const NetView* nets;          // device array [n_nets]
+    const uint32_t* lif_prefix;   // device [n_nets + 1] cumulative LIF tiles (1024 neurons)
+    const uint32_t* pull_prefix;  // device [n_nets + 1] cumulative pull tiles (256 neurons)
+    const uint32_t* vbase;        // device [n_nets + 1] cumulative padded neuron counts
+    uint32_t n_nets;
+    uint32_t lif_tiles_total;
+    uint32_t pull_tiles_total;
+    uint32_t push_ctas;
+    SpikeList spikes;
+};
+
+cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop_mode, cudaStream_t s);
+cudaError_t launch_push(const LaunchBatch& b, int exact, int weight_type, cudaStream_t s);
+cudaError_t launch_pull(const LaunchBatch& b, int gather, int weight_type, uint32_t flags, int prop_mode, cudaStream_t s);
+cudaError_t launch_fold_finish(const LaunchBatch& b, cudaStream_t s);
+cudaError_t launch_gather_finish(const LaunchBatch& b, int weight_type, cudaStream_t s);
+
+// ---- device network generator (dtb_generate.cu)
+struct GenSpec {
+    uint32_t n, n_pops, in_degree, dyadic;
+    unsigned long long seed;
+    const uint32_t* pop_off;          // device [n_pops + 1]
+    const uint32_t* pop_exc;          // device [n_pops]
+    const unsigned long long* cdf;    // device [n_pops * n_pops]
+};
+
+// Builds the requested CSRs on the device.  out_* / in_* may be null when not
+// wanted.  Temporary device memory is allocated and released inside.
+cudaError_t build_structured(const GenSpec& g, int weight_type,
+                             unsigned long long* out_ptr, uint32_t* out_col, void* out_w,
+                             unsigned long long* in_ptr, uint32_t* in_col, void* in_w,
+                             uint32_t* out_deg, cudaStream_t s);
+
+// Host mirror of one generated edge (used by the host builder for small networks
+// and by the tests through the oracle).
+void host_gen_edge(uint32_t n_pops, const uint32_t* pop_off, const uint32_t* pop_exc,
+                   const unsigned long long* cdf, unsigned long long seed, uint32_t dyadic,
+                   uint32_t post, uint32_t pop_of_post, uint32_t k,
+                   uint32_t* pre, uint32_t* kind, float* w0, float* w1);
+
+}  // namespace dtb

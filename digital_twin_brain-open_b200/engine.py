@@ -1,0 +1,340 @@
+"""ctypes binding of ``include/dtb_b200.h`` -- the host-side mirror of the reference's
+block engine (``dtb::BrainBlock``, include/block.hpp:21-889) as driven by the
+``snn.proto`` service.
+
+Every call goes to the CUDA library ``libdtb_b200.so`` built in-tree; there is no
+CPU fallback: if the library is missing, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdtb_b200.so")
+
+# status codes (dtb_status)
+OK, INVALID_PARAMETER, UNSET_SAMPLE_FAILURE, UNSUPPORTED, NOT_ENABLE_METRIC, INVALID_NETWORK = 0, 1, 2, 3, 4, 5
+OUT_OF_MEMORY, CUDA_ERROR, DEVICE_FAULT, IO_ERROR, NO_DEVICE = 16, 17, 18, 19, 20
+
+W_F32, W_BF16, W_F16, W_U8, W_F64 = 0, 1, 2, 3, 4
+PROP_THRESHOLD, PROP_NOISE, PROP_OR = 0, 1, 2
+SYN_PUSH, SYN_PUSH_EXACT, SYN_PULL = 0, 1, 2
+NOISE_PHILOX, NOISE_INJECTED = 0, 1
+RUN_USE_OU, RUN_FREQ, RUN_VMEAN, RUN_RECORD_SPIKES = 1, 2, 4, 8
+STATE_V, STATE_J, STATE_I_OU, STATE_T_LAST = 0, 1, 2, 3
+
+# snn.proto PropType
+PROP_IDS = dict(EXT_STIMULI_I=0, MEMBRANE_C=1, REF_T=2, LEAKAGE_G=3, LEAKAGE_V=4, THRESHOLD_V=5, RESET_V=6,
+                CONDUCT_G_AMPA=7, CONDUCT_G_NMDA=8, CONDUCT_G_GABAa=9, CONDUCT_G_GABAb=10,
+                MEMBRANE_V_AMPA=11, MEMBRANE_V_NMDA=12, MEMBRANE_V_GABAa=13, MEMBRANE_V_GABAb=14,
+                TAO_AMPA=15, TAO_NMDA=16, TAO_GABAa=17, TAO_GABAb=18, NOISE_RATE=19)
+
+
+class DtbError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{status_string(status)}: {message}")
+        self.status = status
+
+
+class Options(C.Structure):
+    _fields_ = [("dt", C.c_float), ("weight_type", C.c_uint32), ("seed", C.c_uint64),
+                ("build_push", C.c_uint32), ("build_pull", C.c_uint32),
+                ("ou_mean", C.c_float), ("ou_sigma", C.c_float), ("ou_tau", C.c_float),
+                ("reserved", C.c_uint32 * 8)]
+
+
+class NetworkArrays(C.Structure):
+    _fields_ = [("n_neurons", C.c_uint32), ("property", C.c_void_p), ("n_edges", C.c_uint64),
+                ("input_block_idx", C.c_void_p), ("input_neuron_idx", C.c_void_p),
+                ("output_neuron_idx", C.c_void_p), ("input_channel_offset", C.c_void_p),
+                ("weight", C.c_void_p), ("weight_type", C.c_uint32)]
+
+
+class StructuredSpecC(C.Structure):
+    _fields_ = [("n_pops", C.c_uint32), ("pop_sizes", C.c_void_p), ("pop_exc", C.c_void_p),
+                ("src_cdf", C.c_void_p), ("pop_property", C.c_void_p), ("pop_id_base", C.c_uint32),
+                ("in_degree", C.c_uint32), ("seed", C.c_uint64), ("dyadic_weights", C.c_uint32)]
+
+
+class EngineInfo(C.Structure):
+    _fields_ = [("n_neurons", C.c_uint32), ("n_pops", C.c_uint32), ("n_edges", C.c_uint64),
+                ("device_bytes", C.c_uint64), ("step", C.c_uint64), ("t", C.c_float),
+                ("weight_type", C.c_uint32), ("has_push", C.c_uint32), ("has_pull", C.c_uint32),
+                ("per_neuron_params", C.c_uint32)]
+
+
+class RunRequest(C.Structure):
+    _fields_ = [("iters", C.c_uint32), ("flags", C.c_uint32), ("prop_mode", C.c_uint32),
+                ("syn_mode", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+
+
+class RunOutput(C.Structure):
+    _fields_ = [("freqs", C.c_void_p), ("vmeans", C.c_void_p), ("spike_bits", C.c_void_p),
+                ("events", C.c_uint64), ("device_ms", C.c_double)]
+
+
+_P = C.c_void_p
+_U32 = C.c_uint32
+_I32 = C.c_int32
+SIGNATURES = {
+    "dtb_abi_version": (_I32, []),
+    "dtb_engine_version": (_I32, []),
+    "dtb_status_string": (C.c_char_p, [_I32]),
+    "dtb_last_error": (C.c_char_p, []),
+    "dtb_default_options": (None, [_P]),
+    "dtb_create": (_I32, [_P, _P, C.POINTER(C.c_void_p)]),
+    "dtb_create_structured": (_I32, [_P, _P, C.POINTER(C.c_void_p)]),
+    "dtb_create_from_npz": (_I32, [C.c_char_p, _P, C.POINTER(C.c_void_p)]),
+    "dtb_destroy": (_I32, [_P]),
+    "dtb_info": (_I32, [_P, _P]),
+    "dtb_populations": (_I32, [_P, _P, _P]),
+    "dtb_update_props": (_I32, [_P, _U32, _P, _P, _P]),
+    "dtb_update_prop_cols": (_I32, [_P, _U32, _P, _P, _P, _I32]),
+    "dtb_update_gamma": (_I32, [_P, _U32, _P, _P, _P, _P]),
+    "dtb_set_ou": (_I32, [_P, _U32, _P, _P, _P, _P]),
+    "dtb_set_noise": (_I32, [_P, _U32, _U32, _P, _P]),
+    "dtb_run": (_I32, [_P, _P, _P]),
+    "dtb_read_state": (_I32, [_P, _I32, _P]),
+    "dtb_write_state": (_I32, [_P, _I32, _P]),
+    "dtb_read_out_csr": (_I32, [_P, _P, _P, _P, _P, _P, _P, _P]),
+    "dtb_state_size": (_I32, [_P, _P]),
+    "dtb_save_state": (_I32, [_P, _P, C.c_uint64]),
+    "dtb_load_state": (_I32, [_P, _P, C.c_uint64]),
+    "dtb_build_out_csr_host": (_I32, [_U32, C.c_uint64, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+}
+
+
+def load_library(path=LIB_PATH):
+    if not os.path.exists(path):
+        raise ImportError(f"libdtb_b200.so not built ({path}); run digital_twin_brain-open_b200/build.py")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+LIB = load_library()
+
+
+def status_string(status):
+    return LIB.dtb_status_string(int(status)).decode()
+
+
+def _check(status):
+    if status != OK:
+        raise DtbError(status, LIB.dtb_last_error().decode())
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def default_options(dt=0.1, weight_type=W_F32, seed=0, push=True, pull=False, ou=(0.6, 0.2, 10.0)):
+    o = Options()
+    LIB.dtb_default_options(C.byref(o))
+    o.dt = dt
+    o.weight_type = weight_type
+    o.seed = seed
+    o.build_push = int(push)
+    o.build_pull = int(pull)
+    o.ou_mean, o.ou_sigma, o.ou_tau = ou
+    return o
+
+
+def build_out_csr_host(n, pre, post, kind):
+    """The reference's out-degree CSR built on the host (no GPU): rows, row_ptr, post, kind, perm."""
+    pre, post = _u32(pre), _u32(post)
+    kind = np.ascontiguousarray(kind, np.uint8)
+    s = pre.shape[0]
+    rows = np.empty(n, np.uint32)
+    row_ptr = np.empty(n + 1, np.uint64)
+    post_o = np.empty(s, np.uint32)
+    kind_o = np.empty(s, np.uint8)
+    perm = np.empty(s, np.uint64)
+    nr = C.c_uint32()
+    _check(LIB.dtb_build_out_csr_host(n, s, _ptr(pre), _ptr(post), _ptr(kind), C.byref(nr), _ptr(rows),
+                                      _ptr(row_ptr), _ptr(post_o), _ptr(kind_o), _ptr(perm)))
+    nr = nr.value
+    return rows[:nr], row_ptr[:nr + 1], post_o, kind_o, perm
+
+
+@dataclasses.dataclass
+class RunResult:
+    freqs: np.ndarray | None
+    vmeans: np.ndarray | None
+    spikes: np.ndarray | None      # bool [iters, n] threshold spikes
+    events: int
+    device_ms: float
+
+
+class Engine:
+    """One network resident in HBM (reference: BrainBlock + snn_run)."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle)
+        inf = self.info()
+        self.n = inf.n_neurons
+        self.n_pops = inf.n_pops
+        self.pop_ids, self.pop_sizes = self.populations()
+
+    # ---- construction
+    @classmethod
+    def from_arrays(cls, net, **opts):
+        prop = _f32(net["property"])
+        n = prop.shape[0]
+        w = np.ascontiguousarray(net["weight"])
+        wt = {np.dtype(np.float32): W_F32, np.dtype(np.float64): W_F64, np.dtype(np.float16): W_F16,
+              np.dtype(np.uint8): W_U8}[w.dtype]
+        pre = _u32(net["input_neuron_idx"])
+        post = _u32(net["output_neuron_idx"])
+        kind = np.ascontiguousarray(net["input_channel_offset"], np.uint8)
+        blk = net.get("input_block_idx")
+        blk = None if blk is None else np.ascontiguousarray(blk, np.int16)
+        a = NetworkArrays(n, prop.ctypes.data, pre.shape[0], None if blk is None else blk.ctypes.data,
+                          pre.ctypes.data, post.ctypes.data, kind.ctypes.data, w.ctypes.data, wt)
+        o = default_options(**opts)
+        h = C.c_void_p()
+        _check(LIB.dtb_create(C.byref(a), C.byref(o), C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def structured(cls, spec, pop_id_base=0, **opts):
+        sizes = _u32(spec.pop_sizes)
+        exc = _u32(spec.pop_exc)
+        cdf = np.ascontiguousarray(spec.src_cdf, np.uint64)
+        prop = np.ascontiguousarray(spec.property_rows(), np.float32)
+        s = StructuredSpecC(spec.n_pops, sizes.ctypes.data, exc.ctypes.data, cdf.ctypes.data, prop.ctypes.data,
+                            pop_id_base, spec.in_degree, spec.seed, int(spec.dyadic_weights))
+        o = default_options(**opts)
+        h = C.c_void_p()
+        _check(LIB.dtb_create_structured(C.byref(s), C.byref(o), C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_npz(cls, path, **opts):
+        o = default_options(**opts)
+        h = C.c_void_p()
+        _check(LIB.dtb_create_from_npz(os.fsencode(path), C.byref(o), C.byref(h)))
+        return cls(h.value)
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            _check(LIB.dtb_destroy(self._h))
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- queries
+    def info(self):
+        inf = EngineInfo()
+        _check(LIB.dtb_info(self._h, C.byref(inf)))
+        return inf
+
+    def populations(self):
+        p = self.info().n_pops
+        ids = np.empty(p, np.uint32)
+        counts = np.empty(p, np.uint32)
+        _check(LIB.dtb_populations(self._h, _ptr(ids), _ptr(counts)))
+        return ids, counts
+
+    # ---- property surface
+    def update_props(self, neuron_ids, prop_ids, values):
+        nid, pid, val = _u32(neuron_ids), _u32(prop_ids), _f32(values)
+        _check(LIB.dtb_update_props(self._h, nid.shape[0], _ptr(nid), _ptr(pid), _ptr(val)))
+
+    def update_prop_cols(self, prop_ids, pop_ids, values, assign=False):
+        pid, pop, val = _u32(prop_ids), _u32(pop_ids), _f32(values)
+        _check(LIB.dtb_update_prop_cols(self._h, pid.shape[0], _ptr(pid), _ptr(pop), _ptr(val), int(assign)))
+
+    def update_gamma(self, prop_ids, pop_ids, alpha, beta):
+        pid, pop, a, b = _u32(prop_ids), _u32(pop_ids), _f32(alpha), _f32(beta)
+        _check(LIB.dtb_update_gamma(self._h, pid.shape[0], _ptr(pid), _ptr(pop), _ptr(a), _ptr(b)))
+
+    def set_ou(self, pop_ids, mean, sigma, tau):
+        pop, m, s, t = _u32(pop_ids), _f32(mean), _f32(sigma), _f32(tau)
+        _check(LIB.dtb_set_ou(self._h, pop.shape[0], _ptr(pop), _ptr(m), _ptr(s), _ptr(t)))
+
+    def set_noise_injected(self, z, u=None):
+        z = _f32(z)
+        u = None if u is None else _f32(u)
+        _check(LIB.dtb_set_noise(self._h, NOISE_INJECTED, z.shape[0], _ptr(z), _ptr(u)))
+
+    def set_noise_philox(self):
+        _check(LIB.dtb_set_noise(self._h, NOISE_PHILOX, 0, None, None))
+
+    # ---- stepping
+    def run(self, iters, use_ou=True, freq=True, vmean=False, record_spikes=False,
+            prop_mode=PROP_THRESHOLD, syn_mode=SYN_PUSH):
+        flags = (RUN_USE_OU if use_ou else 0) | (RUN_FREQ if freq else 0) | \
+                (RUN_VMEAN if vmean else 0) | (RUN_RECORD_SPIKES if record_spikes else 0)
+        rq = RunRequest(iters, flags, prop_mode, syn_mode)
+        fr = np.zeros((iters, self.n_pops), np.int32) if freq else None
+        vm = np.zeros((iters, self.n_pops), np.float32) if vmean else None
+        words = (self.n + 31) // 32
+        sb = np.zeros((iters, words), np.uint32) if record_spikes else None
+        out = RunOutput(None if fr is None else fr.ctypes.data, None if vm is None else vm.ctypes.data,
+                        None if sb is None else sb.ctypes.data, 0, 0.0)
+        _check(LIB.dtb_run(self._h, C.byref(rq), C.byref(out)))
+        spikes = None
+        if sb is not None:
+            spikes = np.unpackbits(sb.view(np.uint8), axis=1, bitorder="little")[:, :self.n].astype(bool)
+        return RunResult(fr, vm, spikes, int(out.events), float(out.device_ms))
+
+    # ---- state
+    def read_state(self, which):
+        shape = (self.n, 4) if which == STATE_J else (self.n,)
+        a = np.empty(shape, np.float32)
+        _check(LIB.dtb_read_state(self._h, which, _ptr(a)))
+        return a
+
+    def write_state(self, which, a):
+        a = _f32(a)
+        _check(LIB.dtb_write_state(self._h, which, _ptr(a)))
+
+    def read_out_csr(self, weights=True):
+        nr, ne = C.c_uint32(), C.c_uint64()
+        _check(LIB.dtb_read_out_csr(self._h, C.byref(nr), C.byref(ne), None, None, None, None, None))
+        nr, ne = nr.value, ne.value
+        rows = np.empty(nr, np.uint32)
+        ptr = np.empty(nr + 1, np.uint64)
+        post = np.empty(ne, np.uint32)
+        kind = np.empty(ne, np.uint8)
+        w = np.empty((ne, 2), np.float32) if weights else None
+        _check(LIB.dtb_read_out_csr(self._h, C.byref(C.c_uint32()), C.byref(C.c_uint64()), _ptr(rows), _ptr(ptr),
+                                    _ptr(post), _ptr(kind), _ptr(w)))
+        return rows, ptr, post, kind, w
+
+    def save_state(self):
+        size = C.c_uint64()
+        _check(LIB.dtb_state_size(self._h, C.byref(size)))
+        blob = np.empty(size.value, np.uint8)
+        _check(LIB.dtb_save_state(self._h, _ptr(blob), size.value))
+        return blob
+
+    def load_state(self, blob):
+        blob = np.ascontiguousarray(blob, np.uint8)
+        _check(LIB.dtb_load_state(self._h, _ptr(blob), blob.shape[0]))

@@ -1,0 +1,253 @@
+/*
+ * dtb_b200.h -- C-ABI of the B200 engine for the Digital Twin Brain per-timestep
+ * hot path: LIF membrane update with four receptor conductances (AMPA, NMDA,
+ * GABAa, GABAb), refractory clamp and Ornstein-Uhlenbeck background current;
+ * spike detection and compaction; CSR spike propagation into per-receptor
+ * accumulators.
+ *
+ * This library replaces the reference's block engine, the C++ class
+ * dtb::BrainBlock<T,T2> (include/block.hpp:21-889) and its stage launchers
+ * (include/stage.hpp:45-422), behind the service surface of protos/snn.proto.
+ * Every entry point takes plain pointers and sizes; host buffers are copied in
+ * or filled; device memory is owned by the engine.  Every call returns a
+ * dtb_status (the snn.proto SnnStatus codes, extended with engine codes) and
+ * never aborts the process: the reference kills its process on any internal
+ * error (MPICHECK / HIP_CHECK, tools/dist_simulator.cpp:63-70,
+ * include/common.hpp:83).
+ *
+ * Threading: calls on one engine must be serialised by the caller; distinct
+ * engines may be used from different threads.  All engines of a process use
+ * the CUDA device that was current when they were created.
+ */
+#ifndef DTB_B200_H
+#define DTB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DTB_ABI_VERSION 1
+
+/* Status codes.  0-5 are snn.proto's SnnStatus (protos/snn.proto:44-51). */
+typedef enum dtb_status {
+    DTB_OK = 0,
+    DTB_INVALID_PARAMETER = 1,
+    DTB_UNSET_SAMPLE_FAILURE = 2,
+    DTB_UNSUPPORTED = 3,
+    DTB_NOT_ENABLE_METRIC = 4,
+    DTB_INVALID_NETWORK = 5,
+    DTB_OUT_OF_MEMORY = 16,   /* device or pinned-host allocation failed      */
+    DTB_CUDA_ERROR = 17,      /* a CUDA call failed; see dtb_last_error()     */
+    DTB_DEVICE_FAULT = 18,    /* a kernel reported an in-kernel check failure */
+    DTB_IO_ERROR = 19,        /* file missing, short or malformed             */
+    DTB_NO_DEVICE = 20
+} dtb_status;
+
+/* Synaptic weight storage (reference: DataType, include/weights.hpp:14-21,
+ * chosen there by a directory-name substring, src/configuration.cpp:1411-1435). */
+typedef enum dtb_weight_type {
+    DTB_W_F32 = 0,
+    DTB_W_BF16 = 1,   /* bf16 pair, accumulated in fp32 (no reference counterpart) */
+    DTB_W_F16 = 2,    /* reference "half"                                          */
+    DTB_W_U8 = 3,     /* reference "int8"/"uint8": value / 255                      */
+    DTB_W_F64 = 4     /* reference "double": narrowed to fp32 on upload             */
+} dtb_weight_type;
+
+/* What drives the receptor accumulators each step. */
+typedef enum dtb_prop_mode {
+    DTB_PROP_THRESHOLD = 0, /* threshold spikes (models/block_new.py:147, debug_mode=False) */
+    DTB_PROP_NOISE = 1,     /* noise train u < noise_rate replaces them (block_new.py:143-146) */
+    DTB_PROP_OR = 2         /* noise OR threshold (src/stage/spike.cpp:42-68)                 */
+} dtb_prop_mode;
+
+/* How spikes reach the accumulators. */
+typedef enum dtb_syn_mode {
+    DTB_SYN_PUSH = 0,        /* out-degree CSR, fp32 vector reductions into J (fastest)       */
+    DTB_SYN_PUSH_EXACT = 1,  /* out-degree CSR, 64-bit fixed-point atomics: deterministic     */
+    DTB_SYN_PULL = 2         /* in-degree CSR gather fused into the LIF step: deterministic   */
+} dtb_syn_mode;
+
+/* Source of the OU normal draws and the noise-train uniforms. */
+typedef enum dtb_noise_source {
+    DTB_NOISE_PHILOX = 0,    /* counter-based Philox4x32-10 keyed by (seed, step, neuron)     */
+    DTB_NOISE_INJECTED = 1   /* host-supplied draws, e.g. a replay of the reference's stream  */
+} dtb_noise_source;
+
+/* Property ids: snn.proto PropType (protos/snn.proto:94-115). */
+typedef enum dtb_prop_id {
+    DTB_EXT_STIMULI_I = 0, DTB_MEMBRANE_C = 1, DTB_REF_T = 2, DTB_LEAKAGE_G = 3,
+    DTB_LEAKAGE_V = 4, DTB_THRESHOLD_V = 5, DTB_RESET_V = 6,
+    DTB_CONDUCT_G_AMPA = 7, DTB_CONDUCT_G_NMDA = 8, DTB_CONDUCT_G_GABAa = 9, DTB_CONDUCT_G_GABAb = 10,
+    DTB_MEMBRANE_V_AMPA = 11, DTB_MEMBRANE_V_NMDA = 12, DTB_MEMBRANE_V_GABAa = 13, DTB_MEMBRANE_V_GABAb = 14,
+    DTB_TAO_AMPA = 15, DTB_TAO_NMDA = 16, DTB_TAO_GABAa = 17, DTB_TAO_GABAb = 18,
+    DTB_NOISE_RATE = 19,
+    DTB_N_PROPS = 20
+} dtb_prop_id;
+
+/* Options fixed at creation. */
+typedef struct dtb_options {
+    float dt;                 /* ms; InitRequest.delta_t (snn.proto:27-37)                 */
+    uint32_t weight_type;     /* dtb_weight_type of the device copy                        */
+    uint64_t seed;            /* Philox key                                                */
+    uint32_t build_push;      /* build the out-degree CSR (push modes)                     */
+    uint32_t build_pull;      /* build the in-degree CSR (pull mode)                       */
+    float ou_mean, ou_sigma, ou_tau; /* initial OU parameters of every population          */
+    uint32_t reserved[8];
+} dtb_options;
+
+/* A block in the reference's npz key set (src/configuration.cpp:1094-1098,
+ * 1508-1517, 1789).  Edges may come in any order; rows keep the input order
+ * of each presynaptic neuron (the reference's stable sort,
+ * src/configuration.cpp:227-249, 1079-1392). */
+typedef struct dtb_network_arrays {
+    uint32_t n_neurons;
+    const float* property;            /* [n_neurons * 22] row-major float32          */
+    uint64_t n_edges;
+    const int16_t* input_block_idx;   /* [n_edges] relative block id, or NULL (all 0) */
+    const uint32_t* input_neuron_idx; /* [n_edges] presynaptic neuron                */
+    const uint32_t* output_neuron_idx;/* [n_edges] postsynaptic neuron               */
+    const uint8_t* input_channel_offset; /* [n_edges] 0: AMPA/NMDA, nonzero: GABAa/GABAb */
+    const void* weight;               /* [n_edges * 2] of weight_type                */
+    uint32_t weight_type;             /* dtb_weight_type of `weight`                 */
+} dtb_network_arrays;
+
+/* A regional network generated on the device (counter-based, reproducible). */
+typedef struct dtb_structured_spec {
+    uint32_t n_pops;
+    const uint32_t* pop_sizes;   /* [n_pops], contiguous populations in id order            */
+    const uint32_t* pop_exc;     /* [n_pops], first pop_exc[b] neurons of b are excitatory    */
+    const uint64_t* src_cdf;     /* [n_pops*n_pops], row a: source-population CDF x 2^32      */
+    const float* pop_property;   /* [n_pops*22] property row of each population (column 3,
+                                    the population id, is ignored)                            */
+    uint32_t pop_id_base;        /* id of population 0                                       */
+    uint32_t in_degree;          /* edges per postsynaptic neuron                            */
+    uint64_t seed;               /* Philox key of the edge stream                            */
+    uint32_t dyadic_weights;     /* weights quantised to multiples of 1/256                  */
+} dtb_structured_spec;
+
+typedef struct dtb_engine_info {
+    uint32_t n_neurons;
+    uint32_t n_pops;
+    uint64_t n_edges;
+    uint64_t device_bytes;       /* bytes held on the device                                 */
+    uint64_t step;               /* steps simulated so far                                   */
+    float t;                     /* simulated time, ms (float32, advanced by t += dt)        */
+    uint32_t weight_type;
+    uint32_t has_push, has_pull;
+    uint32_t per_neuron_params;  /* 1 once any parameter differs within a population        */
+} dtb_engine_info;
+
+/* RunRequest (snn.proto:63-77) flags. */
+#define DTB_RUN_USE_OU        (1u << 0)  /* use_ou_background                                 */
+#define DTB_RUN_FREQ          (1u << 1)  /* output_freq: per-population spike counts          */
+#define DTB_RUN_VMEAN         (1u << 2)  /* output_vmean                                      */
+#define DTB_RUN_RECORD_SPIKES (1u << 3)  /* copy every step's threshold-spike bitmap out      */
+
+typedef struct dtb_run_request {
+    uint32_t iters;      /* RunRequest.iter; > 0                                                */
+    uint32_t flags;      /* DTB_RUN_*                                                            */
+    uint32_t prop_mode;  /* dtb_prop_mode                                                        */
+    uint32_t syn_mode;   /* dtb_syn_mode                                                         */
+    uint32_t reserved[4];
+} dtb_run_request;
+
+typedef struct dtb_run_output {
+    int32_t* freqs;         /* [iters * n_pops] spike counts (freq_char is derived on the host) */
+    float* vmeans;          /* [iters * n_pops]                                                 */
+    uint32_t* spike_bits;   /* [iters * ceil(n_neurons/32)] threshold spikes, bit i = neuron i  */
+    uint64_t events;        /* out: synaptic events delivered (sum over steps of out-degrees of
+                               the propagated spikes)                                          */
+    double device_ms;       /* out: device time of the run, CUDA events on the engine stream    */
+} dtb_run_output;
+
+/* --- version and errors ------------------------------------------------- */
+int32_t dtb_abi_version(void);
+/* GetVersion (snn.proto:6): major*1000 + minor*100 + patch (include/version.hpp:3-5). */
+int32_t dtb_engine_version(void);
+const char* dtb_status_string(int32_t status);
+/* Message of the last failure on the calling thread (empty if none). */
+const char* dtb_last_error(void);
+
+/* --- lifetime ----------------------------------------------------------- */
+/* Replaces BrainBlock construction + init_connection_table_gpu +
+ * init_config_params_gpu + init_all_stages_gpu (src/block.cpp:19-179). */
+void dtb_default_options(dtb_options* opt);
+int32_t dtb_create(const dtb_network_arrays* net, const dtb_options* opt, void** engine);
+/* Generate a regional network on the device (no reference counterpart: the
+ * reference reads networks from npz files written by python/make_block.py). */
+int32_t dtb_create_structured(const dtb_structured_spec* spec, const dtb_options* opt, void** engine);
+/* InitRequest path: load block_<i>.npz (src/configuration.cpp:1394, 1778). */
+int32_t dtb_create_from_npz(const char* path, const dtb_options* opt, void** engine);
+int32_t dtb_destroy(void* engine);
+int32_t dtb_info(void* engine, dtb_engine_info* info);
+
+/* InitResponse.subblk_info (snn.proto:39-61): population ids and sizes. */
+int32_t dtb_populations(void* engine, uint32_t* ids, uint32_t* counts);
+
+/* --- property surface (snn.proto Update* RPCs) ------------------------------- */
+/* Updateprop: per-neuron set (src/stage/property.cpp:57-160). */
+int32_t dtb_update_props(void* engine, uint32_t n, const uint32_t* neuron_ids,
+                         const uint32_t* prop_ids, const float* values);
+/* Updatehyperpara: per-population multiply (assign=0) or assign (assign=1)
+ * (src/stage/property.cpp:185-438). Unknown population ids are ignored. */
+int32_t dtb_update_prop_cols(void* engine, uint32_t n, const uint32_t* prop_ids,
+                             const uint32_t* pop_ids, const float* values, int32_t assign);
+/* Updategamma: per-neuron value = Gamma(alpha, 1) / beta within each listed
+ * population (src/stage/property.cpp:494-651). */
+int32_t dtb_update_gamma(void* engine, uint32_t n, const uint32_t* prop_ids,
+                         const uint32_t* pop_ids, const float* alpha, const float* beta);
+/* Updateoubackgroundparam: per-population OU mean, sigma, tau
+ * (src/block.cpp:222-281). A population's OU current is reset to its mean the
+ * first time it is configured, as the reference does. */
+int32_t dtb_set_ou(void* engine, uint32_t n, const uint32_t* pop_ids, const float* mean,
+                   const float* sigma, const float* tau);
+
+/* Noise source for subsequent steps.  DTB_NOISE_INJECTED takes `steps` rows of
+ * n_neurons normal draws `z` and (optionally) uniforms `u`, consumed one row per
+ * step from the next step on. */
+int32_t dtb_set_noise(void* engine, uint32_t source, uint32_t steps, const float* z, const float* u);
+
+/* --- stepping ------------------------------------------------------------ */
+/* Run: the per-iteration loop of tools/dist_simulator.cpp:2072-2315 with
+ * in-HBM spike delivery; outputs land in caller-owned host buffers. */
+int32_t dtb_run(void* engine, const dtb_run_request* req, dtb_run_output* out);
+
+/* --- state access (tests, checkpoint, serving eviction) ------------------ */
+#define DTB_STATE_V      0  /* float [n]                                       */
+#define DTB_STATE_J      1  /* float [n*4] (AMPA, NMDA, GABAa, GABAb per neuron) */
+#define DTB_STATE_I_OU   2  /* float [n]                                       */
+#define DTB_STATE_T_LAST 3  /* float [n] time of the last threshold spike      */
+int32_t dtb_read_state(void* engine, int32_t which, void* host_dst);
+int32_t dtb_write_state(void* engine, int32_t which, const void* host_src);
+
+/* The out-degree CSR as the reference's builder lays it out
+ * (src/configuration.cpp:1079-1392): rows are presynaptic neurons with at least
+ * one synapse, in ascending order (`rows`), row_ptr over them, and per synapse
+ * the postsynaptic neuron, the receptor pair (0 or 1) and the weight pair as
+ * float32.  Pass NULL for arrays not wanted; *n_rows / *n_edges are always set. */
+int32_t dtb_read_out_csr(void* engine, uint32_t* n_rows, uint64_t* n_edges, uint32_t* rows,
+                         uint64_t* row_ptr, uint32_t* post, uint8_t* kind, float* weight);
+
+/* The same out-degree CSR built on the host from edge arrays, with no device
+ * involved (src/configuration.cpp:1079-1392 semantics: a stable sort of the
+ * synapses by presynaptic neuron).  Outputs: *n_rows, rows [n_neurons],
+ * row_ptr [n_neurons + 1] (first *n_rows + 1 used), post_out, kind_out (0/1)
+ * and perm (input index of each CSR slot), each [n_edges]. */
+int32_t dtb_build_out_csr_host(uint32_t n_neurons, uint64_t n_edges, const uint32_t* pre, const uint32_t* post,
+                               const uint8_t* kind, uint32_t* n_rows, uint32_t* rows, uint64_t* row_ptr,
+                               uint32_t* post_out, uint8_t* kind_out, uint64_t* perm);
+
+/* Serving eviction: the whole dynamic state (V, J, I_ou, t_last, clock and the
+ * last step's spikes) as one blob.  dtb_state_size gives its size. */
+int32_t dtb_state_size(void* engine, uint64_t* bytes);
+int32_t dtb_save_state(void* engine, void* host_blob, uint64_t bytes);
+int32_t dtb_load_state(void* engine, const void* host_blob, uint64_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DTB_B200_H */

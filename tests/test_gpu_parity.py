@@ -1,0 +1,295 @@
+"""Parity of the CUDA engine with the CPU oracle, through the C-ABI (GPU only).
+
+Bars (fixed by the task statement):
+* bit-exact for integer work: CSR construction, spike lists, spike counts;
+* exact-push and pull modes sum synaptic input in 64-bit fixed point, which is
+  exact for weights that are multiples of 2^-24 (every U(0,1) float32 weight here),
+  so V, J and the spike trains match the oracle bit for bit for the whole run;
+* float-push (vector float reductions, nondeterministic order): spike trains equal
+  until the first threshold divergence, V within 1e-5 relative before it.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from dtb_b200 import engine as E
+from dtb_b200 import network as nw
+from oracle import csr_oracle as co
+from oracle import lif_oracle as lo
+
+pytestmark = pytest.mark.gpu
+
+V_RTOL = 1e-5
+
+
+def oracle_run(net, z, u=None, prop_mode=lo.PROP_THRESHOLD, steps=None, oracle=None):
+    o = oracle or lo.LifOracle(net, prop_mode=prop_mode)
+    steps = steps or z.shape[0]
+    spikes, counts, vmeans = [], [], []
+    for s in range(steps):
+        a, _ = o.step(z[s], None if u is None else u[s])
+        spikes.append(a)
+        c, vm = o.population_stats(a)
+        counts.append(c)
+        vmeans.append(vm)
+    return o, np.array(spikes), np.array(counts), np.array(vmeans)
+
+
+def first_divergence(a, b):
+    bad = np.nonzero((a != b).any(axis=1))[0]
+    return int(bad[0]) if bad.size else None
+
+
+@pytest.fixture(scope="module")
+def block10k():
+    return nw.make_uniform_block(10_000, 100, seed=0)
+
+
+@pytest.mark.parametrize("syn", [E.SYN_PUSH_EXACT, E.SYN_PULL])
+@pytest.mark.parametrize("dyadic", [True, False])
+def test_deterministic_modes_bit_exact(gpu, syn, dyadic):
+    net = nw.make_uniform_block(10_000, 100, seed=0, dyadic_weights=dyadic)
+    steps = 400
+    z, _ = lo.torch_noise_stream(0, 10_000, steps, False)
+    o, spikes, counts, vmeans = oracle_run(net, z)
+    with E.Engine.from_arrays(net, push=True, pull=True) as eng:
+        eng.set_noise_injected(z)
+        r = eng.run(steps, freq=True, vmean=True, record_spikes=True, syn_mode=syn)
+        assert first_divergence(r.spikes, spikes) is None
+        assert np.array_equal(r.freqs, counts.astype(np.int32))
+        assert np.array_equal(eng.read_state(E.STATE_V), o.V)
+        assert np.array_equal(eng.read_state(E.STATE_J), o.J.T)
+        assert np.array_equal(eng.read_state(E.STATE_I_OU), o.i_bg)
+        assert np.array_equal(eng.read_state(E.STATE_T_LAST), o.t_last)
+        assert np.allclose(r.vmeans, vmeans, rtol=1e-6, atol=0)
+        expected_events = int(sum(np.bincount(net["input_neuron_idx"], minlength=10_000)[s].sum() for s in spikes))
+        assert r.events == expected_events
+
+
+def test_float_push_within_tolerance(gpu, block10k):
+    steps = 400
+    z, _ = lo.torch_noise_stream(0, 10_000, steps, False)
+    o = lo.LifOracle(block10k)
+    with E.Engine.from_arrays(block10k) as eng:
+        eng.set_noise_injected(z)
+        div = None
+        for s in range(steps):
+            r = eng.run(1, freq=False, record_spikes=True, syn_mode=E.SYN_PUSH)
+            a, _ = o.step(z[s])
+            if not np.array_equal(r.spikes[0], a):
+                div = s
+                break
+            v = eng.read_state(E.STATE_V)
+            assert np.max(np.abs(v - o.V) / np.abs(o.V)) < V_RTOL, f"step {s}"
+    assert div is None or div > 100, f"threshold divergence at step {div}"
+
+
+@pytest.mark.parametrize("case", ["threshold_dyadic", "noise_dyadic", "threshold", "noise"])
+def test_against_block_new_golden(gpu, case):
+    """Directly against the reference's own CPU model output (no oracle in between)."""
+    g = np.load(os.path.join(GOLDEN, f"block_new_{case}.npz"))
+    n, k, steps = int(g["n"]), int(g["k"]), int(g["steps"])
+    rate, debug, dyadic = float(g["noise_rate"]), bool(g["debug"]), bool(g["dyadic"])
+    net = nw.make_uniform_block(n, k, seed=int(g["seed"]), noise_rate=rate, dyadic_weights=dyadic)
+    z, u = lo.torch_noise_stream(0, n, steps, debug)
+    ref = np.unpackbits(g["spikes"], axis=1)[:, :n].astype(bool)
+    pm = E.PROP_NOISE if debug else E.PROP_THRESHOLD
+    with E.Engine.from_arrays(net) as eng:
+        eng.set_noise_injected(z, u)
+        done = 0
+        for s_end in sorted(int(x.split("_")[-1]) for x in g.files if x.startswith("v_full_")):
+            r = eng.run(s_end - done, freq=True, record_spikes=True, prop_mode=pm, syn_mode=E.SYN_PUSH_EXACT)
+            assert first_divergence(r.spikes, ref[done:s_end]) is None, f"spikes differ in steps {done}..{s_end}"
+            assert np.allclose(r.freqs[:, 0] / n, g["mean_act"][done:s_end], rtol=0, atol=1e-7)
+            v = eng.read_state(E.STATE_V)
+            if dyadic:
+                assert np.array_equal(v, g[f"v_full_{s_end}"])
+                assert np.array_equal(eng.read_state(E.STATE_J), g[f"j_full_{s_end}"].T)
+            else:
+                assert np.max(np.abs(v - g[f"v_full_{s_end}"]) / np.abs(g[f"v_full_{s_end}"])) < V_RTOL
+            done = s_end
+
+
+@pytest.mark.parametrize("prop_mode", [E.PROP_NOISE, E.PROP_OR])
+def test_noise_train_modes(gpu, prop_mode):
+    net = nw.make_uniform_block(4000, 60, seed=4, noise_rate=0.02)
+    steps = 200
+    z, u = lo.torch_noise_stream(3, 4000, steps, True)
+    o, spikes, counts, _ = oracle_run(net, z, u, prop_mode=prop_mode)
+    with E.Engine.from_arrays(net, pull=True) as eng:
+        eng.set_noise_injected(z, u)
+        r = eng.run(steps, record_spikes=True, prop_mode=prop_mode, syn_mode=E.SYN_PUSH_EXACT)
+    assert first_divergence(r.spikes, spikes) is None
+    assert np.array_equal(r.freqs, counts.astype(np.int32))
+
+
+def test_structured_csr_bit_exact(gpu):
+    spec = nw.structured_spec(20_000, 12, 60, seed=21)
+    host = co.reference_out_csr(co.structured_edges(spec))
+    with E.Engine.structured(spec) as eng:
+        rows, ptr, post, kind, w = eng.read_out_csr()
+    assert np.array_equal(rows, host["rows"])
+    assert np.array_equal(ptr, host["row_ptr"])
+    assert np.array_equal(post, host["post"])
+    assert np.array_equal(kind, host["kind"])
+    assert np.array_equal(w, host["weight"])
+
+
+@pytest.mark.parametrize("syn", [E.SYN_PUSH_EXACT, E.SYN_PULL])
+def test_structured_run_bit_exact(gpu, syn):
+    spec = nw.structured_spec(12_000, 8, 80, seed=5)
+    net = co.structured_edges(spec)
+    steps = 300
+    z, _ = lo.torch_noise_stream(7, spec.n, steps, False)
+    o, spikes, counts, vmeans = oracle_run(net, z)
+    with E.Engine.structured(spec, pull=True) as eng:
+        assert list(eng.pop_sizes) == list(spec.pop_sizes)
+        eng.set_noise_injected(z)
+        r = eng.run(steps, vmean=True, record_spikes=True, syn_mode=syn)
+        assert first_divergence(r.spikes, spikes) is None
+        assert np.array_equal(r.freqs, counts.astype(np.int32))
+        assert np.allclose(r.vmeans, vmeans, rtol=1e-6)
+        assert np.array_equal(eng.read_state(E.STATE_V), o.V)
+
+
+def test_property_updates_follow_oracle(gpu):
+    spec = nw.structured_spec(6000, 5, 50, seed=9)
+    net = co.structured_edges(spec)
+    steps = 240
+    z, _ = lo.torch_noise_stream(2, spec.n, steps, False)
+    o = lo.LifOracle(net)
+    prop = net["property"].copy()
+    with E.Engine.structured(spec) as eng:
+        eng.set_noise_injected(z)
+        seg = 60
+        r = eng.run(seg, record_spikes=True, syn_mode=E.SYN_PUSH_EXACT)
+        ref = np.array([o.step(z[s])[0] for s in range(0, seg)])
+        assert first_divergence(r.spikes, ref) is None
+        # per-population multiply (Updatehyperpara, assigned=False) of g_AMPA and tau_NMDA
+        eng.update_prop_cols([E.PROP_IDS["CONDUCT_G_AMPA"], E.PROP_IDS["TAO_NMDA"]], [1, 3], [1.5, 0.5])
+        off = spec.pop_offsets
+        prop[off[1]:off[2], 10] *= np.float32(1.5)
+        prop[off[3]:off[4], 19] *= np.float32(0.5)
+        o.set_property(prop)
+        r = eng.run(seg, record_spikes=True, syn_mode=E.SYN_PUSH_EXACT)
+        ref = np.array([o.step(z[s])[0] for s in range(seg, 2 * seg)])
+        assert first_divergence(r.spikes, ref) is None
+        # per-neuron set (Updateprop): thresholds of a few neurons
+        nid = np.array([3, 100, 2500, 5999])
+        eng.update_props(nid, [E.PROP_IDS["THRESHOLD_V"]] * 4, [-52.0] * 4)
+        prop[nid, 8] = -52.0
+        o.set_property(prop)
+        assert eng.info().per_neuron_params == 1
+        r = eng.run(seg, record_spikes=True, syn_mode=E.SYN_PUSH_EXACT)
+        ref = np.array([o.step(z[s])[0] for s in range(2 * seg, 3 * seg)])
+        assert first_divergence(r.spikes, ref) is None
+        # OU parameters of one population (Updateoubackgroundparam): first set resets i_ou to the mean
+        eng.set_ou([2], [0.8], [0.25], [8.0])
+        m = np.zeros(spec.n, bool)
+        m[off[2]:off[3]] = True
+        o.set_ou(0.8, 0.25, 8.0, m)
+        o.i_bg[m] = np.float32(0.8)
+        r = eng.run(seg, record_spikes=True, syn_mode=E.SYN_PUSH_EXACT)
+        ref = np.array([o.step(z[s])[0] for s in range(3 * seg, 4 * seg)])
+        assert first_divergence(r.spikes, ref) is None
+        assert np.array_equal(eng.read_state(E.STATE_V), o.V)
+
+
+def test_gamma_resample(gpu):
+    spec = nw.structured_spec(8000, 4, 40, seed=1)
+    with E.Engine.structured(spec) as eng:
+        eng.update_gamma([E.PROP_IDS["CONDUCT_G_AMPA"]], [1], [4.0], [400.0])
+        assert eng.info().per_neuron_params == 1
+        eng.run(50)   # runs with per-neuron parameters
+
+
+def test_save_load_round_trip(gpu):
+    net = nw.make_uniform_block(5000, 50, seed=8)
+    z, _ = lo.torch_noise_stream(5, 5000, 300, False)
+    with E.Engine.from_arrays(net, pull=True) as eng:
+        eng.set_noise_injected(z)
+        eng.run(100, syn_mode=E.SYN_PULL)
+        blob = eng.save_state()
+        a = eng.run(100, record_spikes=True, syn_mode=E.SYN_PUSH_EXACT)
+        va = eng.read_state(E.STATE_V)
+        eng.load_state(blob)
+        assert eng.info().step == 100
+        eng.set_noise_injected(z[100:])
+        b = eng.run(100, record_spikes=True, syn_mode=E.SYN_PUSH_EXACT)
+        assert np.array_equal(a.spikes, b.spikes)
+        assert np.array_equal(va, eng.read_state(E.STATE_V))
+
+
+def test_mode_switch_keeps_state_consistent(gpu, block10k):
+    """push, exact push and pull leave the same canonical state between runs."""
+    z, _ = lo.torch_noise_stream(1, 10_000, 300, False)
+    o, spikes, _, _ = oracle_run(block10k, z)
+    with E.Engine.from_arrays(block10k, pull=True) as eng:
+        eng.set_noise_injected(z)
+        got = []
+        for syn in (E.SYN_PULL, E.SYN_PUSH_EXACT, E.SYN_PULL):
+            got.append(eng.run(100, record_spikes=True, syn_mode=syn).spikes)
+        assert first_divergence(np.concatenate(got), spikes) is None
+        assert np.array_equal(eng.read_state(E.STATE_V), o.V)
+
+
+def test_npz_loading_matches_arrays(gpu, tmp_path):
+    net = nw.make_uniform_block(3000, 40, seed=6)
+    p1 = tmp_path / "single" / "block_0.npz"
+    p1.parent.mkdir()
+    nw.write_npz(str(p1), net)
+    p2 = tmp_path / "block_c.npz"
+    np.savez_compressed(p2, **net)
+    z, _ = lo.torch_noise_stream(0, 3000, 100, False)
+    outs = []
+    for make in (lambda: E.Engine.from_arrays(net), lambda: E.Engine.from_npz(str(p1)),
+                 lambda: E.Engine.from_npz(str(p2))):
+        with make() as eng:
+            csr = eng.read_out_csr()
+            eng.set_noise_injected(z)
+            outs.append((csr, eng.run(100, record_spikes=True, syn_mode=E.SYN_PUSH_EXACT).spikes))
+    for csr, sp in outs[1:]:
+        for a, b in zip(csr, outs[0][0]):
+            assert np.array_equal(a, b)
+        assert np.array_equal(sp, outs[0][1])
+
+
+def test_errors_are_statuses(gpu):
+    net = nw.make_uniform_block(1000, 10, seed=1)
+    with E.Engine.from_arrays(net) as eng:
+        with pytest.raises(E.DtbError) as ei:
+            eng.run(0)
+        assert ei.value.status == E.INVALID_PARAMETER
+        with pytest.raises(E.DtbError) as ei:
+            eng.run(10, syn_mode=E.SYN_PULL)
+        assert ei.value.status == E.UNSUPPORTED
+        z, _ = lo.torch_noise_stream(0, 1000, 5, False)
+        eng.set_noise_injected(z)
+        with pytest.raises(E.DtbError) as ei:
+            eng.run(10)
+        assert ei.value.status == E.INVALID_PARAMETER
+        eng.set_noise_philox()
+        eng.run(10)
+    bad = dict(net)
+    bad["input_neuron_idx"] = net["input_neuron_idx"].copy()
+    bad["input_neuron_idx"][5] = 1000
+    with pytest.raises(E.DtbError) as ei:
+        E.Engine.from_arrays(bad)
+    assert ei.value.status == E.INVALID_NETWORK
+    with pytest.raises(E.DtbError) as ei:
+        E.Engine.from_npz("/nonexistent/block_0.npz")
+    assert ei.value.status == E.IO_ERROR
+
+
+def test_philox_noise_statistics(gpu, block10k):
+    """Philox OU noise: the same firing statistics as the reference's noise stream."""
+    steps = 3000
+    z, _ = lo.torch_noise_stream(0, 10_000, steps, False)
+    _, spikes, _, _ = oracle_run(block10k, z)
+    with E.Engine.from_arrays(block10k, seed=123) as eng:
+        r = eng.run(steps, record_spikes=True)
+    rate_ref = spikes[1000:].mean()
+    rate_gpu = r.spikes[1000:].mean()
+    assert abs(rate_gpu - rate_ref) / rate_ref < 0.1
