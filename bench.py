@@ -1,0 +1,334 @@
+"""Throughput of the DTB per-timestep hot path on B200: synaptic events/s and
+simulated-ms per wall-second on the 5M-neuron regional network (200 populations,
+in-degree 1000, FP32 weights, OU background, 10,000 steps of 0.1 ms).
+
+Contract (one JSON line on rank 0):
+* a bench step = one window of 500 simulation steps (50 ms simulated) of the whole
+  network, with per-step population spike counts recorded (RunRequest output_freq);
+  --steps 20 is the configuration's full 10,000-step run;
+* value = synaptic events delivered / device time, events summed over ranks and
+  time = max over ranks of CUDA-event time on the engine's own stream;
+* e2e = the same metric through the public C-ABI call (dtb_set_ou + dtb_run) with
+  host buffers: each window uploads new per-population OU parameters and reads
+  back every step's spike counts and mean potentials;
+* roofline = the push kernel (the dominant kernel) against the measured HBM copy
+  bandwidth; cpu_baseline = the C port of the reference CPU model on a sample.
+N > 1 GPUs run independent replicas (no data-path collective: "scaling": "weak").
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "synaptic events/s and sim-ms per wall-s; batched/served vs plain p50/p99 at equal rate"
+UNIT = "synaptic events/s"
+WINDOW = 500
+N_NEURONS, N_POPS, IN_DEGREE, SPEC_SEED = 5_000_000, 200, 1000, 1
+CPU_SAMPLE = dict(n=50_000, pops=20, in_degree=1000, seed=7, burn_in=400, timed=60)
+BYTES_STATE = 56          # V, J x4, i_ou, t_last read + written per neuron per step
+CSR_COL_BYTES = 4
+ACC_BYTES = 8             # one logical accumulator update (a float pair) per event
+ROW_BYTES = 12            # rowptr pair + spike-list entry per spiking row
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--weights", default="f32", choices=["f32", "bf16"])
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--neurons", type=int, default=N_NEURONS, help="network size (profiling runs use a small one)")
+    p.add_argument("--pops", type=int, default=N_POPS)
+    p.add_argument("--degree", type=int, default=IN_DEGREE)
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# CPU: the C port of the reference model on a bounded sample
+# ---------------------------------------------------------------------------
+def cpu_sample_rate(max_seconds=None):
+    from dtb_b200 import network as nw
+    from oracle import c_oracle as cc
+    from oracle import lif_oracle as lo
+    s = CPU_SAMPLE
+    spec = nw.structured_spec(s["n"], s["pops"], s["in_degree"], s["seed"])
+    net = cc.structured_edges(spec)
+    orc = cc.COracle(net)
+    rng = np.random.default_rng(0)
+    z = rng.standard_normal((s["burn_in"], spec.n), dtype=np.float32)
+    orc.run(z, record=False)                             # untimed burn-in past the start-up transient
+    z = rng.standard_normal((s["timed"], spec.n), dtype=np.float32)
+    t0 = time.perf_counter()
+    _, counts, events = orc.run(z, record=False)
+    dt = time.perf_counter() - t0
+    threads = cc.lib().oracle_threads()
+    sample = (f"C port of models/block_new.py (W.s over all synapses each step, float32) on a "
+              f"{spec.n}-neuron, {spec.n_pops}-population, in-degree-{spec.in_degree} network of the same "
+              f"construction: {s['timed']} steps timed after {s['burn_in']} untimed, "
+              f"{int(counts.sum())} spikes, {events} events in {dt:.2f} s")
+    return dict(value=events / dt, unit=UNIT, cores=threads, kind="port", sample=sample,
+                sim_ms_per_wall_s=s["timed"] * 0.1 / dt, ms_per_step=1e3 * dt / s["timed"])
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 8 and (not self.uuid or parts[0].endswith(self.uuid) or self.uuid.endswith(parts[0])):
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        for r in self.rows:
+            for name, val in zip(self.NAMES, r[4:8]):
+                if val.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch(events_per_launch):
+    """DRAM bytes per push launch from the committed ncu summary, scaled by events."""
+    path = os.path.join(ROOT, "profiles", "push_kernel_ncu.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["dram_bytes_per_launch"]) * events_per_launch / float(d["events_per_launch"])
+    except Exception:
+        return None
+
+
+def run_ours(args):
+    import torch
+    import __graft_entry__
+    __graft_entry__.load_package()
+    from dtb_b200 import engine as E
+    from dtb_b200 import network as nw
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    wt = E.W_BF16 if args.weights == "bf16" else E.W_F32
+    spec = nw.structured_spec(args.neurons, args.pops, args.degree, SPEC_SEED)
+    t0 = time.perf_counter()
+    eng = E.Engine.structured(spec, weight_type=wt, seed=1000 + rank)
+    build_s = time.perf_counter() - t0
+    info = eng.info()
+    stream = torch.cuda.ExternalStream(eng.stream(), device=dev)
+    P = eng.n_pops
+    fr = np.zeros((WINDOW, P), np.int32)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        eng.run(WINDOW, freq=True, out=(fr, None))
+
+    uuid = str(getattr(torch.cuda.get_device_properties(dev), "uuid", ""))
+    sampler = ClockSampler(uuid)
+    barrier()
+    sampler.start()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    events = 0
+    spikes = 0
+    launches = 0
+    with torch.cuda.stream(stream):
+        start.record(stream)
+        for _ in range(args.steps):
+            r = eng.run(WINDOW, freq=True, out=(fr, None))
+            events += r.events
+            spikes += int(fr.sum())
+            launches += r.launches
+        end.record(stream)
+    end.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms = start.elapsed_time(end)
+
+    # per-kernel timing window (after the timed region)
+    rk = eng.run(WINDOW, freq=True, out=(fr, None), time_kernels=True)
+    lif_ms, push_ms = rk.kernel_ms[0] / WINDOW, rk.kernel_ms[1] / WINDOW
+    ev_launch = rk.events / WINDOW
+    spk_launch = fr.sum() / WINDOW
+    wbytes = 4 if wt == E.W_BF16 else 8
+    push_bytes = spk_launch * ROW_BYTES + ev_launch * (CSR_COL_BYTES + wbytes + ACC_BYTES)
+    lif_bytes = info.n_neurons * BYTES_STATE + info.n_neurons / 8
+
+    # e2e through the C-ABI with host buffers (H2D of OU parameters, D2H of every step's outputs)
+    rng = np.random.default_rng(rank)
+    pop_ids = eng.pop_ids
+    vm = np.zeros((WINDOW, P), np.float32)
+    e2e_events = 0
+    barrier()
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e_start.record(stream)
+        for _ in range(args.steps):
+            mean = rng.uniform(0.55, 0.65, P).astype(np.float32)
+            sigma = rng.uniform(0.18, 0.22, P).astype(np.float32)
+            eng.set_ou(pop_ids, mean, sigma, np.full(P, 10.0, np.float32))
+            r = eng.run(WINDOW, freq=True, vmean=True, out=(fr, vm))
+            e2e_events += r.events
+        e_end.record(stream)
+    e_end.synchronize()
+    barrier()
+    e2e_ms = e_start.elapsed_time(e_end)
+
+    tot = np.array([events, e2e_events, spikes], np.float64)
+    times = np.array([ms, e2e_ms], np.float64)
+    if dist is not None:
+        t = torch.tensor(tot, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        tot = t.cpu().numpy()
+        tt = torch.tensor(times, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        times = tt.cpu().numpy()
+    events, e2e_events, spikes = tot
+    ms, e2e_ms = times
+    value = events / (ms / 1e3)
+    out = None
+    if rank == 0:
+        peak, peak_kind = peaks()
+        achieved = push_bytes / (push_ms * 1e-3) / 1e9
+        traffic = traffic_per_launch(ev_launch)
+        step_bytes = push_bytes + lif_bytes
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            cpu = cpu_sample_rate()
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        h2d = P * 96 + P * 3 * 4
+        d2h = WINDOW * P * (4 + 8)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if wt == E.W_F32 else "bf16-weights/f32-state",
+            "data": "synthetic (seeded regional network generated on the device)",
+            "sim_ms_per_wall_s": args.steps * WINDOW * 0.1 / (ms / 1e3),
+            "config": {"workload": f"{info.n_neurons}-neuron regional LIF network, {P} populations, "
+                                   f"in-degree {args.degree}, {args.weights} weights, OU background, push propagation",
+                       "neurons": info.n_neurons, "synapses": int(info.n_edges), "populations": P,
+                       "dt_ms": 0.1, "steps_per_bench_step": WINDOW,
+                       "timed_sim_steps": args.steps * WINDOW, "warmup_sim_steps": args.warmup * WINDOW,
+                       "mean_rate_hz": spikes / (world * args.steps * WINDOW) / info.n_neurons * 1e4,
+                       "events_per_sim_step": events / (world * args.steps * WINDOW),
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": f"inputs larger than L2 ({info.n_edges * (4 + wbytes) / 1e9:.1f} GB CSR, "
+                             f"{info.n_neurons * 56 / 1e6:.0f} MB neuron state)",
+                       "device_bytes": int(info.device_bytes), "build_s": build_s,
+                       "lif_ms_per_step": lif_ms, "push_ms_per_step": push_ms,
+                       "step_roofline_frac": step_bytes / ((lif_ms + push_ms) * 1e-3) / 1e9 / peak},
+            "roofline": {"bound": "hbm", "kernel": "push_kernel", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": push_bytes},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_events / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "clocks": clocks,
+            "gpu_launches": int(launches),
+        }
+        if cpu:
+            out["config"]["gpu_over_cpu_port"] = value / cpu["value"]
+    eng.close()
+    del stream
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    cpu = cpu_sample_rate()
+    v = cpu["value"]
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": cpu["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "sim_ms_per_wall_s": cpu["sim_ms_per_wall_s"],
+        "config": {"workload": "5M-neuron regional LIF network, 200 populations, in-degree 1000, f32 weights "
+                               "(timed on a bounded sample of the same construction)"},
+        "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

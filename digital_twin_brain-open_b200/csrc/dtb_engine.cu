@@ -45,6 +45,7 @@ Engine::~Engine() {
     for (void* p : allocs) cudaFree(p);
     if (h_cnt) cudaFreeHost(h_cnt);
     if (h_vsum) cudaFreeHost(h_vsum);
+    for (cudaEvent_t e : tev) cudaEventDestroy(e);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -586,39 +587,62 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     if (injected) kflags |= kFlagInjected;
     const LaunchBatch b = single_batch();
     const int pm = static_cast<int>(rq.prop_mode);
+    const bool time_k = (rq.flags & DTB_RUN_TIME_KERNELS) != 0;
     set_u64_kernel<<<1, 1, 0, stream>>>(events, 0ull);
     DTB_CU(cudaGetLastError());
+    uint32_t launches = 1;
     double ms_total = 0.0;
+    double kms[4] = {0.0, 0.0, 0.0, 0.0};
     uint32_t done = 0;
     while (done < rq.iters) {
         const uint32_t rows = std::min(cap, rq.iters - done);
         DTB_TRY(begin_run_chunk(steps, rows, freq || vmean));
+        ++launches;
+        std::vector<std::pair<int, size_t>> timed;   // (kernel class, event pair index)
+        if (time_k) DTB_TRY(ensure_timing_events(2 * rows + 2));
+        auto timed_launch = [&](int cls, auto&& fn) -> int {
+            if (time_k) DTB_CU(cudaEventRecord(tev[2 * timed.size()], stream));
+            DTB_CU(fn());
+            if (time_k) {
+                DTB_CU(cudaEventRecord(tev[2 * timed.size() + 1], stream));
+                timed.emplace_back(cls, timed.size());
+            }
+            ++launches;
+            return DTB_OK;
+        };
         DTB_CU(cudaEventRecord(ev0, stream));
         for (uint32_t s = 0; s < rows; ++s) {
             const bool first = (done + s) == 0;
             switch (rq.syn_mode) {
                 case DTB_SYN_PUSH:
-                    DTB_CU(launch_lif(b, J_DIRECT, kflags, pm, stream));
-                    DTB_CU(launch_push(b, 0, static_cast<int>(wtype), stream));
+                    DTB_TRY(timed_launch(0, [&] { return launch_lif(b, J_DIRECT, kflags, pm, stream); }));
+                    DTB_TRY(timed_launch(1, [&] { return launch_push(b, 0, static_cast<int>(wtype), stream); }));
                     break;
                 case DTB_SYN_PUSH_EXACT:
-                    DTB_CU(launch_lif(b, first ? J_ASIS : J_FOLD, kflags, pm, stream));
-                    DTB_CU(launch_push(b, 1, static_cast<int>(wtype), stream));
+                    DTB_TRY(timed_launch(0, [&] { return launch_lif(b, first ? J_ASIS : J_FOLD, kflags, pm, stream); }));
+                    DTB_TRY(timed_launch(1, [&] { return launch_push(b, 1, static_cast<int>(wtype), stream); }));
                     break;
                 default:
-                    DTB_CU(launch_pull(b, first ? 0 : 1, static_cast<int>(wtype), kflags, pm, stream));
+                    DTB_TRY(timed_launch(2, [&] { return launch_pull(b, first ? 0 : 1, static_cast<int>(wtype), kflags, pm, stream); }));
                     break;
             }
         }
         if (done + rows == rq.iters) {
-            if (rq.syn_mode == DTB_SYN_PUSH_EXACT) DTB_CU(launch_fold_finish(b, stream));
-            if (rq.syn_mode == DTB_SYN_PULL) DTB_CU(launch_gather_finish(b, static_cast<int>(wtype), stream));
+            if (rq.syn_mode == DTB_SYN_PUSH_EXACT)
+                DTB_TRY(timed_launch(3, [&] { return launch_fold_finish(b, stream); }));
+            if (rq.syn_mode == DTB_SYN_PULL)
+                DTB_TRY(timed_launch(3, [&] { return launch_gather_finish(b, static_cast<int>(wtype), stream); }));
         }
         DTB_CU(cudaEventRecord(ev1, stream));
         DTB_CU(cudaEventSynchronize(ev1));
         float ms = 0.f;
         DTB_CU(cudaEventElapsedTime(&ms, ev0, ev1));
         ms_total += ms;
+        for (const auto& tp : timed) {
+            float km = 0.f;
+            DTB_CU(cudaEventElapsedTime(&km, tev[2 * tp.second], tev[2 * tp.second + 1]));
+            kms[tp.first] += km;
+        }
         for (uint32_t s = 0; s < rows; ++s) {
             volatile float tt = t + dt;
             t = tt;
@@ -627,6 +651,8 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
         DTB_TRY(finish_hist(rows, done, out, freq, vmean, record));
         done += rows;
     }
+    for (int k = 0; k < 4; ++k) out.kernel_ms[k] = kms[k];
+    out.launches = launches;
     Clock ck;
     unsigned long long ev = 0;
     DTB_CU(cudaMemcpyAsync(&ck, clock, sizeof(Clock), cudaMemcpyDeviceToHost, stream));
@@ -639,6 +665,15 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
         set_clock_kernel<<<1, 1, 0, stream>>>(clock, ck.t, ck.n);
         cudaStreamSynchronize(stream);
         return fail(DTB_DEVICE_FAULT, "kernel check failed, error bits " + std::to_string(ck.err));
+    }
+    return DTB_OK;
+}
+
+int Engine::ensure_timing_events(size_t count) {
+    while (tev.size() < count) {
+        cudaEvent_t e;
+        DTB_CU(cudaEventCreate(&e));
+        tev.push_back(e);
     }
     return DTB_OK;
 }
@@ -1025,6 +1060,12 @@ int32_t dtb_destroy(void* engine) {
 int32_t dtb_info(void* engine, dtb_engine_info* info) {
     if (!engine || !info) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
     return as_engine(engine)->info(*info);
+}
+
+int32_t dtb_get_stream(void* engine, void** stream) {
+    if (!engine || !stream) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
+    *stream = as_engine(engine)->stream;
+    return DTB_OK;
 }
 
 int32_t dtb_populations(void* engine, uint32_t* ids, uint32_t* counts) {

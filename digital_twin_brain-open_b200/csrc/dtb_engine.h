@@ -141,6 +141,8 @@ private:
     int upload_csr_host(const uint32_t* pre, const uint32_t* post, const uint8_t* kind_in, const void* w, uint32_t in_type,
                         bool build_push, bool build_pull);
     int weight_bytes() const;
+    int ensure_timing_events(size_t count);
+    std::vector<cudaEvent_t> tev;
 };
 
 }  // namespace dtb

@@ -24,7 +24,7 @@ W_F32, W_BF16, W_F16, W_U8, W_F64 = 0, 1, 2, 3, 4
 PROP_THRESHOLD, PROP_NOISE, PROP_OR = 0, 1, 2
 SYN_PUSH, SYN_PUSH_EXACT, SYN_PULL = 0, 1, 2
 NOISE_PHILOX, NOISE_INJECTED = 0, 1
-RUN_USE_OU, RUN_FREQ, RUN_VMEAN, RUN_RECORD_SPIKES = 1, 2, 4, 8
+RUN_USE_OU, RUN_FREQ, RUN_VMEAN, RUN_RECORD_SPIKES, RUN_TIME_KERNELS = 1, 2, 4, 8, 16
 STATE_V, STATE_J, STATE_I_OU, STATE_T_LAST = 0, 1, 2, 3
 
 # snn.proto PropType
@@ -74,7 +74,8 @@ class RunRequest(C.Structure):
 
 class RunOutput(C.Structure):
     _fields_ = [("freqs", C.c_void_p), ("vmeans", C.c_void_p), ("spike_bits", C.c_void_p),
-                ("events", C.c_uint64), ("device_ms", C.c_double)]
+                ("events", C.c_uint64), ("device_ms", C.c_double), ("kernel_ms", C.c_double * 4),
+                ("launches", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 _P = C.c_void_p
@@ -91,6 +92,7 @@ SIGNATURES = {
     "dtb_create_from_npz": (_I32, [C.c_char_p, _P, C.POINTER(C.c_void_p)]),
     "dtb_destroy": (_I32, [_P]),
     "dtb_info": (_I32, [_P, _P]),
+    "dtb_get_stream": (_I32, [_P, C.POINTER(C.c_void_p)]),
     "dtb_populations": (_I32, [_P, _P, _P]),
     "dtb_update_props": (_I32, [_P, _U32, _P, _P, _P]),
     "dtb_update_prop_cols": (_I32, [_P, _U32, _P, _P, _P, _I32]),
@@ -179,6 +181,8 @@ class RunResult:
     spikes: np.ndarray | None      # bool [iters, n] threshold spikes
     events: int
     device_ms: float
+    kernel_ms: tuple = (0.0, 0.0, 0.0, 0.0)   # LIF, push, pull, end-of-run (with time_kernels)
+    launches: int = 0
 
 
 class Engine:
@@ -254,6 +258,12 @@ class Engine:
         _check(LIB.dtb_info(self._h, C.byref(inf)))
         return inf
 
+    def stream(self):
+        """The engine's cudaStream_t as an integer handle."""
+        s = C.c_void_p()
+        _check(LIB.dtb_get_stream(self._h, C.byref(s)))
+        return s.value or 0
+
     def populations(self):
         p = self.info().n_pops
         ids = np.empty(p, np.uint32)
@@ -288,21 +298,29 @@ class Engine:
 
     # ---- stepping
     def run(self, iters, use_ou=True, freq=True, vmean=False, record_spikes=False,
-            prop_mode=PROP_THRESHOLD, syn_mode=SYN_PUSH):
+            prop_mode=PROP_THRESHOLD, syn_mode=SYN_PUSH, time_kernels=False, out=None):
+        """Advance ``iters`` steps (RunRequest, snn.proto:63-77).
+
+        ``out`` may pass preallocated (freqs, vmeans) host arrays of shape [iters, P].
+        """
         flags = (RUN_USE_OU if use_ou else 0) | (RUN_FREQ if freq else 0) | \
-                (RUN_VMEAN if vmean else 0) | (RUN_RECORD_SPIKES if record_spikes else 0)
+                (RUN_VMEAN if vmean else 0) | (RUN_RECORD_SPIKES if record_spikes else 0) | \
+                (RUN_TIME_KERNELS if time_kernels else 0)
         rq = RunRequest(iters, flags, prop_mode, syn_mode)
-        fr = np.zeros((iters, self.n_pops), np.int32) if freq else None
-        vm = np.zeros((iters, self.n_pops), np.float32) if vmean else None
+        if out is not None:
+            fr, vm = out
+        else:
+            fr = np.zeros((iters, self.n_pops), np.int32) if freq else None
+            vm = np.zeros((iters, self.n_pops), np.float32) if vmean else None
         words = (self.n + 31) // 32
         sb = np.zeros((iters, words), np.uint32) if record_spikes else None
-        out = RunOutput(None if fr is None else fr.ctypes.data, None if vm is None else vm.ctypes.data,
+        res = RunOutput(None if fr is None else fr.ctypes.data, None if vm is None else vm.ctypes.data,
                         None if sb is None else sb.ctypes.data, 0, 0.0)
-        _check(LIB.dtb_run(self._h, C.byref(rq), C.byref(out)))
+        _check(LIB.dtb_run(self._h, C.byref(rq), C.byref(res)))
         spikes = None
         if sb is not None:
             spikes = np.unpackbits(sb.view(np.uint8), axis=1, bitorder="little")[:, :self.n].astype(bool)
-        return RunResult(fr, vm, spikes, int(out.events), float(out.device_ms))
+        return RunResult(fr, vm, spikes, int(res.events), float(res.device_ms), tuple(res.kernel_ms), int(res.launches))
 
     # ---- state
     def read_state(self, which):

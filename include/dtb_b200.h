@@ -145,6 +145,7 @@ typedef struct dtb_engine_info {
 #define DTB_RUN_FREQ          (1u << 1)  /* output_freq: per-population spike counts          */
 #define DTB_RUN_VMEAN         (1u << 2)  /* output_vmean                                      */
 #define DTB_RUN_RECORD_SPIKES (1u << 3)  /* copy every step's threshold-spike bitmap out      */
+#define DTB_RUN_TIME_KERNELS  (1u << 4)  /* time every kernel launch with CUDA events          */
 
 typedef struct dtb_run_request {
     uint32_t iters;      /* RunRequest.iter; > 0                                                */
@@ -161,6 +162,10 @@ typedef struct dtb_run_output {
     uint64_t events;        /* out: synaptic events delivered (sum over steps of out-degrees of
                                the propagated spikes)                                          */
     double device_ms;       /* out: device time of the run, CUDA events on the engine stream    */
+    double kernel_ms[4];    /* out, with DTB_RUN_TIME_KERNELS: summed device time of the LIF,
+                               push, pull and end-of-run kernels                               */
+    uint32_t launches;      /* out: kernels launched by this run                               */
+    uint32_t reserved;
 } dtb_run_output;
 
 /* --- version and errors ------------------------------------------------- */
@@ -183,6 +188,9 @@ int32_t dtb_create_structured(const dtb_structured_spec* spec, const dtb_options
 int32_t dtb_create_from_npz(const char* path, const dtb_options* opt, void** engine);
 int32_t dtb_destroy(void* engine);
 int32_t dtb_info(void* engine, dtb_engine_info* info);
+/* The CUDA stream (cudaStream_t) every kernel and copy of this engine runs on,
+ * so a caller can order its own work and CUDA events against the engine. */
+int32_t dtb_get_stream(void* engine, void** stream);
 
 /* InitResponse.subblk_info (snn.proto:39-61): population ids and sizes. */
 int32_t dtb_populations(void* engine, uint32_t* ids, uint32_t* counts);

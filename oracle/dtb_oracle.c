@@ -1,0 +1,200 @@
+/*
+ * CPU oracle of the DTB per-timestep hot path, in C -- TEST INFRASTRUCTURE ONLY.
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it,
+ * as the checker and as the timed CPU port; the product never does.
+ *
+ * It restates the reference's CPU model models/block_new.py:
+ *   run                   block_new.py:122-158
+ *   update_i_background   block_new.py:92-96
+ *   update_Vi             block_new.py:104-117
+ *   update_J_ui / bmm     block_new.py:71-84   (W.s over ALL synapses every step,
+ *                                               the cost structure of torch.sparse.mm)
+ *   update_I_syn          block_new.py:86-90
+ *   update_t_ik_last      block_new.py:119-120
+ * in the same float32 operation order as oracle/lif_oracle.py (which is pinned
+ * to block_new's own output).  W.s is accumulated in double per postsynaptic
+ * neuron in in-edge order and rounded once, exactly like numpy.bincount.
+ * Build with -ffp-contract=off so no multiply-add is fused.
+ *
+ * It also replays the engine's regional-network edge stream (Philox4x32-10,
+ * Salmon et al. SC'11) so large sample networks can be built on the host fast.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef struct {
+    int32_t n;
+    const int64_t* in_ptr;    /* [n+1] in-edge CSR by postsynaptic neuron      */
+    const uint32_t* in_pre;   /* [S] presynaptic neuron                         */
+    const uint8_t* in_kind;   /* [S] 0: AMPA/NMDA, 1: GABAa/GABAb               */
+    const float* w0;          /* [S]                                            */
+    const float* w1;          /* [S]                                            */
+    /* per-neuron derived constants (see lif_oracle.LifOracle) */
+    const float* dtC;
+    const float* neg_gL;
+    const float* V_L;
+    const float* V_th;
+    const float* V_reset;
+    const float* T_ref;
+    const float* I_ext;
+    const float* noise_rate;
+    const float* g;           /* [4*n] channel-major */
+    const float* Vu;          /* [4*n] */
+    const float* decay;       /* [4*n] */
+    const float* ou_mean;
+    const float* ou_f1;
+    const float* ou_f2s;
+    /* state (updated in place) */
+    float* V;
+    float* i_bg;
+    float* t_last;
+    float* J;                 /* [4*n] channel-major */
+    float* I_syn;
+    float* t;                 /* scalar */
+    /* scratch */
+    uint8_t* active;
+    uint8_t* prop;
+} oracle_net;
+
+static float fadd(float a, float b) { return a + b; }
+static float fmul(float a, float b) { return a * b; }
+static float fsub(float a, float b) { return a - b; }
+
+/* `steps` steps; z [steps*n] normal draws, u [steps*n] uniforms or NULL;
+ * prop_mode 0/1/2 as in lif_oracle.  Threshold spikes go to spikes_out
+ * [steps*n] and per-step spike counts to counts_out [steps] when non-NULL.
+ * Returns the synaptic events delivered (in-edges whose source propagated). */
+int64_t oracle_run(oracle_net* s, int32_t steps, float dt, const float* z, const float* u, int prop_mode,
+                   uint8_t* spikes_out, int64_t* counts_out) {
+    const int32_t n = s->n;
+    int64_t events = 0;
+    for (int32_t st = 0; st < steps; ++st) {
+        const float* zs = z + (int64_t)st * n;
+        const float* us = u ? u + (int64_t)st * n : NULL;
+        const float t = fadd(*s->t, dt);
+        *s->t = t;
+        int64_t cnt = 0;
+#pragma omp parallel for schedule(static) reduction(+ : cnt)
+        for (int32_t i = 0; i < n; ++i) {
+            const float ib = fadd(s->i_bg[i], fadd(fmul(s->ou_f1[i], fsub(s->ou_mean[i], s->i_bg[i])),
+                                                   fmul(s->ou_f2s[i], zs[i])));
+            s->i_bg[i] = ib;
+            const float main_part = fmul(s->neg_gL[i], fsub(s->V[i], s->V_L[i]));
+            const float cd = fadd(fadd(fadd(main_part, s->I_syn[i]), s->I_ext[i]), ib);
+            const float vn = fadd(s->V[i], fmul(s->dtC[i], cd));
+            const int not_sat = t >= fadd(s->t_last[i], s->T_ref[i]);
+            const float v = not_sat ? vn : s->V_reset[i];
+            const uint8_t a = v >= s->V_th[i];
+            s->V[i] = v < s->V_th[i] ? v : s->V_th[i];
+            s->active[i] = a;
+            uint8_t p = a;
+            if (prop_mode != 0) {
+                const uint8_t noise = us[i] < s->noise_rate[i];
+                p = prop_mode == 1 ? noise : (uint8_t)(noise | a);
+            }
+            s->prop[i] = p;
+            cnt += a;
+        }
+        int64_t ev = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : ev)
+        for (int32_t i = 0; i < n; ++i) {
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int64_t e = s->in_ptr[i]; e < s->in_ptr[i + 1]; ++e) {
+                if (s->prop[s->in_pre[e]]) {
+                    const int c = s->in_kind[e] ? 2 : 0;
+                    acc[c] += (double)s->w0[e];
+                    acc[c + 1] += (double)s->w1[e];
+                    ++ev;
+                }
+            }
+            float I[4];
+            for (int c = 0; c < 4; ++c) {
+                const int64_t k = (int64_t)c * n + i;
+                const float j = fadd(fmul(s->J[k], s->decay[k]), (float)acc[c]);
+                s->J[k] = j;
+                I[c] = fmul(fmul(s->g[k], fsub(s->Vu[k], s->V[i])), j);
+            }
+            s->I_syn[i] = fadd(fadd(fadd(I[0], I[1]), I[2]), I[3]);
+            if (s->active[i]) s->t_last[i] = t;
+        }
+        events += ev;
+        if (spikes_out) memcpy(spikes_out + (int64_t)st * n, s->active, (size_t)n);
+        if (counts_out) counts_out[st] = cnt;
+    }
+    return events;
+}
+
+/* ---- Philox4x32-10 and the regional-network edge stream ---------------- */
+static void philox(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t o0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
+        const uint32_t o1 = (uint32_t)p1;
+        const uint32_t o2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+        const uint32_t o3 = (uint32_t)p0;
+        c[0] = o0; c[1] = o1; c[2] = o2; c[3] = o3;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+/* Edges (post, k) for k < in_degree of every post, post-major, written to
+ * pre/kind/w0/w1 at index post*in_degree + k. */
+void oracle_structured_edges(int32_t n_pops, const uint32_t* pop_off, const uint32_t* pop_exc, const uint64_t* cdf,
+                             uint64_t seed, int32_t dyadic, uint32_t in_degree, uint32_t* pre, uint8_t* kind,
+                             float* w0, float* w1) {
+    const uint32_t n = pop_off[n_pops];
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t post = 0; post < (int64_t)n; ++post) {
+        int32_t lo = 0, hi = n_pops - 1;
+        while (lo < hi) {
+            const int32_t mid = (lo + hi + 1) >> 1;
+            if (pop_off[mid] <= (uint32_t)post) lo = mid; else hi = mid - 1;
+        }
+        const int32_t a = lo;
+        const uint64_t* row = cdf + (int64_t)a * n_pops;
+        for (uint32_t k = 0; k < in_degree; ++k) {
+            uint32_t c[4] = {(uint32_t)post, k, 0x5EED0001u, 0u};
+            philox(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+            int32_t b0 = 0, b1 = n_pops - 1;
+            while (b0 < b1) {
+                const int32_t mid = (b0 + b1) >> 1;
+                if ((uint64_t)c[0] < row[mid]) b1 = mid; else b0 = mid + 1;
+            }
+            const int32_t b = b0;
+            const uint32_t off = pop_off[b], size = pop_off[b + 1] - off;
+            uint32_t j;
+            if (b == a) {
+                j = off + (uint32_t)(((uint64_t)c[1] * (size - 1)) >> 32);
+                if (j >= (uint32_t)post) ++j;
+            } else {
+                j = off + (uint32_t)(((uint64_t)c[1] * size) >> 32);
+            }
+            const int64_t e = post * (int64_t)in_degree + k;
+            pre[e] = j;
+            kind[e] = (j - off) >= pop_exc[b];
+            if (dyadic) {
+                w0[e] = (float)(c[2] >> 24) * (1.0f / 256.0f);
+                w1[e] = (float)(c[3] >> 24) * (1.0f / 256.0f);
+            } else {
+                w0[e] = (float)(c[2] >> 8) * (1.0f / 16777216.0f);
+                w1[e] = (float)(c[3] >> 8) * (1.0f / 16777216.0f);
+            }
+        }
+    }
+}
+
+int32_t oracle_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

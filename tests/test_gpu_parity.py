@@ -293,3 +293,34 @@ def test_philox_noise_statistics(gpu, block10k):
     rate_ref = spikes[1000:].mean()
     rate_gpu = r.spikes[1000:].mean()
     assert abs(rate_gpu - rate_ref) / rate_ref < 0.1
+
+
+def test_exact_push_equals_pull_at_in_degree_1000(gpu):
+    """The two deterministic paths give identical trains through the active regime."""
+    spec = nw.structured_spec(200_000, 20, 1000, seed=2)
+    res = []
+    for syn in (E.SYN_PUSH_EXACT, E.SYN_PULL):
+        with E.Engine.structured(spec, pull=True, seed=77) as eng:
+            r = eng.run(700, record_spikes=True, syn_mode=syn)
+            res.append((r.spikes, eng.read_state(E.STATE_V), r.events))
+    assert res[0][0][400:].mean() > 0.005          # the network is active
+    assert first_divergence(res[0][0], res[1][0]) is None
+    assert np.array_equal(res[0][1], res[1][1])
+    assert res[0][2] == res[1][2]
+
+
+def test_large_in_degree_against_c_oracle(gpu):
+    """In-degree 1000 through the active regime, bit-exact against the C oracle."""
+    from oracle import c_oracle as cc
+    spec = nw.structured_spec(30_000, 10, 1000, seed=3)
+    net = cc.structured_edges(spec)
+    steps = 600
+    z, _ = lo.torch_noise_stream(9, spec.n, steps, False)
+    orc = cc.COracle(net)
+    sp, counts, _ = orc.run(z)
+    assert sp[400:].mean() > 0.005
+    with E.Engine.structured(spec, pull=True) as eng:
+        eng.set_noise_injected(z)
+        r = eng.run(steps, record_spikes=True, syn_mode=E.SYN_PULL)
+        assert first_divergence(r.spikes, sp) is None
+        assert np.array_equal(eng.read_state(E.STATE_V), orc.V)
