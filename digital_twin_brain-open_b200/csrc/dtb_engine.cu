@@ -599,7 +599,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
         DTB_TRY(begin_run_chunk(steps, rows, freq || vmean));
         ++launches;
         std::vector<std::pair<int, size_t>> timed;   // (kernel class, event pair index)
-        if (time_k) DTB_TRY(ensure_timing_events(2 * rows + 2));
+        if (time_k) DTB_TRY(ensure_timing_events(4 * static_cast<size_t>(rows) + 4));   // 2 events x (2 launches per step + 1)
         auto timed_launch = [&](int cls, auto&& fn) -> int {
             if (time_k) DTB_CU(cudaEventRecord(tev[2 * timed.size()], stream));
             DTB_CU(fn());
