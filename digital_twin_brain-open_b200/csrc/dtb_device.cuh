@@ -108,7 +108,8 @@ struct NetView {
     int* hist_cnt;                 // [hist_cap * n_pops]
     long long* hist_vsum;          // [hist_cap * n_pops] fixed point, scale 2^24
     unsigned long long* events;    // cumulative synaptic events
-    uint32_t* ticket;              // last-CTA counter of the LIF kernel
+    uint32_t* ticket;              // last-tile counter of the per-step kernels
+    const uint32_t* tile_pop;      // [lif_tiles] population of each LIF tile's first neuron
     uint32_t lif_tiles;
     uint32_t pad1;
 };

@@ -192,6 +192,7 @@ int Engine::refresh_view() {
     v.events = events;
     v.ticket = ticket;
     v.lif_tiles = n_pad / kLifTile;
+    v.tile_pop = tile_pop;
     view = v;
     DTB_CU(cudaMemcpyAsync(view_dev, &view, sizeof(NetView), cudaMemcpyHostToDevice, stream));
     DTB_CU(cudaStreamSynchronize(stream));
@@ -208,6 +209,7 @@ LaunchBatch Engine::single_batch() const {
     b.lif_tiles_total = n_pad / kLifTile;
     b.pull_tiles_total = n_pad / kPullTile;
     b.push_ctas = static_cast<uint32_t>(sm_count) * 8u;
+    b.lif_ctas = static_cast<uint32_t>(sm_count) * lif_ctas_per_sm;
     b.spikes = SpikeList{list, list_count, list_ticket, n_pad};
     return b;
 }
@@ -231,6 +233,19 @@ static int alloc_core(Engine& e) {
     DTB_TRY(e.dalloc(e.list, e.n_pad, false));
     DTB_TRY(e.dalloc(e.list_count, 1));
     DTB_TRY(e.dalloc(e.list_ticket, 1));
+    {
+        // population of the first neuron of every 1024-neuron LIF tile
+        const uint32_t tiles = e.n_pad / kLifTile;
+        std::vector<uint32_t> tp(tiles);
+        uint32_t p = 0;
+        for (uint32_t t = 0; t < tiles; ++t) {
+            const uint32_t i = std::min(t * static_cast<uint32_t>(kLifTile), e.n - 1);
+            while (p + 1 < e.P && e.pop_off[p + 1] <= i) ++p;
+            tp[t] = p;
+        }
+        DTB_TRY(e.dalloc(e.tile_pop, tiles));
+        DTB_CU(cudaMemcpyAsync(e.tile_pop, tp.data(), sizeof(uint32_t) * tiles, cudaMemcpyHostToDevice, e.stream));
+    }
     const uint32_t pre[6] = {0u, e.n_pad / kLifTile, 0u, e.n_pad / kPullTile, 0u, e.n_pad};
     DTB_CU(cudaMemcpyAsync(e.prefix_dev, pre, sizeof(pre), cudaMemcpyHostToDevice, e.stream));
     DTB_CU(cudaMemcpyAsync(e.pop_off_dev, e.pop_off.data(), sizeof(uint32_t) * (e.P + 1), cudaMemcpyHostToDevice, e.stream));

@@ -115,6 +115,8 @@ public:
     uint32_t* list = nullptr;
     uint32_t* list_count = nullptr;
     uint32_t* list_ticket = nullptr;
+    uint32_t* tile_pop = nullptr;
+    uint32_t lif_ctas_per_sm = 2;
     NetView view{};
 
     // pinned staging for the statistics

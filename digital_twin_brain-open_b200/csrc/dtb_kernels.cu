@@ -18,6 +18,8 @@
 // A launch covers a batch of networks (one for the plain path).  CTA -> network is
 // a binary search over the batch's tile prefix; every network keeps its own clock,
 // and the last CTA of a network to finish (ticket counter) advances that clock.
+#include <algorithm>
+
 #include "dtb_device.cuh"
 #include "dtb_kernels.h"
 
@@ -25,6 +27,15 @@ namespace dtb {
 
 constexpr int kStatSlots = 32;
 constexpr int kPushThreads = 256;
+constexpr int kPushUnroll = 8;
+
+// Fire-and-forget reductions (no returned value, so no scoreboard wait).
+__device__ __forceinline__ void red_add_f32x2(float2* addr, float2 v) {
+    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" :: "l"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
+__device__ __forceinline__ void red_add_u64(unsigned long long* addr, unsigned long long v) {
+    asm volatile("red.global.add.u64 [%0], %1;" :: "l"(addr), "l"(v) : "memory");
+}
 
 __device__ inline uint32_t find_net(const uint32_t* __restrict__ prefix, uint32_t n_nets, uint32_t x) {
     uint32_t lo = 0, hi = n_nets - 1;
@@ -176,216 +187,215 @@ __device__ inline void advance_clock(const NetView& nv, uint32_t tiles, float t,
 }
 
 // ---------------------------------------------------------------------------
-// Fused LIF step (push and exact-push modes)
+// Fused LIF step (push and exact-push modes): a persistent grid walks the
+// batch's 1024-neuron tiles.  Per tile, every thread issues its state loads
+// first (V, i_ou, t_last, J, noise draws), then steps its 4 neurons.
 // ---------------------------------------------------------------------------
 template <int JM>
-__global__ void __launch_bounds__(kLifThreads)
+__global__ void __launch_bounds__(kLifThreads, 2)
 lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_prefix,
-           const uint32_t* __restrict__ vbase, uint32_t n_nets, SpikeList sl, uint32_t flags, int prop_mode) {
+           const uint32_t* __restrict__ vbase, uint32_t n_nets, uint32_t total_tiles, SpikeList sl, uint32_t flags,
+           int prop_mode) {
     __shared__ NetView s_nv;
-    __shared__ uint32_t s_net, s_tile, s_p0, s_base;
+    __shared__ uint32_t s_base;
     __shared__ uint32_t s_warp[kLifThreads / 32];
     __shared__ unsigned long long s_events;
     __shared__ int s_cnt[kStatSlots];
     __shared__ long long s_vs[kStatSlots];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) {
-        const uint32_t k = n_nets > 1 ? find_net(tile_prefix, n_nets, blockIdx.x) : 0u;
-        s_net = k;
-        s_tile = blockIdx.x - __ldg(tile_prefix + k);
-        s_events = 0ull;
-    }
-    if (tid < kStatSlots) { s_cnt[tid] = 0; s_vs[tid] = 0; }
-    __syncthreads();
-    load_netview(s_nv, nets + s_net);
-    __syncthreads();
-    const NetView& nv = s_nv;
-
-    const float t_prev = nv.clock->t;
-    const unsigned long long n_prev = nv.clock->n;
-    const unsigned long long run_base = nv.clock->run_base;
-    const unsigned long long inj_base = nv.clock->inj_base;
-    const unsigned long long n = n_prev + 1;
-    const float t = __fadd_rn(t_prev, nv.dt);
-    const uint32_t parity = static_cast<uint32_t>(n & 1ull);
-    const uint32_t tile_first = s_tile * kLifTile;
-    const uint32_t i0 = tile_first + tid * 4;
-    uint32_t err = 0;
-
-    const long long row = static_cast<long long>(n - run_base - 1);
-    bool stats = (flags & kFlagStats) != 0;
-    bool record = (flags & kFlagRecord) != 0 && nv.rec_bits != nullptr;
-    if ((stats || record) && (row < 0 || row >= static_cast<long long>(nv.hist_cap))) {
-        stats = false; record = false; err |= kErrHistOverflow;
-    }
-    if (tid == 0) s_p0 = find_pop(nv.pop_off, nv.n_pops, min(tile_first, nv.n - 1));
-    __syncthreads();
-    StatAcc sa{s_cnt, s_vs, s_p0};
-
-    // ---- state loads: 128-bit per array, 4 neurons per thread
-    float4 V4 = *reinterpret_cast<const float4*>(nv.V + i0);
-    float4 I4 = *reinterpret_cast<const float4*>(nv.iou + i0);
-    float4 T4 = *reinterpret_cast<const float4*>(nv.tlast + i0);
-    float4 J4[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) J4[k] = nv.J[i0 + k];
-    longlong2 D[8];
-    if constexpr (JM == J_FOLD) {
-        const longlong2* dsrc = reinterpret_cast<const longlong2*>(nv.dJ + static_cast<size_t>(i0) * 4);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) D[k] = dsrc[k];
-    }
+    uint32_t cur_net = 0xFFFFFFFFu;
     const bool use_ou = (flags & kFlagUseOU) != 0;
     const bool need_u = prop_mode != PROP_THRESHOLD;
-    float z[4], u[4] = {1.f, 1.f, 1.f, 1.f};
-    draw_noise(nv, i0, n, inj_base, (flags & kFlagInjected) != 0, need_u, z, u, err);
+    const bool injected = (flags & kFlagInjected) != 0;
 
-    float* Vv = reinterpret_cast<float*>(&V4);
-    float* Iv = reinterpret_cast<float*>(&I4);
-    float* Tv = reinterpret_cast<float*>(&T4);
-    uint32_t nib_prop = 0, nib_act = 0;
-    unsigned long long ev = 0;
-
-    uint32_t p = find_pop(nv.pop_off, nv.n_pops, min(i0, nv.n - 1));
-    uint32_t p_first = p;
-    bool uniform = true;
-    int cnt_acc = 0;
-    long long vs_acc = 0;
-    PopParams pp;
-    load_pop_params(nv, p, i0, pp);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const uint32_t i = i0 + k;
-        if (i >= nv.n) { uniform = false; continue; }
-        if (!nv.per_neuron) {
-            if (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) {
-                while (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) ++p;
-                load_pop_params(nv, p, i, pp);
-                uniform = false;
-            }
-        } else {
-            if (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) {
-                while (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) ++p;
-                uniform = false;
-            }
-            if (k > 0) load_pop_params(nv, p, i, pp);
+    for (uint32_t gt = blockIdx.x; gt < total_tiles; gt += gridDim.x) {
+        const uint32_t net = n_nets > 1 ? find_net(tile_prefix, n_nets, gt) : 0u;
+        if (net != cur_net) {
+            __syncthreads();
+            load_netview(s_nv, nets + net);
+            cur_net = net;
         }
-        float* Jk = reinterpret_cast<float*>(&J4[k]);
-        NeuronIn in;
-        in.V = Vv[k];
-        in.iou = Iv[k];
-        in.tlast = Tv[k];
+        if (tid < kStatSlots) { s_cnt[tid] = 0; s_vs[tid] = 0; }
+        if (tid == 0) s_events = 0ull;
+        __syncthreads();
+        const NetView& nv = s_nv;
+        const uint32_t tile = gt - __ldg(tile_prefix + net);
+        const uint32_t tile_first = tile * kLifTile;
+        const uint32_t i0 = tile_first + tid * 4;
+
+        // ---- state loads first: 128-bit per array, 4 neurons per thread
+        float4 V4 = *reinterpret_cast<const float4*>(nv.V + i0);
+        float4 I4 = *reinterpret_cast<const float4*>(nv.iou + i0);
+        float4 T4 = *reinterpret_cast<const float4*>(nv.tlast + i0);
+        float4 J4[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) J4[k] = nv.J[i0 + k];
+        longlong2 D[8];
         if constexpr (JM == J_FOLD) {
-            const long long* dk = reinterpret_cast<const long long*>(&D[2 * k]);
+            const longlong2* dsrc = reinterpret_cast<const longlong2*>(nv.dJ + static_cast<size_t>(i0) * 4);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) in.J[c] = decay_add(Jk[c], pp.decay[c], fix_to_float(dk[c]));
-        } else {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) in.J[c] = Jk[c];
+            for (int k = 0; k < 8; ++k) D[k] = dsrc[k];
         }
-        const NeuronOut o = lif_update(pp, in, t, z[k], use_ou);
-        Vv[k] = o.V;
-        Iv[k] = o.iou;
-        Tv[k] = o.tlast;
-        if constexpr (JM == J_DIRECT) {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) Jk[c] = __fmul_rn(in.J[c], pp.decay[c]);
-        } else if constexpr (JM == J_FOLD) {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) Jk[c] = in.J[c];
+        const float t_prev = nv.clock->t;
+        const unsigned long long n_prev = nv.clock->n;
+        const unsigned long long run_base = nv.clock->run_base;
+        const unsigned long long inj_base = nv.clock->inj_base;
+        const uint32_t p_tile = __ldg(nv.tile_pop + tile);
+        const unsigned long long n = n_prev + 1;
+        const float t = __fadd_rn(t_prev, nv.dt);
+        const uint32_t parity = static_cast<uint32_t>(n & 1ull);
+        uint32_t err = 0;
+        const long long row = static_cast<long long>(n - run_base - 1);
+        bool stats = (flags & kFlagStats) != 0;
+        bool record = (flags & kFlagRecord) != 0 && nv.rec_bits != nullptr;
+        if ((stats || record) && (row < 0 || row >= static_cast<long long>(nv.hist_cap))) {
+            stats = false; record = false; err |= kErrHistOverflow;
         }
-        const bool sp = propagated(prop_mode, o.active, u[k], pp.noise_rate);
-        nib_prop |= static_cast<uint32_t>(sp) << k;
-        nib_act |= static_cast<uint32_t>(o.active) << k;
-        if (sp) ev += __ldg(nv.out_deg + i);
-        if (stats) {
-            if (excluded(nv, i)) { uniform = false; continue; }
-            if (p == p_first) {
-                cnt_acc += o.active;
-                vs_acc += v_fix(o.V);
+        StatAcc sa{s_cnt, s_vs, p_tile};
+        float z[4], u[4] = {1.f, 1.f, 1.f, 1.f};
+        draw_noise(nv, i0, n, inj_base, injected, need_u, z, u, err);
+
+        float* Vv = reinterpret_cast<float*>(&V4);
+        float* Iv = reinterpret_cast<float*>(&I4);
+        float* Tv = reinterpret_cast<float*>(&T4);
+        uint32_t nib_prop = 0, nib_act = 0;
+        unsigned long long ev = 0;
+        uint32_t p = p_tile;
+        const uint32_t i_first = min(i0, nv.n - 1);
+        while (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i_first) ++p;
+        const uint32_t p_first = p;
+        bool uniform = true;
+        int cnt_acc = 0;
+        long long vs_acc = 0;
+        PopParams pp;
+        load_pop_params(nv, p, i_first, pp);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t i = i0 + k;
+            if (i >= nv.n) { uniform = false; continue; }
+            if (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) {
+                while (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) ++p;
+                uniform = false;
+                if (!nv.per_neuron) load_pop_params(nv, p, i, pp);
+            }
+            if (nv.per_neuron && k > 0) load_pop_params(nv, p, i, pp);
+            float* Jk = reinterpret_cast<float*>(&J4[k]);
+            NeuronIn in;
+            in.V = Vv[k];
+            in.iou = Iv[k];
+            in.tlast = Tv[k];
+            if constexpr (JM == J_FOLD) {
+                const long long* dk = reinterpret_cast<const long long*>(&D[2 * k]);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) in.J[c] = decay_add(Jk[c], pp.decay[c], fix_to_float(dk[c]));
             } else {
-                stat_add(nv, sa, row, p, o.active, v_fix(o.V));
+#pragma unroll
+                for (int c = 0; c < 4; ++c) in.J[c] = Jk[c];
+            }
+            const NeuronOut o = lif_update(pp, in, t, z[k], use_ou);
+            Vv[k] = o.V;
+            Iv[k] = o.iou;
+            Tv[k] = o.tlast;
+            if constexpr (JM == J_DIRECT) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) Jk[c] = __fmul_rn(in.J[c], pp.decay[c]);
+            } else if constexpr (JM == J_FOLD) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) Jk[c] = in.J[c];
+            }
+            const bool sp = propagated(prop_mode, o.active, u[k], pp.noise_rate);
+            nib_prop |= static_cast<uint32_t>(sp) << k;
+            nib_act |= static_cast<uint32_t>(o.active) << k;
+            if (sp) ev += __ldg(nv.out_deg + i);
+            if (stats) {
+                if (excluded(nv, i)) { uniform = false; continue; }
+                if (p == p_first) {
+                    cnt_acc += o.active;
+                    vs_acc += v_fix(o.V);
+                } else {
+                    stat_add(nv, sa, row, p, o.active, v_fix(o.V));
+                }
             }
         }
-    }
 
-    // ---- state stores
-    *reinterpret_cast<float4*>(nv.V + i0) = V4;
-    *reinterpret_cast<float4*>(nv.iou + i0) = I4;
-    *reinterpret_cast<float4*>(nv.tlast + i0) = T4;
-    if constexpr (JM != J_ASIS) {
+        // ---- state stores
+        *reinterpret_cast<float4*>(nv.V + i0) = V4;
+        *reinterpret_cast<float4*>(nv.iou + i0) = I4;
+        *reinterpret_cast<float4*>(nv.tlast + i0) = T4;
+        if constexpr (JM != J_ASIS) {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) nv.J[i0 + k] = J4[k];
-    }
-    if constexpr (JM == J_FOLD) {
-        longlong2* ddst = reinterpret_cast<longlong2*>(nv.dJ + static_cast<size_t>(i0) * 4);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) ddst[k] = make_longlong2(0, 0);
-    }
-
-    // ---- spike bitmaps (propagated: parity buffer; threshold: history row)
-    {
-        const uint32_t wprop = nibbles_to_word(nib_prop, lane);
-        const uint32_t wact = nibbles_to_word(nib_act, lane);
-        if ((lane & 7) == 0) {
-            const uint32_t word = (i0 >> 5);   // lane 8w holds neurons 32w.. of this warp
-            uint32_t* bits = parity ? nv.bits1 : nv.bits0;
-            bits[word] = wprop;
-            if (record) nv.rec_bits[static_cast<size_t>(row) * nv.n_words + word] = wact;
+            for (int k = 0; k < 4; ++k) nv.J[i0 + k] = J4[k];
         }
-    }
-
-    // ---- population statistics: warp-uniform fast path, else per-thread slots
-    if (stats) {
-        const uint32_t pl = __shfl_sync(0xffffffffu, p_first, 0);
-        const bool wuni = __all_sync(0xffffffffu, uniform && p_first == pl);
-        if (wuni) {
-            const int c = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(cnt_acc));
-            const long long v = warp_sum_ll(vs_acc);
-            if (lane == 0) stat_add(nv, sa, row, pl, c, v);
-        } else if (i0 < nv.n) {
-            stat_add(nv, sa, row, p_first, cnt_acc, vs_acc);
+        if constexpr (JM == J_FOLD) {
+            longlong2* ddst = reinterpret_cast<longlong2*>(nv.dJ + static_cast<size_t>(i0) * 4);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) ddst[k] = make_longlong2(0, 0);
         }
-    }
 
-    // ---- spike list (push modes): CTA-aggregated, ascending within the CTA
-    const uint32_t my_cnt = __popc(nib_prop);
-    uint32_t incl = my_cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-    }
-    if (lane == 31) s_warp[warp] = incl;
-    const unsigned long long wev = warp_sum_ull(ev);
-    if (lane == 0 && wev) atomicAdd(&s_events, wev);
-    __syncthreads();
-    if (tid == 0) {
-        uint32_t total = 0;
-#pragma unroll
-        for (int w = 0; w < kLifThreads / 32; ++w) { const uint32_t c = s_warp[w]; s_warp[w] = total; total += c; }
-        s_base = ((flags & kFlagList) && total) ? atomicAdd(sl.count, total) : 0u;
-        if (s_events) atomicAdd(nv.events, s_events);
-    }
-    __syncthreads();
-    if ((flags & kFlagList) && my_cnt) {
-        uint32_t pos = s_base + s_warp[warp] + incl - my_cnt;
-        const uint32_t vb = __ldg(vbase + s_net);
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-            if ((nib_prop >> k) & 1u) sl.list[pos++] = vb + i0 + k;
-    }
-    if (stats && tid < kStatSlots) {
-        const int c = s_cnt[tid];
-        const long long v = s_vs[tid];
-        if (c || v) {
-            const size_t o = static_cast<size_t>(row) * nv.n_pops + (s_p0 + tid);
-            if (c) atomicAdd(nv.hist_cnt + o, c);
-            atomicAdd(reinterpret_cast<unsigned long long*>(nv.hist_vsum + o), static_cast<unsigned long long>(v));
+        // ---- spike bitmaps (propagated: parity buffer; threshold: history row)
+        {
+            const uint32_t wprop = nibbles_to_word(nib_prop, lane);
+            const uint32_t wact = nibbles_to_word(nib_act, lane);
+            if ((lane & 7) == 0) {
+                const uint32_t word = (i0 >> 5);
+                uint32_t* bits = parity ? nv.bits1 : nv.bits0;
+                bits[word] = wprop;
+                if (record) nv.rec_bits[static_cast<size_t>(row) * nv.n_words + word] = wact;
+            }
         }
+
+        // ---- population statistics: warp-uniform fast path, else per-thread slots
+        if (stats) {
+            const uint32_t pl = __shfl_sync(0xffffffffu, p_first, 0);
+            const bool wuni = __all_sync(0xffffffffu, uniform && p_first == pl);
+            if (wuni) {
+                const int c = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(cnt_acc));
+                const long long v = warp_sum_ll(vs_acc);
+                if (lane == 0) stat_add(nv, sa, row, pl, c, v);
+            } else if (i0 < nv.n) {
+                stat_add(nv, sa, row, p_first, cnt_acc, vs_acc);
+            }
+        }
+
+        // ---- spike list (push modes): CTA-aggregated, ascending within the tile
+        const uint32_t my_cnt = __popc(nib_prop);
+        uint32_t incl = my_cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_warp[warp] = incl;
+        const unsigned long long wev = warp_sum_ull(ev);
+        if (lane == 0 && wev) atomicAdd(&s_events, wev);
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t total = 0;
+#pragma unroll
+            for (int w = 0; w < kLifThreads / 32; ++w) { const uint32_t c = s_warp[w]; s_warp[w] = total; total += c; }
+            s_base = ((flags & kFlagList) && total) ? atomicAdd(sl.count, total) : 0u;
+            if (s_events) atomicAdd(nv.events, s_events);
+        }
+        __syncthreads();
+        if ((flags & kFlagList) && my_cnt) {
+            uint32_t pos = s_base + s_warp[warp] + incl - my_cnt;
+            const uint32_t vb = __ldg(vbase + net);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if ((nib_prop >> k) & 1u) sl.list[pos++] = vb + i0 + k;
+        }
+        if (stats && tid < kStatSlots) {
+            const int c = s_cnt[tid];
+            const long long v = s_vs[tid];
+            if (c || v) {
+                const size_t o = static_cast<size_t>(row) * nv.n_pops + (p_tile + tid);
+                if (c) atomicAdd(nv.hist_cnt + o, c);
+                atomicAdd(reinterpret_cast<unsigned long long*>(nv.hist_vsum + o), static_cast<unsigned long long>(v));
+            }
+        }
+        advance_clock(nv, nv.lif_tiles, t, n, err);
     }
-    advance_clock(nv, nv.lif_tiles, t, n, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -417,11 +427,11 @@ push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase
         }
         const uint32_t j = v - vb;
         const unsigned long long beg = __ldg(ptr + j), end = __ldg(ptr + j + 1);
-        for (unsigned long long e = beg + lane; e < end; e += 128) {
-            uint32_t c[4];
-            float2 w[4];
+        for (unsigned long long e = beg + lane; e < end; e += 32ull * kPushUnroll) {
+            uint32_t c[kPushUnroll];
+            float2 w[kPushUnroll];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < kPushUnroll; ++q) {
                 const unsigned long long idx = e + 32ull * q;
                 if (idx < end) {
                     c[q] = __ldcs(col + idx);
@@ -429,17 +439,17 @@ push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase
                 }
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < kPushUnroll; ++q) {
                 const unsigned long long idx = e + 32ull * q;
                 if (idx < end) {
                     const uint32_t target = c[q] & kIndexMask;
                     const uint32_t kind = c[q] >> 31;
                     if constexpr (ACC == 0) {
-                        atomicAdd(reinterpret_cast<float2*>(J + target) + kind, w[q]);
+                        red_add_f32x2(reinterpret_cast<float2*>(J + target) + kind, w[q]);
                     } else {
                         unsigned long long* d = reinterpret_cast<unsigned long long*>(dJ) + static_cast<size_t>(target) * 4 + 2 * kind;
-                        atomicAdd(d, static_cast<unsigned long long>(float_to_fix(w[q].x)));
-                        atomicAdd(d + 1, static_cast<unsigned long long>(float_to_fix(w[q].y)));
+                        red_add_u64(d, static_cast<unsigned long long>(float_to_fix(w[q].x)));
+                        red_add_u64(d + 1, static_cast<unsigned long long>(float_to_fix(w[q].y)));
                     }
                 }
             }
@@ -672,11 +682,12 @@ gather_finish_kernel(const NetView* __restrict__ nets, const uint32_t* __restric
 // ---------------------------------------------------------------------------
 cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop_mode, cudaStream_t s) {
     if (b.lif_tiles_total == 0) return cudaSuccess;
-    const dim3 grid(b.lif_tiles_total), block(kLifThreads);
+    const dim3 grid(std::min(b.lif_tiles_total, b.lif_ctas)), block(kLifThreads);
+    const uint32_t T = b.lif_tiles_total;
     switch (jmode) {
-        case J_DIRECT: lif_kernel<J_DIRECT><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, b.spikes, flags, prop_mode); break;
-        case J_FOLD: lif_kernel<J_FOLD><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, b.spikes, flags, prop_mode); break;
-        default: lif_kernel<J_ASIS><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, b.spikes, flags, prop_mode); break;
+        case J_DIRECT: lif_kernel<J_DIRECT><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode); break;
+        case J_FOLD: lif_kernel<J_FOLD><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode); break;
+        default: lif_kernel<J_ASIS><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode); break;
     }
     return cudaGetLastError();
 }

@@ -18,6 +18,7 @@ struct LaunchBatch {
     uint32_t lif_tiles_total;
     uint32_t pull_tiles_total;
     uint32_t push_ctas;
+    uint32_t lif_ctas;            // persistent grid of the LIF kernel
     SpikeList spikes;
 };
 
