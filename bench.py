@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--neurons", type=int, default=N_NEURONS, help="network size (profiling runs use a small one)")
     p.add_argument("--pops", type=int, default=N_POPS)
     p.add_argument("--degree", type=int, default=IN_DEGREE)
+    p.add_argument("--push", default="auto", help="push kernel: auto (autotuned), reg:4|8|16, tma:256|512")
     return p.parse_args()
 
 
@@ -179,6 +180,9 @@ def run_ours(args):
     t0 = time.perf_counter()
     eng = E.Engine.structured(spec, weight_type=wt, seed=1000 + rank)
     build_s = time.perf_counter() - t0
+    if args.push != "auto":
+        kind, param = args.push.split(":")
+        eng.set_push_variant({"reg": 0, "tma": 1}[kind], int(param))
     info = eng.info()
     stream = torch.cuda.ExternalStream(eng.stream(), device=dev)
     P = eng.n_pops
@@ -213,6 +217,8 @@ def run_ours(args):
     clocks = sampler.stop()
     ms = start.elapsed_time(end)
 
+    info = eng.info()
+    tuning = [{"kernel": ("reg" if k == 0 else "tma"), "param": p, "ms": m} for k, p, m in eng.tuning_report()]
     # per-kernel timing window (after the timed region)
     rk = eng.run(WINDOW, freq=True, out=(fr, None), time_kernels=True)
     lif_ms, push_ms = rk.kernel_ms[0] / WINDOW, rk.kernel_ms[1] / WINDOW
@@ -284,6 +290,8 @@ def run_ours(args):
                              f"{info.n_neurons * 56 / 1e6:.0f} MB neuron state)",
                        "device_bytes": int(info.device_bytes), "build_s": build_s,
                        "lif_ms_per_step": lif_ms, "push_ms_per_step": push_ms,
+                       "push_variant": ("reg" if info.push_kind == 0 else "tma") + f":{info.push_param}",
+                       "push_autotune": tuning,
                        "step_roofline_frac": step_bytes / ((lif_ms + push_ms) * 1e-3) / 1e9 / peak},
             "roofline": {"bound": "hbm", "kernel": "push_kernel", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,

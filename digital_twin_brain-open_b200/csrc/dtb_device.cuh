@@ -42,6 +42,7 @@ constexpr uint32_t kStreamGamma = 0x0D0E0003u;
 constexpr uint32_t kErrHistOverflow = 1u;
 constexpr uint32_t kErrNoiseExhausted = 2u;
 constexpr uint32_t kErrIndex = 4u;
+constexpr uint32_t kErrTimeout = 8u;      // a bounded wait gave up
 
 enum JMode : int { J_DIRECT = 0, J_FOLD = 1, J_ASIS = 2 };
 enum WType : int { W_F32 = 0, W_BF16 = 1, W_F16 = 2, W_U8 = 3 };

@@ -29,6 +29,10 @@ int cuda_fail(cudaError_t e, const char* what) {
 }
 
 __global__ void set_u64_kernel(unsigned long long* p, unsigned long long v) { *p = v; }
+__global__ void set_u32_kernel(uint32_t* p, uint32_t v) { *p = v; }
+
+static constexpr size_t kCsrPadWords = 16;   // 64 bytes after every CSR array
+static constexpr size_t kCsrPadBytes = 64;
 __global__ void set_clock_kernel(Clock* c, float t, unsigned long long n) {
     c->t = t;
     c->n = n;
@@ -46,6 +50,8 @@ Engine::~Engine() {
     if (h_cnt) cudaFreeHost(h_cnt);
     if (h_vsum) cudaFreeHost(h_vsum);
     for (cudaEvent_t e : tev) cudaEventDestroy(e);
+    if (tune_ev[0]) cudaEventDestroy(tune_ev[0]);
+    if (tune_ev[1]) cudaEventDestroy(tune_ev[1]);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -308,9 +314,9 @@ int Engine::upload_csr_host(const uint32_t* pre, const uint32_t* post, const uin
             encode_weight(w, in_type, e, wtype, wt.data(), q);
         }
         DTB_TRY(dalloc(d_ptr, static_cast<size_t>(n) + 1, false));
-        DTB_TRY(dalloc(d_col, n_edges, false));
+        DTB_TRY(dalloc(d_col, n_edges + kCsrPadWords));
         uint8_t* wdev = nullptr;
-        DTB_TRY(dalloc(wdev, static_cast<size_t>(n_edges) * wb, false));
+        DTB_TRY(dalloc(wdev, static_cast<size_t>(n_edges) * wb + kCsrPadBytes));
         d_w = wdev;
         DTB_CU(cudaMemcpyAsync(d_ptr, ptr.data(), sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, stream));
         DTB_CU(cudaMemcpyAsync(d_col, col.data(), sizeof(uint32_t) * n_edges, cudaMemcpyHostToDevice, stream));
@@ -420,17 +426,17 @@ int Engine::create_structured(const dtb_structured_spec& s, const dtb_options& o
     const int wb = weight_bytes();
     if (opt.build_push) {
         DTB_TRY(dalloc(out_ptr, static_cast<size_t>(n) + 1, false));
-        DTB_TRY(dalloc(out_col, n_edges, false));
+        DTB_TRY(dalloc(out_col, n_edges + kCsrPadWords, false));
         uint8_t* w = nullptr;
-        DTB_TRY(dalloc(w, static_cast<size_t>(n_edges) * wb, false));
+        DTB_TRY(dalloc(w, static_cast<size_t>(n_edges) * wb + kCsrPadBytes, false));
         out_w = w;
         has_push = true;
     }
     if (opt.build_pull) {
         DTB_TRY(dalloc(in_ptr, static_cast<size_t>(n) + 1, false));
-        DTB_TRY(dalloc(in_col, n_edges, false));
+        DTB_TRY(dalloc(in_col, n_edges + kCsrPadWords, false));
         uint8_t* w = nullptr;
-        DTB_TRY(dalloc(w, static_cast<size_t>(n_edges) * wb, false));
+        DTB_TRY(dalloc(w, static_cast<size_t>(n_edges) * wb + kCsrPadBytes, false));
         in_w = w;
         has_pull = true;
     }
@@ -603,6 +609,16 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     const LaunchBatch b = single_batch();
     const int pm = static_cast<int>(rq.prop_mode);
     const bool time_k = (rq.flags & DTB_RUN_TIME_KERNELS) != 0;
+    const int exact = rq.syn_mode == DTB_SYN_PUSH_EXACT ? 1 : 0;
+    uint64_t tune_at = ~0ull;   // run-relative step at which the push variants are timed
+    if (rq.syn_mode != DTB_SYN_PULL) {
+        DTB_CU(push_prepare(exact, static_cast<int>(wtype), push_cfg, sm_count, &push_ctas));
+        if (autotune && !push_tuned[exact]) {
+            // time the variants on a live spike list, once the network has left its quiet start
+            const uint64_t settle = 300;
+            tune_at = steps >= settle ? 1 : (settle - steps < rq.iters ? settle - steps : ~0ull);
+        }
+    }
     set_u64_kernel<<<1, 1, 0, stream>>>(events, 0ull);
     DTB_CU(cudaGetLastError());
     uint32_t launches = 1;
@@ -631,11 +647,13 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
             switch (rq.syn_mode) {
                 case DTB_SYN_PUSH:
                     DTB_TRY(timed_launch(0, [&] { return launch_lif(b, J_DIRECT, kflags, pm, stream); }));
-                    DTB_TRY(timed_launch(1, [&] { return launch_push(b, 0, static_cast<int>(wtype), stream); }));
+                    if (tune_at == done + s) DTB_TRY(tune_push(b, 0));
+                    DTB_TRY(timed_launch(1, [&] { return launch_push(b, 0, static_cast<int>(wtype), push_cfg, push_ctas, stream); }));
                     break;
                 case DTB_SYN_PUSH_EXACT:
                     DTB_TRY(timed_launch(0, [&] { return launch_lif(b, first ? J_ASIS : J_FOLD, kflags, pm, stream); }));
-                    DTB_TRY(timed_launch(1, [&] { return launch_push(b, 1, static_cast<int>(wtype), stream); }));
+                    if (tune_at == done + s) DTB_TRY(tune_push(b, 1));
+                    DTB_TRY(timed_launch(1, [&] { return launch_push(b, 1, static_cast<int>(wtype), push_cfg, push_ctas, stream); }));
                     break;
                 default:
                     DTB_TRY(timed_launch(2, [&] { return launch_pull(b, first ? 0 : 1, static_cast<int>(wtype), kflags, pm, stream); }));
@@ -684,6 +702,70 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     return DTB_OK;
 }
 
+// Time every push variant on the spike list the LIF kernel just wrote, into a
+// scratch accumulator so the simulation state is untouched, and keep the fastest.
+int Engine::tune_push(const LaunchBatch& b, int exact) {
+    uint32_t count = 0;
+    DTB_CU(cudaMemcpyAsync(&count, list_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    DTB_CU(cudaStreamSynchronize(stream));
+    if (count < std::max<uint32_t>(64u, n / 5000u)) return DTB_OK;   // too quiet to be representative
+    void* scratch = nullptr;
+    NetView* tview = nullptr;
+    const size_t sbytes = exact ? sizeof(long long) * 4 * n_pad : sizeof(float4) * n_pad;
+    DTB_CU(cudaMalloc(&scratch, sbytes));
+    if (cudaMalloc(reinterpret_cast<void**>(&tview), sizeof(NetView)) != cudaSuccess) {
+        cudaFree(scratch);
+        return cuda_fail(cudaErrorMemoryAllocation, "tune_push");
+    }
+    NetView v = view;
+    if (exact) v.dJ = static_cast<long long*>(scratch); else v.J = static_cast<float4*>(scratch);
+    int st = DTB_OK;
+    const PushCfg cands[] = {{PUSH_REG, 4}, {PUSH_REG, 8}, {PUSH_REG, 16}, {PUSH_TMA, 256}, {PUSH_TMA, 512}};
+    PushCfg best = push_cfg;
+    float best_ms = 1e30f;
+    tune_report.clear();
+    auto body = [&]() -> int {
+        DTB_CU(cudaMemcpyAsync(tview, &v, sizeof(NetView), cudaMemcpyHostToDevice, stream));
+        DTB_CU(cudaMemsetAsync(scratch, 0, sbytes, stream));
+        LaunchBatch tb = b;
+        tb.nets = tview;
+        if (!tune_ev[0]) {
+            DTB_CU(cudaEventCreate(&tune_ev[0]));
+            DTB_CU(cudaEventCreate(&tune_ev[1]));
+        }
+        for (const PushCfg& c : cands) {
+            uint32_t ctas = 0;
+            DTB_CU(push_prepare(exact, static_cast<int>(wtype), c, sm_count, &ctas));
+            float ms_min = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {
+                set_u32_kernel<<<1, 1, 0, stream>>>(list_count, count);
+                DTB_CU(cudaEventRecord(tune_ev[0], stream));
+                DTB_CU(launch_push(tb, exact, static_cast<int>(wtype), c, ctas, stream));
+                DTB_CU(cudaEventRecord(tune_ev[1], stream));
+                DTB_CU(cudaEventSynchronize(tune_ev[1]));
+                float ms = 0.f;
+                DTB_CU(cudaEventElapsedTime(&ms, tune_ev[0], tune_ev[1]));
+                ms_min = std::min(ms_min, ms);
+            }
+            tune_report.push_back({c, ms_min});
+            if (ms_min < best_ms) { best_ms = ms_min; best = c; }
+        }
+        set_u32_kernel<<<1, 1, 0, stream>>>(list_count, count);
+        DTB_CU(cudaGetLastError());
+        return DTB_OK;
+    };
+    st = body();
+    cudaStreamSynchronize(stream);
+    cudaFree(scratch);
+    cudaFree(tview);
+    if (st != DTB_OK) return st;
+    push_cfg = best;
+    push_tuned[exact] = true;
+    tuned_ms = best_ms;
+    DTB_CU(push_prepare(exact, static_cast<int>(wtype), push_cfg, sm_count, &push_ctas));
+    return DTB_OK;
+}
+
 int Engine::ensure_timing_events(size_t count) {
     while (tev.size() < count) {
         cudaEvent_t e;
@@ -704,6 +786,9 @@ int Engine::info(dtb_engine_info& inf) const {
     inf.has_push = has_push;
     inf.has_pull = has_pull;
     inf.per_neuron_params = per_neuron;
+    inf.push_kind = static_cast<uint32_t>(push_cfg.kind);
+    inf.push_param = static_cast<uint32_t>(push_cfg.param);
+    inf.push_tuned_ms = tuned_ms;
     return DTB_OK;
 }
 
@@ -1075,6 +1160,35 @@ int32_t dtb_destroy(void* engine) {
 int32_t dtb_info(void* engine, dtb_engine_info* info) {
     if (!engine || !info) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
     return as_engine(engine)->info(*info);
+}
+
+int32_t dtb_set_push_variant(void* engine, int32_t kind, int32_t param) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    Engine* e = as_engine(engine);
+    if (kind < 0) {
+        e->autotune = true;
+        e->push_tuned[0] = e->push_tuned[1] = false;
+        return DTB_OK;
+    }
+    const bool ok = (kind == dtb::PUSH_REG && (param == 4 || param == 8 || param == 16)) ||
+                    (kind == dtb::PUSH_TMA && (param == 256 || param == 512));
+    if (!ok) return dtb::fail(DTB_INVALID_PARAMETER, "unknown push variant");
+    e->push_cfg = dtb::PushCfg{kind, param};
+    e->autotune = false;
+    return DTB_OK;
+}
+
+int32_t dtb_tuning_report(void* engine, uint32_t* n, int32_t* kinds, int32_t* params, float* ms) {
+    if (!engine || !n) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
+    Engine* e = as_engine(engine);
+    const uint32_t cap = *n;
+    *n = static_cast<uint32_t>(e->tune_report.size());
+    for (uint32_t i = 0; i < *n && i < cap; ++i) {
+        if (kinds) kinds[i] = e->tune_report[i].cfg.kind;
+        if (params) params[i] = e->tune_report[i].cfg.param;
+        if (ms) ms[i] = e->tune_report[i].ms;
+    }
+    return DTB_OK;
 }
 
 int32_t dtb_get_stream(void* engine, void** stream) {

@@ -117,6 +117,17 @@ public:
     uint32_t* list_ticket = nullptr;
     uint32_t* tile_pop = nullptr;
     uint32_t lif_ctas_per_sm = 2;
+
+    // push kernel variant (autotuned on the first active run)
+    PushCfg push_cfg{PUSH_REG, 8};
+    uint32_t push_ctas = 0;
+    bool autotune = true;
+    bool push_tuned[2] = {false, false};
+    float tuned_ms = 0.0f;
+    struct TuneEntry { PushCfg cfg; float ms; };
+    std::vector<TuneEntry> tune_report;
+    int tune_push(const LaunchBatch& b, int exact);
+    cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     NetView view{};
 
     // pinned staging for the statistics

@@ -27,7 +27,8 @@ namespace dtb {
 
 constexpr int kStatSlots = 32;
 constexpr int kPushThreads = 256;
-constexpr int kPushUnroll = 8;
+constexpr int kTmaWarps = 4;
+constexpr uint32_t kWaitLimit = 1u << 22;   // mbarrier polls before a wait is declared failed
 
 // Fire-and-forget reductions (no returned value, so no scoreboard wait).
 __device__ __forceinline__ void red_add_f32x2(float2* addr, float2 v) {
@@ -401,7 +402,7 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
 // ---------------------------------------------------------------------------
 // Push propagation: one warp per spiking row of the out-degree CSR
 // ---------------------------------------------------------------------------
-template <int ACC, int WT>
+template <int ACC, int WT, int kPushUnroll>
 __global__ void __launch_bounds__(kPushThreads)
 push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase, uint32_t n_nets, SpikeList sl) {
     const uint32_t count = *sl.count;
@@ -454,6 +455,180 @@ push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase
                 }
             }
         }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(sl.ticket, 1u) == gridDim.x - 1) {
+            *sl.count = 0u;
+            *sl.ticket = 0u;
+            __threadfence();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Push propagation with TMA-staged row fetches.  Every warp owns a two-stage
+// ring in shared memory; lane 0 issues bulk copies (cp.async.bulk, no
+// multicast) of the next row chunk -- postsynaptic ids and weight pairs -- while
+// the warp turns the current chunk into vector reductions.  Copies start on the
+// 16-byte boundary at or below the chunk and end on the one at or above it (the
+// CSR arrays carry 64 bytes of tail padding), and the consumer skips the slack.
+// Every mbarrier wait is bounded: on timeout the kernel raises an error bit,
+// waits (bounded) for its other copy in flight, and stops.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    uint64_t g;
+    asm volatile("cvta.to.global.u64 %0, %1;" : "=l"(g) : "l"(src));
+    asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_addr(dst)), "l"(g), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                 : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// Bounded wait on one mbarrier phase; false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (uint32_t it = 0; it < kWaitLimit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+template <int WT> struct WBytes { static constexpr int v = 4; };
+template <> struct WBytes<W_F32> { static constexpr int v = 8; };
+template <> struct WBytes<W_U8> { static constexpr int v = 2; };
+
+template <int WT, int CH>
+struct TmaLayout {
+    static constexpr int WB = WBytes<WT>::v;
+    static constexpr int COLB = CH * 4 + 32;
+    static constexpr int WTB = CH * WB + 32;
+    static constexpr int STAGE = (COLB + WTB + 127) / 128 * 128;
+    static constexpr int SMEM = kTmaWarps * 2 * STAGE + kTmaWarps * 2 * 8;
+};
+
+template <int WT>
+__device__ __forceinline__ float2 smem_weight(const unsigned char* base, uint32_t e) {
+    if constexpr (WT == W_F32) {
+        return reinterpret_cast<const float2*>(base)[e];
+    } else if constexpr (WT == W_BF16) {
+        return __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(base)[e]);
+    } else if constexpr (WT == W_F16) {
+        return __half22float2(reinterpret_cast<const __half2*>(base)[e]);
+    } else {
+        const uchar2 u = reinterpret_cast<const uchar2*>(base)[e];
+        return make_float2(static_cast<float>(u.x) / 255.f, static_cast<float>(u.y) / 255.f);
+    }
+}
+
+template <int ACC, int WT, int CH>
+__global__ void __launch_bounds__(kTmaWarps * 32)
+push_tma_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase, uint32_t n_nets, SpikeList sl) {
+    using L = TmaLayout<WT, CH>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* ring = smem + warp * 2 * L::STAGE;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kTmaWarps * 2 * L::STAGE) + warp * 2;
+    if (lane == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncwarp();
+    const uint32_t count = *sl.count;
+    const uint32_t nw = gridDim.x * kTmaWarps;
+    // producer cursor (lane-uniform): list index, remaining range of the row, its network
+    uint32_t pr = blockIdx.x * kTmaWarps + warp;
+    unsigned long long pc = 0, pe = 0;
+    uint32_t pnet = 0;
+    auto next_row = [&]() -> bool {
+        while (pr < count) {
+            const uint32_t v = __ldg(sl.list + pr);
+            pnet = n_nets > 1 ? find_net(vbase, n_nets, v) : 0u;
+            const uint32_t j = v - __ldg(vbase + pnet);
+            const unsigned long long* ptr = nets[pnet].out_ptr;
+            pc = __ldg(ptr + j);
+            pe = __ldg(ptr + j + 1);
+            if (pc < pe) return true;
+            pr += nw;
+        }
+        return false;
+    };
+    bool have = next_row();
+    uint32_t s_cnt[2] = {0, 0}, s_oc[2] = {0, 0}, s_ow[2] = {0, 0}, s_net[2] = {0, 0};
+    bool s_full[2] = {false, false};
+    uint32_t phase[2] = {0, 0};
+    auto issue = [&](int stg) {
+        const unsigned long long e0 = pc, e1 = min(pe, pc + static_cast<unsigned long long>(CH));
+        const unsigned long long c0 = (e0 * 4) & ~15ull, c1 = (e1 * 4 + 15) & ~15ull;
+        const unsigned long long w0 = (e0 * L::WB) & ~15ull, w1 = (e1 * L::WB + 15) & ~15ull;
+        unsigned char* stage = ring + stg * L::STAGE;
+        if (lane == 0) {
+            const unsigned char* colb = reinterpret_cast<const unsigned char*>(nets[pnet].out_col);
+            const unsigned char* wb = reinterpret_cast<const unsigned char*>(nets[pnet].out_w);
+            mbar_expect_tx(&bars[stg], static_cast<uint32_t>((c1 - c0) + (w1 - w0)));
+            bulk_load(stage, colb + c0, static_cast<uint32_t>(c1 - c0), &bars[stg]);
+            bulk_load(stage + L::COLB, wb + w0, static_cast<uint32_t>(w1 - w0), &bars[stg]);
+        }
+        s_cnt[stg] = static_cast<uint32_t>(e1 - e0);
+        s_oc[stg] = static_cast<uint32_t>((e0 * 4 - c0) / 4);
+        s_ow[stg] = static_cast<uint32_t>((e0 * L::WB - w0) / L::WB);
+        s_net[stg] = pnet;
+        s_full[stg] = true;
+        pc = e1;
+        if (pc >= pe) {
+            pr += nw;
+            have = next_row();
+        }
+    };
+    if (have) issue(0);
+    int st = 0;
+    bool failed = false;
+    while (s_full[st]) {
+        if (have) issue(st ^ 1);
+        if (!mbar_wait_bounded(&bars[st], phase[st])) {
+            failed = true;
+            break;
+        }
+        phase[st] ^= 1;
+        const unsigned char* stage = ring + st * L::STAGE;
+        const uint32_t* scol = reinterpret_cast<const uint32_t*>(stage) + s_oc[st];
+        const unsigned char* sw = stage + L::COLB;
+        const uint32_t cnt = s_cnt[st], ow = s_ow[st];
+        float4* J = nets[s_net[st]].J;
+        long long* dJ = nets[s_net[st]].dJ;
+#pragma unroll 4
+        for (uint32_t e = lane; e < cnt; e += 32) {
+            const uint32_t c = scol[e];
+            const float2 w = smem_weight<WT>(sw, ow + e);
+            const uint32_t target = c & kIndexMask, kind = c >> 31;
+            if constexpr (ACC == 0) {
+                red_add_f32x2(reinterpret_cast<float2*>(J + target) + kind, w);
+            } else {
+                unsigned long long* d = reinterpret_cast<unsigned long long*>(dJ) + static_cast<size_t>(target) * 4 + 2 * kind;
+                red_add_u64(d, static_cast<unsigned long long>(float_to_fix(w.x)));
+                red_add_u64(d + 1, static_cast<unsigned long long>(float_to_fix(w.y)));
+            }
+        }
+        __syncwarp();
+        s_full[st] = false;
+        st ^= 1;
+    }
+    if (failed) {
+        if (lane == 0) atomicOr(&nets[0].clock->err, kErrTimeout);
+        // let the other copy in flight land before the CTA's shared memory is released
+        if (s_full[st ^ 1]) mbar_wait_bounded(&bars[st ^ 1], phase[st ^ 1]);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -692,20 +867,83 @@ cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop
     return cudaGetLastError();
 }
 
+template <int ACC, int WT>
+static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint32_t ctas, cudaStream_t s) {
+    if (cfg.kind == PUSH_REG) {
+        const dim3 grid(ctas), block(kPushThreads);
+        switch (cfg.param) {
+            case 4: push_kernel<ACC, WT, 4><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
+            case 16: push_kernel<ACC, WT, 16><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
+            default: push_kernel<ACC, WT, 8><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
+        }
+    } else {
+        const dim3 grid(ctas), block(kTmaWarps * 32);
+        if (cfg.param == 256) {
+            using L = TmaLayout<WT, 256>;
+            push_tma_kernel<ACC, WT, 256><<<grid, block, L::SMEM, s>>>(b.nets, b.vbase, b.n_nets, b.spikes);
+        } else {
+            using L = TmaLayout<WT, 512>;
+            push_tma_kernel<ACC, WT, 512><<<grid, block, L::SMEM, s>>>(b.nets, b.vbase, b.n_nets, b.spikes);
+        }
+    }
+    return cudaGetLastError();
+}
+
+template <int ACC, int WT>
+static cudaError_t push_prepare_wt(const PushCfg& cfg, int sm_count, uint32_t* ctas) {
+    int per_sm = 0;
+    cudaError_t e = cudaSuccess;
+    if (cfg.kind == PUSH_REG) {
+        switch (cfg.param) {
+            case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_kernel<ACC, WT, 4>, kPushThreads, 0); break;
+            case 16: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_kernel<ACC, WT, 16>, kPushThreads, 0); break;
+            default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_kernel<ACC, WT, 8>, kPushThreads, 0); break;
+        }
+    } else if (cfg.param == 256) {
+        using L = TmaLayout<WT, 256>;
+        e = cudaFuncSetAttribute(push_tma_kernel<ACC, WT, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_tma_kernel<ACC, WT, 256>, kTmaWarps * 32, L::SMEM);
+    } else {
+        using L = TmaLayout<WT, 512>;
+        e = cudaFuncSetAttribute(push_tma_kernel<ACC, WT, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_tma_kernel<ACC, WT, 512>, kTmaWarps * 32, L::SMEM);
+    }
+    if (e != cudaSuccess) return e;
+    *ctas = static_cast<uint32_t>(std::max(1, per_sm) * sm_count);
+    return cudaSuccess;
+}
+
 template <int ACC>
-static void push_dispatch(const LaunchBatch& b, int wt, cudaStream_t s) {
-    const dim3 grid(b.push_ctas), block(kPushThreads);
+static cudaError_t push_launch_acc(const LaunchBatch& b, int wt, const PushCfg& cfg, uint32_t ctas, cudaStream_t s) {
     switch (wt) {
-        case W_F32: push_kernel<ACC, W_F32><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
-        case W_BF16: push_kernel<ACC, W_BF16><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
-        case W_F16: push_kernel<ACC, W_F16><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
-        default: push_kernel<ACC, W_U8><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
+        case W_F32: return push_launch_wt<ACC, W_F32>(b, cfg, ctas, s);
+        case W_BF16: return push_launch_wt<ACC, W_BF16>(b, cfg, ctas, s);
+        case W_F16: return push_launch_wt<ACC, W_F16>(b, cfg, ctas, s);
+        default: return push_launch_wt<ACC, W_U8>(b, cfg, ctas, s);
     }
 }
 
-cudaError_t launch_push(const LaunchBatch& b, int exact, int wt, cudaStream_t s) {
-    if (exact) push_dispatch<1>(b, wt, s); else push_dispatch<0>(b, wt, s);
-    return cudaGetLastError();
+cudaError_t push_prepare(int exact, int wt, const PushCfg& cfg, int sm_count, uint32_t* ctas) {
+    if (exact) {
+        switch (wt) {
+            case W_F32: return push_prepare_wt<1, W_F32>(cfg, sm_count, ctas);
+            case W_BF16: return push_prepare_wt<1, W_BF16>(cfg, sm_count, ctas);
+            case W_F16: return push_prepare_wt<1, W_F16>(cfg, sm_count, ctas);
+            default: return push_prepare_wt<1, W_U8>(cfg, sm_count, ctas);
+        }
+    }
+    switch (wt) {
+        case W_F32: return push_prepare_wt<0, W_F32>(cfg, sm_count, ctas);
+        case W_BF16: return push_prepare_wt<0, W_BF16>(cfg, sm_count, ctas);
+        case W_F16: return push_prepare_wt<0, W_F16>(cfg, sm_count, ctas);
+        default: return push_prepare_wt<0, W_U8>(cfg, sm_count, ctas);
+    }
+}
+
+cudaError_t launch_push(const LaunchBatch& b, int exact, int wt, const PushCfg& cfg, uint32_t ctas, cudaStream_t s) {
+    return exact ? push_launch_acc<1>(b, wt, cfg, ctas, s) : push_launch_acc<0>(b, wt, cfg, ctas, s);
 }
 
 template <int G>

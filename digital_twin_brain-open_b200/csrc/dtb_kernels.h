@@ -23,7 +23,17 @@ struct LaunchBatch {
 };
 
 cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop_mode, cudaStream_t s);
-cudaError_t launch_push(const LaunchBatch& b, int exact, int weight_type, cudaStream_t s);
+// Push kernel variants chosen by the autotuner.
+enum PushKind : int { PUSH_REG = 0, PUSH_TMA = 1 };
+struct PushCfg {
+    int kind;    // PUSH_REG: register-staged loads, param = synapses in flight per lane (4, 8, 16)
+                 // PUSH_TMA: bulk-copy staged rows, param = synapses per stage (256, 512)
+    int param;
+};
+// Sets kernel attributes and returns the persistent grid (max resident CTAs).
+cudaError_t push_prepare(int exact, int weight_type, const PushCfg& cfg, int sm_count, uint32_t* ctas);
+cudaError_t launch_push(const LaunchBatch& b, int exact, int weight_type, const PushCfg& cfg, uint32_t ctas,
+                        cudaStream_t s);
 cudaError_t launch_pull(const LaunchBatch& b, int gather, int weight_type, uint32_t flags, int prop_mode, cudaStream_t s);
 cudaError_t launch_fold_finish(const LaunchBatch& b, cudaStream_t s);
 cudaError_t launch_gather_finish(const LaunchBatch& b, int weight_type, cudaStream_t s);

@@ -64,7 +64,8 @@ class EngineInfo(C.Structure):
     _fields_ = [("n_neurons", C.c_uint32), ("n_pops", C.c_uint32), ("n_edges", C.c_uint64),
                 ("device_bytes", C.c_uint64), ("step", C.c_uint64), ("t", C.c_float),
                 ("weight_type", C.c_uint32), ("has_push", C.c_uint32), ("has_pull", C.c_uint32),
-                ("per_neuron_params", C.c_uint32)]
+                ("per_neuron_params", C.c_uint32), ("push_kind", C.c_uint32), ("push_param", C.c_uint32),
+                ("push_tuned_ms", C.c_float)]
 
 
 class RunRequest(C.Structure):
@@ -93,6 +94,8 @@ SIGNATURES = {
     "dtb_destroy": (_I32, [_P]),
     "dtb_info": (_I32, [_P, _P]),
     "dtb_get_stream": (_I32, [_P, C.POINTER(C.c_void_p)]),
+    "dtb_set_push_variant": (_I32, [_P, _I32, _I32]),
+    "dtb_tuning_report": (_I32, [_P, _P, _P, _P, _P]),
     "dtb_populations": (_I32, [_P, _P, _P]),
     "dtb_update_props": (_I32, [_P, _U32, _P, _P, _P]),
     "dtb_update_prop_cols": (_I32, [_P, _U32, _P, _P, _P, _I32]),
@@ -257,6 +260,19 @@ class Engine:
         inf = EngineInfo()
         _check(LIB.dtb_info(self._h, C.byref(inf)))
         return inf
+
+    def set_push_variant(self, kind, param=0):
+        """kind 0: register-staged (param 4/8/16), 1: TMA-staged (param 256/512), -1: autotune."""
+        _check(LIB.dtb_set_push_variant(self._h, kind, param))
+
+    def tuning_report(self):
+        """[(kind, param, ms)] of the push variants timed by the autotuner."""
+        n = C.c_uint32(16)
+        k = np.zeros(16, np.int32)
+        p = np.zeros(16, np.int32)
+        ms = np.zeros(16, np.float32)
+        _check(LIB.dtb_tuning_report(self._h, C.byref(n), _ptr(k), _ptr(p), _ptr(ms)))
+        return [(int(k[i]), int(p[i]), float(ms[i])) for i in range(min(n.value, 16))]
 
     def stream(self):
         """The engine's cudaStream_t as an integer handle."""

@@ -138,6 +138,9 @@ typedef struct dtb_engine_info {
     uint32_t weight_type;
     uint32_t has_push, has_pull;
     uint32_t per_neuron_params;  /* 1 once any parameter differs within a population        */
+    uint32_t push_kind;          /* push kernel in use: 0 register-staged, 1 TMA-staged rows   */
+    uint32_t push_param;         /* synapses in flight per lane (0) or per stage (1)          */
+    float push_tuned_ms;         /* push time of the chosen variant when it was tuned, ms     */
 } dtb_engine_info;
 
 /* RunRequest (snn.proto:63-77) flags. */
@@ -188,6 +191,14 @@ int32_t dtb_create_structured(const dtb_structured_spec* spec, const dtb_options
 int32_t dtb_create_from_npz(const char* path, const dtb_options* opt, void** engine);
 int32_t dtb_destroy(void* engine);
 int32_t dtb_info(void* engine, dtb_engine_info* info);
+/* Push kernel variant: kind 0 (register-staged, param 4/8/16 synapses in flight
+ * per lane) or 1 (TMA bulk-copy staged rows, param 256/512 synapses per stage);
+ * kind < 0 re-enables the autotuner, which times every variant on a live spike
+ * list of the first active run and keeps the fastest. */
+int32_t dtb_set_push_variant(void* engine, int32_t kind, int32_t param);
+/* The autotuner's last measurement: on entry *n is the capacity of the arrays,
+ * on return the number of variants timed (kind, param, push time in ms). */
+int32_t dtb_tuning_report(void* engine, uint32_t* n, int32_t* kinds, int32_t* params, float* ms);
 /* The CUDA stream (cudaStream_t) every kernel and copy of this engine runs on,
  * so a caller can order its own work and CUDA events against the engine. */
 int32_t dtb_get_stream(void* engine, void** stream);

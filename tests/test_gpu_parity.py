@@ -324,3 +324,36 @@ def test_large_in_degree_against_c_oracle(gpu):
         r = eng.run(steps, record_spikes=True, syn_mode=E.SYN_PULL)
         assert first_divergence(r.spikes, sp) is None
         assert np.array_equal(eng.read_state(E.STATE_V), orc.V)
+
+
+@pytest.mark.parametrize("variant", [(0, 4), (0, 8), (0, 16), (1, 256), (1, 512)])
+def test_every_push_variant_is_exact(gpu, variant):
+    """Each push kernel (register-staged, TMA-staged) gives the oracle's bit-exact result."""
+    spec = nw.structured_spec(12_000, 8, 300, seed=15)
+    net = co.structured_edges(spec)
+    steps = 350
+    z, _ = lo.torch_noise_stream(3, spec.n, steps, False)
+    o, spikes, counts, _ = oracle_run(net, z)
+    assert spikes[250:].mean() > 0.005
+    for wt in (E.W_F32, E.W_BF16):
+        with E.Engine.structured(spec, weight_type=wt) as eng:
+            eng.set_push_variant(*variant)
+            eng.set_noise_injected(z)
+            r = eng.run(steps, record_spikes=True, syn_mode=E.SYN_PUSH_EXACT)
+            info = eng.info()
+            assert (info.push_kind, info.push_param) == variant
+            if wt == E.W_F32:
+                assert first_divergence(r.spikes, spikes) is None
+                assert np.array_equal(eng.read_state(E.STATE_V), o.V)
+            else:
+                assert abs(r.spikes[250:].mean() - spikes[250:].mean()) < 0.1 * spikes[250:].mean()
+
+
+def test_autotuner_picks_a_variant(gpu):
+    spec = nw.structured_spec(100_000, 10, 500, seed=4)
+    with E.Engine.structured(spec) as eng:
+        eng.run(400)
+        rep = eng.tuning_report()
+        assert len(rep) == 5 and all(ms > 0 for _, _, ms in rep)
+        inf = eng.info()
+        assert min(ms for _, _, ms in rep) == pytest.approx(inf.push_tuned_ms)
