@@ -647,12 +647,18 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
             switch (rq.syn_mode) {
                 case DTB_SYN_PUSH:
                     DTB_TRY(timed_launch(0, [&] { return launch_lif(b, J_DIRECT, kflags, pm, stream); }));
-                    if (tune_at == done + s) DTB_TRY(tune_push(b, 0));
+                    if (tune_at == done + s) {
+                        DTB_TRY(tune_push(b, 0));
+                        if (!push_tuned[0]) tune_at += 50;   // still quiet: retry later in this run
+                    }
                     DTB_TRY(timed_launch(1, [&] { return launch_push(b, 0, static_cast<int>(wtype), push_cfg, push_ctas, stream); }));
                     break;
                 case DTB_SYN_PUSH_EXACT:
                     DTB_TRY(timed_launch(0, [&] { return launch_lif(b, first ? J_ASIS : J_FOLD, kflags, pm, stream); }));
-                    if (tune_at == done + s) DTB_TRY(tune_push(b, 1));
+                    if (tune_at == done + s) {
+                        DTB_TRY(tune_push(b, 1));
+                        if (!push_tuned[1]) tune_at += 50;
+                    }
                     DTB_TRY(timed_launch(1, [&] { return launch_push(b, 1, static_cast<int>(wtype), push_cfg, push_ctas, stream); }));
                     break;
                 default:
