@@ -110,6 +110,7 @@ SIGNATURES = {
     "dtb_save_state": (_I32, [_P, _P, C.c_uint64]),
     "dtb_load_state": (_I32, [_P, _P, C.c_uint64]),
     "dtb_build_out_csr_host": (_I32, [_U32, C.c_uint64, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "dtb_compact_spikes": (_I32, [_P, _U32, _P, _P, _P]),
 }
 
 
@@ -175,6 +176,12 @@ def build_out_csr_host(n, pre, post, kind):
                                       _ptr(row_ptr), _ptr(post_o), _ptr(kind_o), _ptr(perm)))
     nr = nr.value
     return rows[:nr], row_ptr[:nr + 1], post_o, kind_o, perm
+
+
+def compact_spikes(d_bits, n, d_indices, d_count, stream=0):
+    """Device spike bitmap -> ascending device index list (all pointers are device addresses)."""
+    _check(LIB.dtb_compact_spikes(C.c_void_p(d_bits), n, C.c_void_p(d_indices), C.c_void_p(d_count),
+                                  C.c_void_p(stream) if stream else None))
 
 
 @dataclasses.dataclass

@@ -259,6 +259,16 @@ int32_t dtb_build_out_csr_host(uint32_t n_neurons, uint64_t n_edges, const uint3
                                const uint8_t* kind, uint32_t* n_rows, uint32_t* rows, uint64_t* row_ptr,
                                uint32_t* post_out, uint8_t* kind_out, uint64_t* perm);
 
+/* Spike compaction (the sending-side compaction of src/stage/spike.cpp:244-762
+ * as one operator): turns the device spike bitmap `d_bits` (bit i of word i/32
+ * is neuron i; ceil(n/32) words) into the ascending list of spiking neurons
+ * `d_indices` (room for n entries) and its length `*d_count`, all in device
+ * memory, ordered on `stream` (a cudaStream_t, NULL = default stream).
+ * Deterministic.  Scratch: one word per 4096 neurons, allocated and released
+ * on `stream` by each call. */
+int32_t dtb_compact_spikes(const uint32_t* d_bits, uint32_t n_neurons, uint32_t* d_indices, uint32_t* d_count,
+                           void* stream);
+
 /* Serving eviction: the whole dynamic state (V, J, I_ou, t_last, clock and the
  * last step's spikes) as one blob.  dtb_state_size gives its size. */
 int32_t dtb_state_size(void* engine, uint64_t* bytes);

@@ -358,3 +358,26 @@ def test_autotuner_picks_a_variant(gpu):
         assert len(rep) == 5 and all(ms > 0 for _, _, ms in rep)
         inf = eng.info()
         assert min(ms for _, _, ms in rep) == pytest.approx(inf.push_tuned_ms)
+
+
+@pytest.mark.parametrize("n", [1, 31, 32, 33, 4095, 4096, 4097, 100_000, 5_000_000])
+def test_compact_spikes_operator(gpu, n):
+    """The standalone compaction: the ascending spiking indices of a device bitmap."""
+    import torch
+    rng = np.random.default_rng(n)
+    words = (n + 31) // 32
+    host = rng.integers(0, 2 ** 32, words, dtype=np.uint64).astype(np.uint32)
+    host &= rng.integers(0, 2 ** 32, words, dtype=np.uint64).astype(np.uint32)   # ~25 % density
+    sparse = rng.random(words) < 0.5
+    host[sparse] = 0
+    bits = torch.from_numpy(host.view(np.int32)).cuda()
+    idx = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = torch.cuda.current_stream()
+    E.compact_spikes(bits.data_ptr(), n, idx.data_ptr(), cnt.data_ptr(), s.cuda_stream)
+    torch.cuda.synchronize()
+    flags = np.unpackbits(host.view(np.uint8), bitorder="little")[:n].astype(bool)
+    ref = np.nonzero(flags)[0]
+    c = int(cnt.item())
+    assert c == ref.size
+    assert np.array_equal(idx[:c].cpu().numpy().astype(np.int64), ref)
