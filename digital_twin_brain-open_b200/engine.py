@@ -111,6 +111,7 @@ SIGNATURES = {
     "dtb_load_state": (_I32, [_P, _P, C.c_uint64]),
     "dtb_build_out_csr_host": (_I32, [_U32, C.c_uint64, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "dtb_compact_spikes": (_I32, [_P, _U32, _P, _P, _P]),
+    "dtb_compact_spikes_noalloc": (_I32, [_P, _U32, _P, _P, _P]),
 }
 
 

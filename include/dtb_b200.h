@@ -269,6 +269,18 @@ int32_t dtb_build_out_csr_host(uint32_t n_neurons, uint64_t n_edges, const uint3
 int32_t dtb_compact_spikes(const uint32_t* d_bits, uint32_t n_neurons, uint32_t* d_indices, uint32_t* d_count,
                            void* stream);
 
+/* The same compaction for callers that cannot allocate device memory at the point
+ * of the call -- a host recording a CUDA graph (no allocation during stream
+ * capture), a loop with a device-memory budget fixed at start-up, a runtime that
+ * owns all device memory.  No counterpart in the reference.  It allocates
+ * nothing: its scratch is a fixed 64 KiB array inside the library, so
+ * n_neurons <= 2^26 (larger inputs return DTB_INVALID_PARAMETER).  All calls
+ * share that array: calls whose kernels overlap on the GPU race and must be
+ * ordered.  The first call on each device looks the array up (with that device
+ * current); make it before any stream capture. */
+int32_t dtb_compact_spikes_noalloc(const uint32_t* d_bits, uint32_t n_neurons, uint32_t* d_indices,
+                                   uint32_t* d_count, void* stream);
+
 /* Serving eviction: the whole dynamic state (V, J, I_ou, t_last, clock and the
  * last step's spikes) as one blob.  dtb_state_size gives its size. */
 int32_t dtb_state_size(void* engine, uint64_t* bytes);
