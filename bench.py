@@ -157,6 +157,21 @@ def traffic_per_launch(events_per_launch):
         return None
 
 
+def aggregate_replicas(counts, times_ms, dist=None, device=None):
+    """Whole-job totals of independent replicas: counts summed over ranks, device
+    times maxed over ranks (each rank timed its own stream with CUDA events)."""
+    import torch
+    c = np.asarray(counts, np.float64)
+    t = np.asarray(times_ms, np.float64)
+    if dist is not None and dist.is_initialized() and dist.get_world_size() > 1:
+        tc = torch.tensor(c, device=device)
+        dist.all_reduce(tc, op=dist.ReduceOp.SUM)
+        tt = torch.tensor(t, device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        c, t = tc.cpu().numpy(), tt.cpu().numpy()
+    return c, t
+
+
 def run_ours(args):
     import torch
     import __graft_entry__
@@ -248,17 +263,8 @@ def run_ours(args):
     barrier()
     e2e_ms = e_start.elapsed_time(e_end)
 
-    tot = np.array([events, e2e_events, spikes], np.float64)
-    times = np.array([ms, e2e_ms], np.float64)
-    if dist is not None:
-        t = torch.tensor(tot, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        tot = t.cpu().numpy()
-        tt = torch.tensor(times, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        times = tt.cpu().numpy()
-    events, e2e_events, spikes = tot
-    ms, e2e_ms = times
+    (events, e2e_events, spikes), (ms, e2e_ms) = aggregate_replicas(
+        [events, e2e_events, spikes], [ms, e2e_ms], dist, dev)
     value = events / (ms / 1e3)
     out = None
     if rank == 0:

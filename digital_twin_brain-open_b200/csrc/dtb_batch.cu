@@ -1,0 +1,324 @@
+// Batched form: many independent networks (data-assimilation ensemble members,
+// served requests) advanced by ONE launch of each per-step kernel.
+//
+// The reference batches an ensemble by packing its members into one network as
+// disjoint population ranges (data_assimilation/DA_voxel.py:47-52, 264-268).  Here
+// the members stay separate engines -- each with its own state, CSR, clock, noise
+// stream and statistics -- and a batch launch walks all of them: CTA -> (member,
+// tile) through a prefix over the members' tiles, one shared spike list whose
+// entries carry a virtual neuron id (member base + neuron).  Uneven members cost
+// nothing extra: tiles and spiking rows are distributed over the whole GPU.
+//
+// A window of steps of the float push mode is captured once into a CUDA graph
+// (2 kernel nodes per step) and replayed per window; the push variant is chosen by
+// the same on-line autotuner as a single engine's, on the batch's own spike list.
+#include <algorithm>
+#include <cstring>
+
+#include "dtb_engine.h"
+
+namespace dtb {
+
+class Batch {
+public:
+    ~Batch();
+    int create(Engine* const* engines, uint32_t n);
+    int run(const dtb_run_request& rq, dtb_run_output* outs);
+    int refresh_views();
+
+    std::vector<Engine*> m;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev[2] = {nullptr, nullptr};
+    int sm_count = 148;
+    uint32_t wtype = W_F32;
+    NetView* d_views = nullptr;
+    uint32_t* d_prefix = nullptr;     // [lif n+1][pull n+1][vbase n+1]
+    uint32_t* list = nullptr;
+    uint32_t* list_count = nullptr;
+    uint32_t* list_ticket = nullptr;
+    LaunchBatch lb{};
+    PushCfg push_cfg{PUSH_REG, 8, 32};
+    uint32_t push_ctas = 0;
+    bool push_tuned[2] = {false, false};
+    TuneResult tune;
+    bool use_graph = true;
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_key[6] = {0, 0, 0, 0, 0, 0};
+    uint32_t graph_launches = 0;
+};
+
+Batch::~Batch() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (graph) cudaGraphExecDestroy(graph);
+    for (void* p : {static_cast<void*>(d_views), static_cast<void*>(d_prefix), static_cast<void*>(list),
+                    static_cast<void*>(list_count), static_cast<void*>(list_ticket)})
+        if (p) cudaFree(p);
+    for (cudaEvent_t e : {ev0, ev1, tev[0], tev[1]})
+        if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+int Batch::create(Engine* const* engines, uint32_t n) {
+    if (n == 0) return fail(DTB_INVALID_PARAMETER, "empty batch");
+    m.assign(engines, engines + n);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!m[i]) return fail(DTB_INVALID_PARAMETER, "NULL engine in batch");
+        for (uint32_t j = 0; j < i; ++j)
+            if (m[j] == m[i]) return fail(DTB_INVALID_PARAMETER, "an engine appears twice in the batch");
+        if (m[i]->wtype != m[0]->wtype) return fail(DTB_UNSUPPORTED, "batch members must share the weight type");
+        if (m[i]->device != m[0]->device) return fail(DTB_UNSUPPORTED, "batch members must share the device");
+    }
+    wtype = m[0]->wtype;
+    sm_count = m[0]->sm_count;
+    DTB_CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    DTB_CU(cudaEventCreate(&ev0));
+    DTB_CU(cudaEventCreate(&ev1));
+    DTB_CU(cudaEventCreate(&tev[0]));
+    DTB_CU(cudaEventCreate(&tev[1]));
+    std::vector<uint32_t> pre(3 * (n + 1), 0);
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        pre[i + 1] = pre[i] + m[i]->n_pad / kLifTile;
+        pre[(n + 1) + i + 1] = pre[(n + 1) + i] + m[i]->n_pad / kPullTile;
+        total += m[i]->n_pad;
+        if (total >= 0xFFFFFFFFull) return fail(DTB_UNSUPPORTED, "a batch holds at most 2^32 neurons");
+        pre[2 * (n + 1) + i + 1] = static_cast<uint32_t>(total);
+    }
+    DTB_CU(cudaMalloc(reinterpret_cast<void**>(&d_views), sizeof(NetView) * n));
+    DTB_CU(cudaMalloc(reinterpret_cast<void**>(&d_prefix), sizeof(uint32_t) * pre.size()));
+    DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list), sizeof(uint32_t) * total));
+    DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_count), sizeof(uint32_t)));
+    DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_ticket), sizeof(uint32_t)));
+    DTB_CU(cudaMemsetAsync(list_count, 0, sizeof(uint32_t), stream));
+    DTB_CU(cudaMemsetAsync(list_ticket, 0, sizeof(uint32_t), stream));
+    DTB_CU(cudaMemcpyAsync(d_prefix, pre.data(), sizeof(uint32_t) * pre.size(), cudaMemcpyHostToDevice, stream));
+    lb.nets = d_views;
+    lb.lif_prefix = d_prefix;
+    lb.pull_prefix = d_prefix + (n + 1);
+    lb.vbase = d_prefix + 2 * (n + 1);
+    lb.n_nets = n;
+    lb.lif_tiles_total = pre[n];
+    lb.pull_tiles_total = pre[(n + 1) + n];
+    lb.push_ctas = static_cast<uint32_t>(sm_count) * 8u;
+    lb.lif_ctas = static_cast<uint32_t>(sm_count) * m[0]->lif_ctas_per_sm;
+    lb.spikes = SpikeList{list, list_count, list_ticket, static_cast<uint32_t>(total)};
+    DTB_CU(cudaStreamSynchronize(stream));
+    return DTB_OK;
+}
+
+int Batch::refresh_views() {
+    std::vector<NetView> v(m.size());
+    for (size_t i = 0; i < m.size(); ++i) v[i] = m[i]->view;
+    DTB_CU(cudaMemcpyAsync(d_views, v.data(), sizeof(NetView) * v.size(), cudaMemcpyHostToDevice, stream));
+    DTB_CU(cudaStreamSynchronize(stream));
+    return DTB_OK;
+}
+
+int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
+    if (rq.iters == 0) return fail(DTB_INVALID_PARAMETER, "iter must be positive");
+    if (rq.prop_mode > DTB_PROP_OR || rq.syn_mode > DTB_SYN_PULL) return fail(DTB_INVALID_PARAMETER, "unknown mode");
+    const bool freq = (rq.flags & DTB_RUN_FREQ) != 0;
+    const bool vmean = (rq.flags & DTB_RUN_VMEAN) != 0;
+    const bool record = (rq.flags & DTB_RUN_RECORD_SPIKES) != 0;
+    const int exact = rq.syn_mode == DTB_SYN_PUSH_EXACT ? 1 : 0;
+    bool injected = false;
+    for (size_t i = 0; i < m.size(); ++i) {
+        Engine& e = *m[i];
+        if (rq.syn_mode != DTB_SYN_PULL && !e.has_push) return fail(DTB_UNSUPPORTED, "a member has no out-degree CSR");
+        if (rq.syn_mode == DTB_SYN_PULL && !e.has_pull) return fail(DTB_UNSUPPORTED, "a member has no in-degree CSR");
+        if ((freq && !outs[i].freqs) || (vmean && !outs[i].vmeans) || (record && !outs[i].spike_bits))
+            return fail(DTB_INVALID_PARAMETER, "requested output buffer is NULL");
+        const bool inj = e.noise_src == DTB_NOISE_INJECTED;
+        if (i > 0 && inj != injected) return fail(DTB_UNSUPPORTED, "batch members must share the noise source");
+        injected = inj;
+        if (inj && (e.steps - e.inj_first) + rq.iters > e.inj_rows)
+            return fail(DTB_INVALID_PARAMETER, "a member has not enough injected noise rows");
+        if (inj && rq.prop_mode != DTB_PROP_THRESHOLD && !e.inj_u)
+            return fail(DTB_INVALID_PARAMETER, "noise train needs injected uniforms");
+        DTB_CU(cudaStreamSynchronize(e.stream));
+    }
+    uint32_t cap = std::min<uint32_t>(rq.iters, 4096u);
+    for (Engine* e : m) {
+        if (record) cap = std::min<uint32_t>(cap, std::max<uint32_t>(1u, static_cast<uint32_t>((512ull << 20) / (4ull * e->n_words))));
+    }
+    for (Engine* e : m) {
+        if (exact) DTB_TRY(e->ensure_dj());
+        DTB_TRY(e->ensure_hist(cap, record));
+    }
+    DTB_TRY(refresh_views());
+    uint32_t kflags = 0;
+    if (rq.flags & DTB_RUN_USE_OU) kflags |= kFlagUseOU;
+    if (freq || vmean) kflags |= kFlagStats;
+    if (record) kflags |= kFlagRecord;
+    if (rq.syn_mode != DTB_SYN_PULL) kflags |= kFlagList;
+    if (injected) kflags |= kFlagInjected;
+    const int pm = static_cast<int>(rq.prop_mode);
+    const int wt = static_cast<int>(wtype);
+    uint64_t tune_at = ~0ull;
+    if (rq.syn_mode != DTB_SYN_PULL) {
+        DTB_CU(push_prepare(exact, wt, push_cfg, sm_count, &push_ctas));
+        if (!push_tuned[exact]) {
+            const uint64_t settle = 300;
+            const uint64_t st = m[0]->steps;
+            tune_at = st >= settle ? 1 : (settle - st < rq.iters ? settle - st : ~0ull);
+        }
+    }
+    for (Engine* e : m) set_u64_kernel<<<1, 1, 0, stream>>>(e->events, 0ull);
+    DTB_CU(cudaGetLastError());
+    uint32_t launches = static_cast<uint32_t>(m.size());
+    double ms_total = 0.0;
+    uint32_t done = 0;
+    while (done < rq.iters) {
+        const uint32_t rows = std::min(cap, rq.iters - done);
+        for (Engine* e : m) {
+            set_u64_kernel<<<1, 1, 0, stream>>>(&e->clock->run_base, e->steps);
+            if (freq || vmean) {
+                DTB_CU(cudaMemsetAsync(e->hist_cnt, 0, sizeof(int) * rows * e->P, stream));
+                DTB_CU(cudaMemsetAsync(e->hist_vsum, 0, sizeof(long long) * rows * e->P, stream));
+            }
+            ++launches;
+        }
+        DTB_CU(cudaEventRecord(ev0, stream));
+        // Graph-replayed window: float push mode, no tuning pending inside it.
+        const bool graphable = use_graph && rq.syn_mode == DTB_SYN_PUSH &&
+                               !(tune_at >= done && tune_at < done + rows);
+        if (graphable) {
+            const uint64_t key[6] = {rows, kflags, static_cast<uint64_t>(pm),
+                                     static_cast<uint64_t>(push_cfg.kind) * 100000 + push_cfg.param * 100 + push_cfg.lpr,
+                                     push_ctas, 1};
+            if (!graph || std::memcmp(key, graph_key, sizeof(key)) != 0) {
+                if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+                cudaGraph_t g = nullptr;
+                DTB_CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+                cudaError_t ce = cudaSuccess;
+                for (uint32_t s = 0; s < rows && ce == cudaSuccess; ++s) {
+                    ce = launch_lif(lb, J_DIRECT, kflags, pm, stream);
+                    if (ce == cudaSuccess) ce = launch_push(lb, 0, wt, push_cfg, push_ctas, stream);
+                }
+                const cudaError_t ee = cudaStreamEndCapture(stream, &g);
+                if (ce != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(ce, "graph capture"); }
+                if (ee != cudaSuccess) return cuda_fail(ee, "cudaStreamEndCapture");
+                const cudaError_t ie = cudaGraphInstantiate(&graph, g, 0);
+                cudaGraphDestroy(g);
+                if (ie != cudaSuccess) { graph = nullptr; return cuda_fail(ie, "cudaGraphInstantiate"); }
+                std::memcpy(graph_key, key, sizeof(key));
+            }
+            DTB_CU(cudaGraphLaunch(graph, stream));
+            ++graph_launches;
+            launches += 2 * rows;
+        } else {
+            for (uint32_t s = 0; s < rows; ++s) {
+                const bool first = (done + s) == 0;
+                if (rq.syn_mode == DTB_SYN_PULL) {
+                    DTB_CU(launch_pull(lb, first ? 0 : 1, wt, kflags, pm, stream));
+                    ++launches;
+                    continue;
+                }
+                DTB_CU(launch_lif(lb, exact ? (first ? J_ASIS : J_FOLD) : J_DIRECT, kflags, pm, stream));
+                if (tune_at == done + s) {
+                    std::vector<NetView> v(m.size());
+                    for (size_t i = 0; i < m.size(); ++i) v[i] = m[i]->view;
+                    DTB_TRY(tune_push_views(lb, v, exact, wt, sm_count, stream, tev, tune));
+                    if (tune.tuned) {
+                        push_cfg = tune.best;
+                        push_tuned[exact] = true;
+                        DTB_CU(push_prepare(exact, wt, push_cfg, sm_count, &push_ctas));
+                    } else {
+                        tune_at += 50;
+                    }
+                }
+                DTB_CU(launch_push(lb, exact, wt, push_cfg, push_ctas, stream));
+                launches += 2;
+            }
+        }
+        if (done + rows == rq.iters) {
+            if (exact) { DTB_CU(launch_fold_finish(lb, stream)); ++launches; }
+            if (rq.syn_mode == DTB_SYN_PULL) { DTB_CU(launch_gather_finish(lb, wt, stream)); ++launches; }
+        }
+        DTB_CU(cudaEventRecord(ev1, stream));
+        DTB_CU(cudaEventSynchronize(ev1));
+        float ms = 0.f;
+        DTB_CU(cudaEventElapsedTime(&ms, ev0, ev1));
+        ms_total += ms;
+        for (size_t i = 0; i < m.size(); ++i) {
+            Engine& e = *m[i];
+            for (uint32_t s = 0; s < rows; ++s) {
+                volatile float tt = e.t + e.dt;
+                e.t = tt;
+            }
+            e.steps += rows;
+            DTB_TRY(e.finish_hist(rows, done, outs[i], freq, vmean, record));
+        }
+        done += rows;
+    }
+    for (size_t i = 0; i < m.size(); ++i) {
+        Engine& e = *m[i];
+        Clock ck;
+        unsigned long long ev = 0;
+        DTB_CU(cudaMemcpyAsync(&ck, e.clock, sizeof(Clock), cudaMemcpyDeviceToHost, stream));
+        DTB_CU(cudaMemcpyAsync(&ev, e.events, sizeof(ev), cudaMemcpyDeviceToHost, stream));
+        DTB_CU(cudaStreamSynchronize(stream));
+        outs[i].events = ev;
+        outs[i].device_ms = ms_total;
+        outs[i].launches = launches;
+        for (int k = 0; k < 4; ++k) outs[i].kernel_ms[k] = 0.0;
+        if (ck.n != e.steps) return fail(DTB_DEVICE_FAULT, "device clock out of step with the host (member " + std::to_string(i) + ")");
+        if (ck.err) return fail(DTB_DEVICE_FAULT, "kernel check failed in member " + std::to_string(i) + ", bits " + std::to_string(ck.err));
+    }
+    return DTB_OK;
+}
+
+}  // namespace dtb
+
+using dtb::Batch;
+using dtb::Engine;
+
+extern "C" {
+
+int32_t dtb_batch_create(void* const* engines, uint32_t n, void** batch) {
+    if (!engines || !batch) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
+    *batch = nullptr;
+    try {
+        auto* b = new Batch();
+        const int s = b->create(reinterpret_cast<Engine* const*>(engines), n);
+        if (s != DTB_OK) { delete b; return s; }
+        *batch = b;
+        return DTB_OK;
+    } catch (const std::bad_alloc&) {
+        return dtb::fail(DTB_OUT_OF_MEMORY, "host allocation failed");
+    }
+}
+
+int32_t dtb_batch_destroy(void* batch) {
+    if (!batch) return dtb::fail(DTB_INVALID_PARAMETER, "NULL batch");
+    delete static_cast<Batch*>(batch);
+    return DTB_OK;
+}
+
+int32_t dtb_batch_run(void* batch, const dtb_run_request* req, dtb_run_output* outs) {
+    if (!batch || !req || !outs) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
+    try {
+        return static_cast<Batch*>(batch)->run(*req, outs);
+    } catch (const std::bad_alloc&) {
+        return dtb::fail(DTB_OUT_OF_MEMORY, "host allocation failed");
+    }
+}
+
+int32_t dtb_batch_set_graph(void* batch, int32_t enable) {
+    if (!batch) return dtb::fail(DTB_INVALID_PARAMETER, "NULL batch");
+    static_cast<Batch*>(batch)->use_graph = enable != 0;
+    return DTB_OK;
+}
+
+int32_t dtb_batch_info(void* batch, uint32_t* n_members, uint32_t* graph_launches, int32_t* push_kind,
+                       int32_t* push_param) {
+    if (!batch) return dtb::fail(DTB_INVALID_PARAMETER, "NULL batch");
+    const Batch* b = static_cast<const Batch*>(batch);
+    if (n_members) *n_members = static_cast<uint32_t>(b->m.size());
+    if (graph_launches) *graph_launches = b->graph_launches;
+    if (push_kind) *push_kind = b->push_cfg.kind;
+    if (push_param) *push_param = b->push_cfg.lpr != 32 ? 1000 + b->push_cfg.lpr : b->push_cfg.param;
+    return DTB_OK;
+}
+
+}  // extern "C"

@@ -708,66 +708,83 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     return DTB_OK;
 }
 
-// Time every push variant on the spike list the LIF kernel just wrote, into a
-// scratch accumulator so the simulation state is untouched, and keep the fastest.
-int Engine::tune_push(const LaunchBatch& b, int exact) {
+// Time every push variant on the spike list the LIF kernel just wrote, into
+// scratch accumulators so the simulation state is untouched, and return the
+// fastest.  `views` are the host copies of the launch's networks.
+int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int exact, int wtype, int sm_count,
+                    cudaStream_t stream, cudaEvent_t ev[2], TuneResult& res) {
+    res.tuned = false;
+    res.report.clear();
     uint32_t count = 0;
-    DTB_CU(cudaMemcpyAsync(&count, list_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    DTB_CU(cudaMemcpyAsync(&count, b.spikes.count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     DTB_CU(cudaStreamSynchronize(stream));
-    if (count < std::max<uint32_t>(64u, n / 5000u)) return DTB_OK;   // too quiet to be representative
+    uint64_t total_n = 0;
+    for (const NetView& v : views) total_n += v.n_pad;
+    if (count < std::max<uint64_t>(64u, total_n / 5000u)) return DTB_OK;   // too quiet to be representative
+    const size_t per = exact ? sizeof(long long) * 4 : sizeof(float4);
     void* scratch = nullptr;
     NetView* tview = nullptr;
-    const size_t sbytes = exact ? sizeof(long long) * 4 * n_pad : sizeof(float4) * n_pad;
-    DTB_CU(cudaMalloc(&scratch, sbytes));
-    if (cudaMalloc(reinterpret_cast<void**>(&tview), sizeof(NetView)) != cudaSuccess) {
+    DTB_CU(cudaMalloc(&scratch, per * total_n));
+    if (cudaMalloc(reinterpret_cast<void**>(&tview), sizeof(NetView) * views.size()) != cudaSuccess) {
         cudaFree(scratch);
         return cuda_fail(cudaErrorMemoryAllocation, "tune_push");
     }
-    NetView v = view;
-    if (exact) v.dJ = static_cast<long long*>(scratch); else v.J = static_cast<float4*>(scratch);
-    int st = DTB_OK;
-    const PushCfg cands[] = {{PUSH_REG, 4}, {PUSH_REG, 8}, {PUSH_REG, 16}, {PUSH_TMA, 256}, {PUSH_TMA, 512}};
-    PushCfg best = push_cfg;
+    std::vector<NetView> tv(views);
+    size_t off = 0;
+    for (NetView& v : tv) {
+        char* base = static_cast<char*>(scratch) + off * per;
+        if (exact) v.dJ = reinterpret_cast<long long*>(base); else v.J = reinterpret_cast<float4*>(base);
+        off += v.n_pad;
+    }
     float best_ms = 1e30f;
-    tune_report.clear();
     auto body = [&]() -> int {
-        DTB_CU(cudaMemcpyAsync(tview, &v, sizeof(NetView), cudaMemcpyHostToDevice, stream));
-        DTB_CU(cudaMemsetAsync(scratch, 0, sbytes, stream));
+        DTB_CU(cudaMemcpyAsync(tview, tv.data(), sizeof(NetView) * tv.size(), cudaMemcpyHostToDevice, stream));
+        DTB_CU(cudaMemsetAsync(scratch, 0, per * total_n, stream));
         LaunchBatch tb = b;
         tb.nets = tview;
-        if (!tune_ev[0]) {
-            DTB_CU(cudaEventCreate(&tune_ev[0]));
-            DTB_CU(cudaEventCreate(&tune_ev[1]));
-        }
-        for (const PushCfg& c : cands) {
+        for (const PushCfg& c : kPushCands) {
             uint32_t ctas = 0;
-            DTB_CU(push_prepare(exact, static_cast<int>(wtype), c, sm_count, &ctas));
+            DTB_CU(push_prepare(exact, wtype, c, sm_count, &ctas));
             float ms_min = 1e30f;
             for (int rep = 0; rep < 3; ++rep) {
-                set_u32_kernel<<<1, 1, 0, stream>>>(list_count, count);
-                DTB_CU(cudaEventRecord(tune_ev[0], stream));
-                DTB_CU(launch_push(tb, exact, static_cast<int>(wtype), c, ctas, stream));
-                DTB_CU(cudaEventRecord(tune_ev[1], stream));
-                DTB_CU(cudaEventSynchronize(tune_ev[1]));
+                set_u32_kernel<<<1, 1, 0, stream>>>(b.spikes.count, count);
+                DTB_CU(cudaEventRecord(ev[0], stream));
+                DTB_CU(launch_push(tb, exact, wtype, c, ctas, stream));
+                DTB_CU(cudaEventRecord(ev[1], stream));
+                DTB_CU(cudaEventSynchronize(ev[1]));
                 float ms = 0.f;
-                DTB_CU(cudaEventElapsedTime(&ms, tune_ev[0], tune_ev[1]));
+                DTB_CU(cudaEventElapsedTime(&ms, ev[0], ev[1]));
                 ms_min = std::min(ms_min, ms);
             }
-            tune_report.push_back({c, ms_min});
-            if (ms_min < best_ms) { best_ms = ms_min; best = c; }
+            res.report.push_back({c, ms_min});
+            if (ms_min < best_ms) { best_ms = ms_min; res.best = c; }
         }
-        set_u32_kernel<<<1, 1, 0, stream>>>(list_count, count);
+        set_u32_kernel<<<1, 1, 0, stream>>>(b.spikes.count, count);
         DTB_CU(cudaGetLastError());
         return DTB_OK;
     };
-    st = body();
+    const int st = body();
     cudaStreamSynchronize(stream);
     cudaFree(scratch);
     cudaFree(tview);
     if (st != DTB_OK) return st;
-    push_cfg = best;
+    res.tuned = true;
+    res.best_ms = best_ms;
+    return DTB_OK;
+}
+
+int Engine::tune_push(const LaunchBatch& b, int exact) {
+    if (!tune_ev[0]) {
+        DTB_CU(cudaEventCreate(&tune_ev[0]));
+        DTB_CU(cudaEventCreate(&tune_ev[1]));
+    }
+    TuneResult res;
+    DTB_TRY(tune_push_views(b, {view}, exact, static_cast<int>(wtype), sm_count, stream, tune_ev, res));
+    if (!res.tuned) return DTB_OK;
+    push_cfg = res.best;
     push_tuned[exact] = true;
-    tuned_ms = best_ms;
+    tuned_ms = res.best_ms;
+    tune_report = res.report;
     DTB_CU(push_prepare(exact, static_cast<int>(wtype), push_cfg, sm_count, &push_ctas));
     return DTB_OK;
 }
@@ -793,7 +810,7 @@ int Engine::info(dtb_engine_info& inf) const {
     inf.has_pull = has_pull;
     inf.per_neuron_params = per_neuron;
     inf.push_kind = static_cast<uint32_t>(push_cfg.kind);
-    inf.push_param = static_cast<uint32_t>(push_cfg.param);
+    inf.push_param = static_cast<uint32_t>(push_cfg.lpr != 32 ? 1000 + push_cfg.lpr : push_cfg.param);
     inf.push_tuned_ms = tuned_ms;
     return DTB_OK;
 }
@@ -1176,10 +1193,16 @@ int32_t dtb_set_push_variant(void* engine, int32_t kind, int32_t param) {
         e->push_tuned[0] = e->push_tuned[1] = false;
         return DTB_OK;
     }
-    const bool ok = (kind == dtb::PUSH_REG && (param == 4 || param == 8 || param == 16)) ||
-                    (kind == dtb::PUSH_TMA && (param == 256 || param == 512));
+    dtb::PushCfg cfg{kind, param, 32};
+    if (kind == dtb::PUSH_REG && param >= 1000) {   // 1000 + lanes per row: sub-warp rows
+        cfg.param = 8;
+        cfg.lpr = param - 1000;
+    }
+    bool ok = false;
+    for (const dtb::PushCfg& c : dtb::kPushCands)
+        ok = ok || (c.kind == cfg.kind && c.param == cfg.param && c.lpr == cfg.lpr);
     if (!ok) return dtb::fail(DTB_INVALID_PARAMETER, "unknown push variant");
-    e->push_cfg = dtb::PushCfg{kind, param};
+    e->push_cfg = cfg;
     e->autotune = false;
     return DTB_OK;
 }
@@ -1190,8 +1213,9 @@ int32_t dtb_tuning_report(void* engine, uint32_t* n, int32_t* kinds, int32_t* pa
     const uint32_t cap = *n;
     *n = static_cast<uint32_t>(e->tune_report.size());
     for (uint32_t i = 0; i < *n && i < cap; ++i) {
-        if (kinds) kinds[i] = e->tune_report[i].cfg.kind;
-        if (params) params[i] = e->tune_report[i].cfg.param;
+        const dtb::PushCfg& c = e->tune_report[i].cfg;
+        if (kinds) kinds[i] = c.kind;
+        if (params) params[i] = c.lpr != 32 ? 1000 + c.lpr : c.param;
         if (ms) ms[i] = e->tune_report[i].ms;
     }
     return DTB_OK;

@@ -21,6 +21,18 @@ int cuda_fail(cudaError_t e, const char* what);
 #define DTB_CU(x) do { cudaError_t e__ = (x); if (e__ != cudaSuccess) return ::dtb::cuda_fail(e__, #x); } while (0)
 #define DTB_TRY(x) do { int s__ = (x); if (s__ != DTB_OK) return s__; } while (0)
 
+struct TuneEntry { PushCfg cfg; float ms; };
+struct TuneResult {
+    bool tuned = false;
+    PushCfg best{PUSH_REG, 8, 32};
+    float best_ms = 0.0f;
+    std::vector<TuneEntry> report;
+};
+__global__ void set_u64_kernel(unsigned long long* p, unsigned long long v);
+__global__ void set_u32_kernel(uint32_t* p, uint32_t v);
+int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int exact, int wtype, int sm_count,
+                    cudaStream_t stream, cudaEvent_t ev[2], TuneResult& res);
+
 class Engine {
 public:
     ~Engine();
@@ -119,12 +131,11 @@ public:
     uint32_t lif_ctas_per_sm = 2;
 
     // push kernel variant (autotuned on the first active run)
-    PushCfg push_cfg{PUSH_REG, 8};
+    PushCfg push_cfg{PUSH_REG, 8, 32};
     uint32_t push_ctas = 0;
     bool autotune = true;
     bool push_tuned[2] = {false, false};
     float tuned_ms = 0.0f;
-    struct TuneEntry { PushCfg cfg; float ms; };
     std::vector<TuneEntry> tune_report;
     int tune_push(const LaunchBatch& b, int exact);
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};

@@ -402,13 +402,15 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
 // ---------------------------------------------------------------------------
 // Push propagation: one warp per spiking row of the out-degree CSR
 // ---------------------------------------------------------------------------
-template <int ACC, int WT, int kPushUnroll>
+template <int ACC, int WT, int kPushUnroll, int LPR>
 __global__ void __launch_bounds__(kPushThreads)
 push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase, uint32_t n_nets, SpikeList sl) {
+    // LPR lanes per row: 32 (a warp per row) or 16 / 8 (2 / 4 rows per warp, for short rows)
+    constexpr uint32_t kGroups = 32 / LPR;
     const uint32_t count = *sl.count;
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lane = (threadIdx.x & 31u) % LPR;
+    const uint32_t gw = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * kGroups + (threadIdx.x & 31u) / LPR;
+    const uint32_t nw = ((gridDim.x * blockDim.x) >> 5) * kGroups;
     const unsigned long long* ptr = nets[0].out_ptr;
     const uint32_t* col = nets[0].out_col;
     const void* wts = nets[0].out_w;
@@ -428,12 +430,12 @@ push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase
         }
         const uint32_t j = v - vb;
         const unsigned long long beg = __ldg(ptr + j), end = __ldg(ptr + j + 1);
-        for (unsigned long long e = beg + lane; e < end; e += 32ull * kPushUnroll) {
+        for (unsigned long long e = beg + lane; e < end; e += static_cast<unsigned long long>(LPR) * kPushUnroll) {
             uint32_t c[kPushUnroll];
             float2 w[kPushUnroll];
 #pragma unroll
             for (int q = 0; q < kPushUnroll; ++q) {
-                const unsigned long long idx = e + 32ull * q;
+                const unsigned long long idx = e + static_cast<unsigned long long>(LPR) * q;
                 if (idx < end) {
                     c[q] = __ldcs(col + idx);
                     w[q] = load_weight<WT>(wts, idx);
@@ -441,7 +443,7 @@ push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase
             }
 #pragma unroll
             for (int q = 0; q < kPushUnroll; ++q) {
-                const unsigned long long idx = e + 32ull * q;
+                const unsigned long long idx = e + static_cast<unsigned long long>(LPR) * q;
                 if (idx < end) {
                     const uint32_t target = c[q] & kIndexMask;
                     const uint32_t kind = c[q] >> 31;
@@ -871,10 +873,16 @@ template <int ACC, int WT>
 static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint32_t ctas, cudaStream_t s) {
     if (cfg.kind == PUSH_REG) {
         const dim3 grid(ctas), block(kPushThreads);
-        switch (cfg.param) {
-            case 4: push_kernel<ACC, WT, 4><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
-            case 16: push_kernel<ACC, WT, 16><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
-            default: push_kernel<ACC, WT, 8><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
+        if (cfg.lpr == 16) {
+            push_kernel<ACC, WT, 8, 16><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes);
+        } else if (cfg.lpr == 8) {
+            push_kernel<ACC, WT, 8, 8><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes);
+        } else {
+            switch (cfg.param) {
+                case 4: push_kernel<ACC, WT, 4, 32><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
+                case 16: push_kernel<ACC, WT, 16, 32><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
+                default: push_kernel<ACC, WT, 8, 32><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes); break;
+            }
         }
     } else {
         const dim3 grid(ctas), block(kTmaWarps * 32);
@@ -894,10 +902,16 @@ static cudaError_t push_prepare_wt(const PushCfg& cfg, int sm_count, uint32_t* c
     int per_sm = 0;
     cudaError_t e = cudaSuccess;
     if (cfg.kind == PUSH_REG) {
-        switch (cfg.param) {
-            case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_kernel<ACC, WT, 4>, kPushThreads, 0); break;
-            case 16: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_kernel<ACC, WT, 16>, kPushThreads, 0); break;
-            default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_kernel<ACC, WT, 8>, kPushThreads, 0); break;
+        if (cfg.lpr == 16) {
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_kernel<ACC, WT, 8, 16>, kPushThreads, 0);
+        } else if (cfg.lpr == 8) {
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_kernel<ACC, WT, 8, 8>, kPushThreads, 0);
+        } else {
+            switch (cfg.param) {
+                case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_kernel<ACC, WT, 4, 32>, kPushThreads, 0); break;
+                case 16: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_kernel<ACC, WT, 16, 32>, kPushThreads, 0); break;
+                default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_kernel<ACC, WT, 8, 32>, kPushThreads, 0); break;
+            }
         }
     } else if (cfg.param == 256) {
         using L = TmaLayout<WT, 256>;
@@ -924,6 +938,10 @@ static cudaError_t push_launch_acc(const LaunchBatch& b, int wt, const PushCfg& 
         default: return push_launch_wt<ACC, W_U8>(b, cfg, ctas, s);
     }
 }
+
+const PushCfg kPushCands[kPushCandidates] = {{PUSH_REG, 4, 32}, {PUSH_REG, 8, 32}, {PUSH_REG, 16, 32},
+                                             {PUSH_REG, 8, 16}, {PUSH_REG, 8, 8},
+                                             {PUSH_TMA, 256, 32}, {PUSH_TMA, 512, 32}};
 
 cudaError_t push_prepare(int exact, int wt, const PushCfg& cfg, int sm_count, uint32_t* ctas) {
     if (exact) {

@@ -29,7 +29,12 @@ struct PushCfg {
     int kind;    // PUSH_REG: register-staged loads, param = synapses in flight per lane (4, 8, 16)
                  // PUSH_TMA: bulk-copy staged rows, param = synapses per stage (256, 512)
     int param;
+    int lpr = 32;  // PUSH_REG: lanes per row (32, 16, 8; sub-warp rows use 8 in flight per lane)
 };
+
+// Every variant the autotuner times.
+constexpr int kPushCandidates = 7;
+extern const PushCfg kPushCands[kPushCandidates];
 // Sets kernel attributes and returns the persistent grid (max resident CTAs).
 cudaError_t push_prepare(int exact, int weight_type, const PushCfg& cfg, int sm_count, uint32_t* ctas);
 cudaError_t launch_push(const LaunchBatch& b, int exact, int weight_type, const PushCfg& cfg, uint32_t ctas,

@@ -111,6 +111,11 @@ SIGNATURES = {
     "dtb_load_state": (_I32, [_P, _P, C.c_uint64]),
     "dtb_build_out_csr_host": (_I32, [_U32, C.c_uint64, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "dtb_compact_spikes": (_I32, [_P, _U32, _P, _P, _P]),
+    "dtb_batch_create": (_I32, [_P, _U32, C.POINTER(C.c_void_p)]),
+    "dtb_batch_destroy": (_I32, [_P]),
+    "dtb_batch_run": (_I32, [_P, _P, _P]),
+    "dtb_batch_set_graph": (_I32, [_P, _I32]),
+    "dtb_batch_info": (_I32, [_P, _P, _P, _P, _P]),
     "dtb_compact_spikes_noalloc": (_I32, [_P, _U32, _P, _P, _P]),
 }
 
@@ -380,3 +385,70 @@ class Engine:
     def load_state(self, blob):
         blob = np.ascontiguousarray(blob, np.uint8)
         _check(LIB.dtb_load_state(self._h, _ptr(blob), blob.shape[0]))
+
+
+class Batch:
+    """Several engines advanced together (dtb_batch_*): one launch per kernel per step."""
+
+    def __init__(self, engines, graph=True):
+        self.engines = list(engines)
+        arr = (C.c_void_p * len(self.engines))(*[e._h.value for e in self.engines])
+        h = C.c_void_p()
+        _check(LIB.dtb_batch_create(arr, len(self.engines), C.byref(h)))
+        self._h = h
+        self.set_graph(graph)
+
+    def set_graph(self, enable):
+        _check(LIB.dtb_batch_set_graph(self._h, int(enable)))
+
+    def info(self):
+        n, g, k, p = C.c_uint32(), C.c_uint32(), C.c_int32(), C.c_int32()
+        _check(LIB.dtb_batch_info(self._h, C.byref(n), C.byref(g), C.byref(k), C.byref(p)))
+        return dict(members=n.value, graph_launches=g.value, push_kind=k.value, push_param=p.value)
+
+    def run(self, iters, use_ou=True, freq=True, vmean=False, record_spikes=False,
+            prop_mode=PROP_THRESHOLD, syn_mode=SYN_PUSH, outs=None):
+        flags = (RUN_USE_OU if use_ou else 0) | (RUN_FREQ if freq else 0) | \
+                (RUN_VMEAN if vmean else 0) | (RUN_RECORD_SPIKES if record_spikes else 0)
+        rq = RunRequest(iters, flags, prop_mode, syn_mode)
+        m = len(self.engines)
+        res = (RunOutput * m)()
+        keep = []
+        for i, e in enumerate(self.engines):
+            if outs is not None:
+                fr, vm = outs[i]
+            else:
+                fr = np.zeros((iters, e.n_pops), np.int32) if freq else None
+                vm = np.zeros((iters, e.n_pops), np.float32) if vmean else None
+            sb = np.zeros((iters, (e.n + 31) // 32), np.uint32) if record_spikes else None
+            keep.append((fr, vm, sb))
+            res[i].freqs = None if fr is None else fr.ctypes.data
+            res[i].vmeans = None if vm is None else vm.ctypes.data
+            res[i].spike_bits = None if sb is None else sb.ctypes.data
+        _check(LIB.dtb_batch_run(self._h, C.byref(rq), res))
+        out = []
+        for i, (fr, vm, sb) in enumerate(keep):
+            spikes = None
+            if sb is not None:
+                n = self.engines[i].n
+                spikes = np.unpackbits(sb.view(np.uint8), axis=1, bitorder="little")[:, :n].astype(bool)
+            out.append(RunResult(fr, vm, spikes, int(res[i].events), float(res[i].device_ms),
+                                 tuple(res[i].kernel_ms), int(res[i].launches)))
+        return out
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            _check(LIB.dtb_batch_destroy(self._h))
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -234,6 +234,23 @@ int32_t dtb_set_noise(void* engine, uint32_t source, uint32_t steps, const float
  * in-HBM spike delivery; outputs land in caller-owned host buffers. */
 int32_t dtb_run(void* engine, const dtb_run_request* req, dtb_run_output* out);
 
+/* --- batched form ---------------------------------------------------------- */
+/* A batch advances several engines (ensemble members, served requests) with one
+ * launch of each per-step kernel; a window of float-push steps is captured once
+ * into a CUDA graph and replayed.  No reference counterpart as an API: the
+ * reference packs an ensemble into one network (data_assimilation/DA_voxel.py:47-52).
+ * Members keep their own state, clock, noise stream and outputs; they must share
+ * the weight type, the device and the noise source.  The engines must outlive the
+ * batch; they stay usable on their own between batch runs. */
+int32_t dtb_batch_create(void* const* engines, uint32_t n, void** batch);
+int32_t dtb_batch_destroy(void* batch);
+/* Run every member `req->iters` steps; outs[i] receives member i's outputs. */
+int32_t dtb_batch_run(void* batch, const dtb_run_request* req, dtb_run_output* outs);
+/* enable != 0: capture float-push windows into a CUDA graph (default). */
+int32_t dtb_batch_set_graph(void* batch, int32_t enable);
+int32_t dtb_batch_info(void* batch, uint32_t* n_members, uint32_t* graph_launches, int32_t* push_kind,
+                       int32_t* push_param);
+
 /* --- state access (tests, checkpoint, serving eviction) ------------------ */
 #define DTB_STATE_V      0  /* float [n]                                       */
 #define DTB_STATE_J      1  /* float [n*4] (AMPA, NMDA, GABAa, GABAb per neuron) */
