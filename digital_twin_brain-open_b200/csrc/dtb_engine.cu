@@ -720,7 +720,7 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
     DTB_CU(cudaStreamSynchronize(stream));
     uint64_t total_n = 0;
     for (const NetView& v : views) total_n += v.n_pad;
-    if (count < std::max<uint64_t>(64u, total_n / 5000u)) return DTB_OK;   // too quiet to be representative
+    if (count < std::max<uint64_t>(64u, total_n / 500u)) return DTB_OK;   // too quiet to be representative
     const size_t per = exact ? sizeof(long long) * 4 : sizeof(float4);
     void* scratch = nullptr;
     NetView* tview = nullptr;

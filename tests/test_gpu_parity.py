@@ -355,7 +355,7 @@ def test_autotuner_picks_a_variant(gpu):
         r = eng.run(1000)
         assert r.freqs[-200:].sum() > 0.005 * 200 * spec.n
         rep = eng.tuning_report()
-        assert len(rep) == 5 and all(ms > 0 for _, _, ms in rep)
+        assert len(rep) == 7 and all(ms > 0 for _, _, ms in rep)
         inf = eng.info()
         assert min(ms for _, _, ms in rep) == pytest.approx(inf.push_tuned_ms)
 
