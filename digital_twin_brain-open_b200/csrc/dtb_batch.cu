@@ -121,6 +121,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
     const bool vmean = (rq.flags & DTB_RUN_VMEAN) != 0;
     const bool record = (rq.flags & DTB_RUN_RECORD_SPIKES) != 0;
     const int exact = rq.syn_mode == DTB_SYN_PUSH_EXACT ? 1 : 0;
+    const bool samples = (rq.flags & (DTB_RUN_SAMPLE_SPIKE | DTB_RUN_SAMPLE_V | DTB_RUN_SAMPLE_IOU)) != 0;
     bool injected = false;
     for (size_t i = 0; i < m.size(); ++i) {
         Engine& e = *m[i];
@@ -143,7 +144,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
     }
     for (Engine* e : m) {
         if (exact) DTB_TRY(e->ensure_dj());
-        DTB_TRY(e->ensure_hist(cap, record));
+        DTB_TRY(e->ensure_hist(cap, record, samples));
     }
     DTB_TRY(refresh_views());
     uint32_t kflags = 0;
@@ -152,6 +153,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
     if (record) kflags |= kFlagRecord;
     if (rq.syn_mode != DTB_SYN_PULL) kflags |= kFlagList;
     if (injected) kflags |= kFlagInjected;
+    if (samples) kflags |= kFlagSample;
     const int pm = static_cast<int>(rq.prop_mode);
     const int wt = static_cast<int>(wtype);
     uint64_t tune_at = ~0ull;
@@ -248,6 +250,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
             }
             e.steps += rows;
             DTB_TRY(e.finish_hist(rows, done, outs[i], freq, vmean, record));
+            if (samples && !e.sample_order.empty()) DTB_TRY(e.finish_samples(rows, done, outs[i]));
         }
         done += rows;
     }

@@ -54,6 +54,7 @@ constexpr uint32_t kFlagStats = 2u;
 constexpr uint32_t kFlagRecord = 4u;
 constexpr uint32_t kFlagList = 8u;       // write the spike list for the push kernel
 constexpr uint32_t kFlagInjected = 16u;
+constexpr uint32_t kFlagSample = 32u;     // record the sampled neurons
 
 // Derived per-population constants (host computes them once per property change).
 struct __align__(16) PopParams {
@@ -112,7 +113,12 @@ struct NetView {
     uint32_t* ticket;              // last-tile counter of the per-step kernels
     const uint32_t* tile_pop;      // [lif_tiles] population of each LIF tile's first neuron
     uint32_t lif_tiles;
-    uint32_t pad1;
+    uint32_t n_samples;            // sampled neurons (set_samples)
+    const uint32_t* sample_bits;   // [n_words] bitmap of sampled neurons
+    const uint32_t* sample_pre;    // [n_words] samples in the words before each word
+    uint8_t* hist_sspk;            // [hist_cap * n_samples] spike of each sampled neuron
+    float* hist_sv;                // [hist_cap * n_samples] V after the step
+    float* hist_siou;              // [hist_cap * n_samples] OU current after the step
 };
 
 // Batch-wide spike list written by the LIF kernel and consumed by the push kernel.

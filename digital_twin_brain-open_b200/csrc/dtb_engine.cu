@@ -199,6 +199,12 @@ int Engine::refresh_view() {
     v.ticket = ticket;
     v.lif_tiles = n_pad / kLifTile;
     v.tile_pop = tile_pop;
+    v.n_samples = n_samples;
+    v.sample_bits = sample_bits;
+    v.sample_pre = sample_pre;
+    v.hist_sspk = hist_sspk;
+    v.hist_sv = hist_sv;
+    v.hist_siou = hist_siou;
     view = v;
     DTB_CU(cudaMemcpyAsync(view_dev, &view, sizeof(NetView), cudaMemcpyHostToDevice, stream));
     DTB_CU(cudaStreamSynchronize(stream));
@@ -514,8 +520,21 @@ int Engine::ensure_dj() {
     return refresh_view();
 }
 
-int Engine::ensure_hist(uint32_t rows, bool record) {
+int Engine::ensure_hist(uint32_t rows, bool record, bool samples) {
     bool changed = false;
+    if (samples && n_samples && sample_cap < std::max(rows, hist_cap)) {
+        dfree(hist_sspk);
+        dfree(hist_sv);
+        dfree(hist_siou);
+        hist_sspk = nullptr;
+        hist_sv = hist_siou = nullptr;
+        const uint32_t r = std::max(rows, hist_cap);
+        DTB_TRY(dalloc(hist_sspk, static_cast<size_t>(r) * n_samples));
+        DTB_TRY(dalloc(hist_sv, static_cast<size_t>(r) * n_samples));
+        DTB_TRY(dalloc(hist_siou, static_cast<size_t>(r) * n_samples));
+        sample_cap = r;
+        changed = true;
+    }
     if (rows > hist_cap) {
         dfree(hist_cnt);
         dfree(hist_vsum);
@@ -550,6 +569,27 @@ int Engine::begin_run_chunk(uint64_t run_base, uint32_t rows, bool stats) {
     if (stats) {
         DTB_CU(cudaMemsetAsync(hist_cnt, 0, sizeof(int) * rows * P, stream));
         DTB_CU(cudaMemsetAsync(hist_vsum, 0, sizeof(long long) * rows * P, stream));
+    }
+    return DTB_OK;
+}
+
+int Engine::finish_samples(uint32_t rows, uint32_t out_row0, const dtb_run_output& out) {
+    const size_t S = n_samples, K = sample_order.size();
+    if (!S) return DTB_OK;
+    std::vector<uint8_t> spk(static_cast<size_t>(rows) * S);
+    std::vector<float> v(static_cast<size_t>(rows) * S), io(static_cast<size_t>(rows) * S);
+    if (out.sample_spike) DTB_CU(cudaMemcpyAsync(spk.data(), hist_sspk, spk.size(), cudaMemcpyDeviceToHost, stream));
+    if (out.sample_v) DTB_CU(cudaMemcpyAsync(v.data(), hist_sv, v.size() * 4, cudaMemcpyDeviceToHost, stream));
+    if (out.sample_iou) DTB_CU(cudaMemcpyAsync(io.data(), hist_siou, io.size() * 4, cudaMemcpyDeviceToHost, stream));
+    DTB_CU(cudaStreamSynchronize(stream));
+    for (uint32_t r = 0; r < rows; ++r) {
+        const size_t dst = static_cast<size_t>(out_row0 + r) * K, src = static_cast<size_t>(r) * S;
+        for (size_t k = 0; k < K; ++k) {
+            const size_t o = src + sample_order[k];
+            if (out.sample_spike) out.sample_spike[dst + k] = spk[o];
+            if (out.sample_v) out.sample_v[dst + k] = v[o];
+            if (out.sample_iou) out.sample_iou[dst + k] = io[o];
+        }
     }
     return DTB_OK;
 }
@@ -590,6 +630,14 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     const bool record = (rq.flags & DTB_RUN_RECORD_SPIKES) != 0;
     if ((freq && !out.freqs) || (vmean && !out.vmeans) || (record && !out.spike_bits))
         return fail(DTB_INVALID_PARAMETER, "requested output buffer is NULL");
+    const bool samples = (rq.flags & (DTB_RUN_SAMPLE_SPIKE | DTB_RUN_SAMPLE_V | DTB_RUN_SAMPLE_IOU)) != 0;
+    if (samples && sample_order.empty())
+        return fail(DTB_UNSET_SAMPLE_FAILURE, "sample outputs requested but no samples are set");
+    if (((rq.flags & DTB_RUN_SAMPLE_SPIKE) && !out.sample_spike) || ((rq.flags & DTB_RUN_SAMPLE_V) && !out.sample_v) ||
+        ((rq.flags & DTB_RUN_SAMPLE_IOU) && !out.sample_iou))
+        return fail(DTB_INVALID_PARAMETER, "requested sample buffer is NULL");
+    if ((rq.flags & DTB_RUN_SAMPLE_IOU) && !(rq.flags & DTB_RUN_USE_OU))
+        return fail(DTB_INVALID_PARAMETER, "sample_iou needs use_ou_background");
     const bool injected = noise_src == DTB_NOISE_INJECTED;
     if (injected) {
         const uint64_t used = steps - inj_first;
@@ -599,8 +647,9 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     if (rq.syn_mode == DTB_SYN_PUSH_EXACT) DTB_TRY(ensure_dj());
     uint32_t cap = std::min<uint32_t>(rq.iters, 4096u);
     if (record) cap = std::min<uint32_t>(cap, std::max<uint32_t>(1u, static_cast<uint32_t>((512ull << 20) / (4ull * n_words))));
-    DTB_TRY(ensure_hist(cap, record));
+    DTB_TRY(ensure_hist(cap, record, samples));
     uint32_t kflags = 0;
+    if (samples) kflags |= kFlagSample;
     if (rq.flags & DTB_RUN_USE_OU) kflags |= kFlagUseOU;
     if (freq || vmean) kflags |= kFlagStats;
     if (record) kflags |= kFlagRecord;
@@ -688,6 +737,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
         }
         steps += rows;
         DTB_TRY(finish_hist(rows, done, out, freq, vmean, record));
+        if (samples) DTB_TRY(finish_samples(rows, done, out));
         done += rows;
     }
     for (int k = 0; k < 4; ++k) out.kernel_ms[k] = kms[k];
@@ -934,6 +984,47 @@ int Engine::set_ou(uint32_t cnt, const uint32_t* pop, const float* mean, const f
         }
     }
     return upload_params();
+}
+
+// Updatesample (dist_simulator.cpp:3635): the neurons whose spike, V and OU
+// current every step reports.  Duplicates are merged; outputs follow the order
+// of first appearance in `idx`.
+int Engine::set_samples(uint32_t count, const uint32_t* idx) {
+    if (count && !idx) return fail(DTB_INVALID_PARAMETER, "NULL sample list");
+    std::vector<uint32_t> bits(n_words, 0);
+    for (uint32_t k = 0; k < count; ++k) {
+        if (idx[k] >= n) return fail(DTB_INVALID_PARAMETER, "sample index outside the network");
+        bits[idx[k] >> 5] |= 1u << (idx[k] & 31u);
+    }
+    std::vector<uint32_t> pre(n_words, 0);
+    uint32_t total = 0;
+    for (uint32_t w = 0; w < n_words; ++w) {
+        pre[w] = total;
+        total += static_cast<uint32_t>(__builtin_popcount(bits[w]));
+    }
+    // slot of each listed neuron (slots are ascending neuron order)
+    sample_order.assign(count, 0);
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint32_t i = idx[k], w = i >> 5, b = i & 31u;
+        sample_order[k] = pre[w] + static_cast<uint32_t>(__builtin_popcount(bits[w] & ((1u << b) - 1u)));
+    }
+    if (!sample_bits) {
+        DTB_TRY(dalloc(sample_bits, n_words));
+        DTB_TRY(dalloc(sample_pre, n_words));
+    }
+    DTB_CU(cudaMemcpyAsync(sample_bits, bits.data(), sizeof(uint32_t) * n_words, cudaMemcpyHostToDevice, stream));
+    DTB_CU(cudaMemcpyAsync(sample_pre, pre.data(), sizeof(uint32_t) * n_words, cudaMemcpyHostToDevice, stream));
+    DTB_CU(cudaStreamSynchronize(stream));
+    if (total != n_samples) {
+        dfree(hist_sspk);
+        dfree(hist_sv);
+        dfree(hist_siou);
+        hist_sspk = nullptr;
+        hist_sv = hist_siou = nullptr;
+        sample_cap = 0;
+    }
+    n_samples = total;
+    return refresh_view();
 }
 
 int Engine::set_noise(uint32_t source, uint32_t rows, const float* z, const float* u) {
@@ -1250,6 +1341,11 @@ int32_t dtb_update_gamma(void* engine, uint32_t n, const uint32_t* pid, const ui
 int32_t dtb_set_ou(void* engine, uint32_t n, const uint32_t* pop, const float* mean, const float* sigma, const float* tau) {
     if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
     return guarded([&] { return as_engine(engine)->set_ou(n, pop, mean, sigma, tau); });
+}
+
+int32_t dtb_set_samples(void* engine, uint32_t n, const uint32_t* neuron_ids) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    return guarded([&] { return as_engine(engine)->set_samples(n, neuron_ids); });
 }
 
 int32_t dtb_set_noise(void* engine, uint32_t source, uint32_t steps, const float* z, const float* u) {

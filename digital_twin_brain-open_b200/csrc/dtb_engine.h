@@ -50,6 +50,7 @@ public:
     int update_gamma(uint32_t n, const uint32_t* pid, const uint32_t* pop, const float* alpha, const float* beta);
     int set_ou(uint32_t n, const uint32_t* pop, const float* mean, const float* sigma, const float* tau);
     int set_noise(uint32_t source, uint32_t steps, const float* z, const float* u);
+    int set_samples(uint32_t count, const uint32_t* idx);
     int read_state(int which, void* dst);
     int write_state(int which, const void* src);
     int read_out_csr(uint32_t* n_rows, uint64_t* n_edges, uint32_t* rows, uint64_t* row_ptr, uint32_t* post,
@@ -62,9 +63,10 @@ public:
     LaunchBatch single_batch() const;
     int refresh_view();
     int ensure_dj();
-    int ensure_hist(uint32_t rows, bool record);
+    int ensure_hist(uint32_t rows, bool record, bool samples = false);
     int begin_run_chunk(uint64_t run_base, uint32_t rows, bool stats);
     int finish_hist(uint32_t rows, uint32_t out_row0, const dtb_run_output& out, bool freq, bool vmean, bool record);
+    int finish_samples(uint32_t rows, uint32_t out_row0, const dtb_run_output& out);
 
     // identity
     int device = 0;
@@ -120,6 +122,13 @@ public:
     long long* hist_vsum = nullptr;
     uint32_t* rec_bits = nullptr;
     uint32_t hist_cap = 0, rec_cap = 0;
+    uint32_t n_samples = 0, sample_cap = 0;
+    uint32_t* sample_bits = nullptr;
+    uint32_t* sample_pre = nullptr;
+    uint8_t* hist_sspk = nullptr;
+    float* hist_sv = nullptr;
+    float* hist_siou = nullptr;
+    std::vector<uint32_t> sample_order;   // sample slot -> position in the caller's list
     float* inj_z = nullptr;
     float* inj_u = nullptr;
     NetView* view_dev = nullptr;

@@ -345,6 +345,24 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
                 if (record) nv.rec_bits[static_cast<size_t>(row) * nv.n_words + word] = wact;
             }
         }
+        // ---- sampled neurons (stat_samples_kernel, src/stage/stat_result.cpp:393-431)
+        if ((flags & kFlagSample) && nv.n_samples && row >= 0 && row < static_cast<long long>(nv.hist_cap)) {
+            const uint32_t word = i0 >> 5, sh = i0 & 31u;
+            const uint32_t sb = (__ldg(nv.sample_bits + word) >> sh) & 0xFu;
+            if (sb) {
+                uint32_t slot = __ldg(nv.sample_pre + word) + __popc(__ldg(nv.sample_bits + word) & ((1u << sh) - 1u));
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if ((sb >> k) & 1u) {
+                        const size_t o = static_cast<size_t>(row) * nv.n_samples + slot;
+                        nv.hist_sspk[o] = static_cast<uint8_t>((nib_act >> k) & 1u);
+                        nv.hist_sv[o] = Vv[k];
+                        nv.hist_siou[o] = Iv[k];
+                        ++slot;
+                    }
+                }
+            }
+        }
 
         // ---- population statistics: warp-uniform fast path, else per-thread slots
         if (stats) {
@@ -769,6 +787,16 @@ lif_pull_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ t
     }
     const uint32_t wprop = __ballot_sync(0xffffffffu, sp);
     const uint32_t wact = __ballot_sync(0xffffffffu, active);
+    if ((flags & kFlagSample) && nv.n_samples && valid && row >= 0 && row < static_cast<long long>(nv.hist_cap)) {
+        const uint32_t sbw = __ldg(nv.sample_bits + (i >> 5));
+        if ((sbw >> (i & 31u)) & 1u) {
+            const uint32_t slot = __ldg(nv.sample_pre + (i >> 5)) + __popc(sbw & ((1u << (i & 31u)) - 1u));
+            const size_t o = static_cast<size_t>(row) * nv.n_samples + slot;
+            nv.hist_sspk[o] = active ? 1 : 0;
+            nv.hist_sv[o] = vnew;
+            nv.hist_siou[o] = nv.iou[i];
+        }
+    }
     if (lane == 0) {
         uint32_t* bits = parity ? nv.bits1 : nv.bits0;
         bits[base >> 5] = wprop;

@@ -25,6 +25,7 @@ PROP_THRESHOLD, PROP_NOISE, PROP_OR = 0, 1, 2
 SYN_PUSH, SYN_PUSH_EXACT, SYN_PULL = 0, 1, 2
 NOISE_PHILOX, NOISE_INJECTED = 0, 1
 RUN_USE_OU, RUN_FREQ, RUN_VMEAN, RUN_RECORD_SPIKES, RUN_TIME_KERNELS = 1, 2, 4, 8, 16
+RUN_SAMPLE_SPIKE, RUN_SAMPLE_V, RUN_SAMPLE_IOU = 32, 64, 128
 STATE_V, STATE_J, STATE_I_OU, STATE_T_LAST = 0, 1, 2, 3
 
 # snn.proto PropType
@@ -76,7 +77,8 @@ class RunRequest(C.Structure):
 class RunOutput(C.Structure):
     _fields_ = [("freqs", C.c_void_p), ("vmeans", C.c_void_p), ("spike_bits", C.c_void_p),
                 ("events", C.c_uint64), ("device_ms", C.c_double), ("kernel_ms", C.c_double * 4),
-                ("launches", C.c_uint32), ("reserved", C.c_uint32)]
+                ("launches", C.c_uint32), ("reserved", C.c_uint32), ("sample_spike", C.c_void_p),
+                ("sample_v", C.c_void_p), ("sample_iou", C.c_void_p)]
 
 
 _P = C.c_void_p
@@ -102,6 +104,7 @@ SIGNATURES = {
     "dtb_update_gamma": (_I32, [_P, _U32, _P, _P, _P, _P]),
     "dtb_set_ou": (_I32, [_P, _U32, _P, _P, _P, _P]),
     "dtb_set_noise": (_I32, [_P, _U32, _U32, _P, _P]),
+    "dtb_set_samples": (_I32, [_P, _U32, _P]),
     "dtb_run": (_I32, [_P, _P, _P]),
     "dtb_read_state": (_I32, [_P, _I32, _P]),
     "dtb_write_state": (_I32, [_P, _I32, _P]),
@@ -199,6 +202,9 @@ class RunResult:
     device_ms: float
     kernel_ms: tuple = (0.0, 0.0, 0.0, 0.0)   # LIF, push, pull, end-of-run (with time_kernels)
     launches: int = 0
+    sample_spike: np.ndarray | None = None   # uint8 [iters, n_samples]
+    sample_v: np.ndarray | None = None
+    sample_iou: np.ndarray | None = None
 
 
 class Engine:
@@ -322,19 +328,30 @@ class Engine:
         u = None if u is None else _f32(u)
         _check(LIB.dtb_set_noise(self._h, NOISE_INJECTED, z.shape[0], _ptr(z), _ptr(u)))
 
+    def set_samples(self, neuron_ids):
+        idx = _u32(neuron_ids)
+        _check(LIB.dtb_set_samples(self._h, idx.shape[0], _ptr(idx)))
+        self.n_sample_list = int(idx.shape[0])
+
     def set_noise_philox(self):
         _check(LIB.dtb_set_noise(self._h, NOISE_PHILOX, 0, None, None))
 
     # ---- stepping
     def run(self, iters, use_ou=True, freq=True, vmean=False, record_spikes=False,
-            prop_mode=PROP_THRESHOLD, syn_mode=SYN_PUSH, time_kernels=False, out=None):
+            prop_mode=PROP_THRESHOLD, syn_mode=SYN_PUSH, time_kernels=False, out=None,
+            sample_spike=False, sample_v=False, sample_iou=False):
         """Advance ``iters`` steps (RunRequest, snn.proto:63-77).
 
         ``out`` may pass preallocated (freqs, vmeans) host arrays of shape [iters, P].
         """
         flags = (RUN_USE_OU if use_ou else 0) | (RUN_FREQ if freq else 0) | \
                 (RUN_VMEAN if vmean else 0) | (RUN_RECORD_SPIKES if record_spikes else 0) | \
-                (RUN_TIME_KERNELS if time_kernels else 0)
+                (RUN_TIME_KERNELS if time_kernels else 0) | (RUN_SAMPLE_SPIKE if sample_spike else 0) | \
+                (RUN_SAMPLE_V if sample_v else 0) | (RUN_SAMPLE_IOU if sample_iou else 0)
+        ns = getattr(self, "n_sample_list", 0)
+        ss = np.zeros((iters, ns), np.uint8) if sample_spike else None
+        sv = np.zeros((iters, ns), np.float32) if sample_v else None
+        si = np.zeros((iters, ns), np.float32) if sample_iou else None
         rq = RunRequest(iters, flags, prop_mode, syn_mode)
         if out is not None:
             fr, vm = out
@@ -345,11 +362,15 @@ class Engine:
         sb = np.zeros((iters, words), np.uint32) if record_spikes else None
         res = RunOutput(None if fr is None else fr.ctypes.data, None if vm is None else vm.ctypes.data,
                         None if sb is None else sb.ctypes.data, 0, 0.0)
+        res.sample_spike = None if ss is None else ss.ctypes.data
+        res.sample_v = None if sv is None else sv.ctypes.data
+        res.sample_iou = None if si is None else si.ctypes.data
         _check(LIB.dtb_run(self._h, C.byref(rq), C.byref(res)))
         spikes = None
         if sb is not None:
             spikes = np.unpackbits(sb.view(np.uint8), axis=1, bitorder="little")[:, :self.n].astype(bool)
-        return RunResult(fr, vm, spikes, int(res.events), float(res.device_ms), tuple(res.kernel_ms), int(res.launches))
+        return RunResult(fr, vm, spikes, int(res.events), float(res.device_ms), tuple(res.kernel_ms), int(res.launches),
+                         ss, sv, si)
 
     # ---- state
     def read_state(self, which):
@@ -407,9 +428,10 @@ class Batch:
         return dict(members=n.value, graph_launches=g.value, push_kind=k.value, push_param=p.value)
 
     def run(self, iters, use_ou=True, freq=True, vmean=False, record_spikes=False,
-            prop_mode=PROP_THRESHOLD, syn_mode=SYN_PUSH, outs=None):
+            prop_mode=PROP_THRESHOLD, syn_mode=SYN_PUSH, outs=None, sample_spike=False):
         flags = (RUN_USE_OU if use_ou else 0) | (RUN_FREQ if freq else 0) | \
-                (RUN_VMEAN if vmean else 0) | (RUN_RECORD_SPIKES if record_spikes else 0)
+                (RUN_VMEAN if vmean else 0) | (RUN_RECORD_SPIKES if record_spikes else 0) | \
+                (RUN_SAMPLE_SPIKE if sample_spike else 0)
         rq = RunRequest(iters, flags, prop_mode, syn_mode)
         m = len(self.engines)
         res = (RunOutput * m)()
@@ -421,19 +443,21 @@ class Batch:
                 fr = np.zeros((iters, e.n_pops), np.int32) if freq else None
                 vm = np.zeros((iters, e.n_pops), np.float32) if vmean else None
             sb = np.zeros((iters, (e.n + 31) // 32), np.uint32) if record_spikes else None
-            keep.append((fr, vm, sb))
+            ss = np.zeros((iters, getattr(e, "n_sample_list", 0)), np.uint8) if sample_spike else None
+            keep.append((fr, vm, sb, ss))
+            res[i].sample_spike = None if ss is None else ss.ctypes.data
             res[i].freqs = None if fr is None else fr.ctypes.data
             res[i].vmeans = None if vm is None else vm.ctypes.data
             res[i].spike_bits = None if sb is None else sb.ctypes.data
         _check(LIB.dtb_batch_run(self._h, C.byref(rq), res))
         out = []
-        for i, (fr, vm, sb) in enumerate(keep):
+        for i, (fr, vm, sb, ss) in enumerate(keep):
             spikes = None
             if sb is not None:
                 n = self.engines[i].n
                 spikes = np.unpackbits(sb.view(np.uint8), axis=1, bitorder="little")[:, :n].astype(bool)
             out.append(RunResult(fr, vm, spikes, int(res[i].events), float(res[i].device_ms),
-                                 tuple(res[i].kernel_ms), int(res[i].launches)))
+                                 tuple(res[i].kernel_ms), int(res[i].launches), ss))
         return out
 
     def close(self):

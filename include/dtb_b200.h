@@ -149,6 +149,9 @@ typedef struct dtb_engine_info {
 #define DTB_RUN_VMEAN         (1u << 2)  /* output_vmean                                      */
 #define DTB_RUN_RECORD_SPIKES (1u << 3)  /* copy every step's threshold-spike bitmap out      */
 #define DTB_RUN_TIME_KERNELS  (1u << 4)  /* time every kernel launch with CUDA events          */
+#define DTB_RUN_SAMPLE_SPIKE  (1u << 5)  /* output_sample_spike: spikes of the sampled neurons */
+#define DTB_RUN_SAMPLE_V      (1u << 6)  /* output_sample_vmemb                                 */
+#define DTB_RUN_SAMPLE_IOU    (1u << 7)  /* output_sample_iou (needs DTB_RUN_USE_OU)            */
 
 typedef struct dtb_run_request {
     uint32_t iters;      /* RunRequest.iter; > 0                                                */
@@ -169,6 +172,9 @@ typedef struct dtb_run_output {
                                push, pull and end-of-run kernels                               */
     uint32_t launches;      /* out: kernels launched by this run                               */
     uint32_t reserved;
+    uint8_t* sample_spike;  /* [iters * n_samples] in the order given to dtb_set_samples          */
+    float* sample_v;        /* [iters * n_samples]                                               */
+    float* sample_iou;      /* [iters * n_samples]                                               */
 } dtb_run_output;
 
 /* --- version and errors ------------------------------------------------- */
@@ -223,6 +229,13 @@ int32_t dtb_update_gamma(void* engine, uint32_t n, const uint32_t* prop_ids,
  * first time it is configured, as the reference does. */
 int32_t dtb_set_ou(void* engine, uint32_t n, const uint32_t* pop_ids, const float* mean,
                    const float* sigma, const float* tau);
+
+/* Updatesample (tools/dist_simulator.cpp:3635; stat_samples_kernel,
+ * src/stage/stat_result.cpp:393-431): neurons whose spike, membrane potential
+ * and OU current each step reports through the DTB_RUN_SAMPLE_* outputs.
+ * Requesting sample outputs with no samples set returns DTB_UNSET_SAMPLE_FAILURE,
+ * as the reference's Run validation does (dist_simulator.cpp:3225-3234). */
+int32_t dtb_set_samples(void* engine, uint32_t n, const uint32_t* neuron_ids);
 
 /* Noise source for subsequent steps.  DTB_NOISE_INJECTED takes `steps` rows of
  * n_neurons normal draws `z` and (optionally) uniforms `u`, consumed one row per

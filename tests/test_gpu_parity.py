@@ -381,3 +381,32 @@ def test_compact_spikes_operator(gpu, n):
     c = int(cnt.item())
     assert c == ref.size
     assert np.array_equal(idx[:c].cpu().numpy().astype(np.int64), ref)
+
+
+def test_samples_follow_oracle(gpu, block10k):
+    """Updatesample + output_sample_*: per-step spike, V and OU current of chosen neurons."""
+    steps = 300
+    z, _ = lo.torch_noise_stream(6, 10_000, steps, False)
+    idx = np.array([5, 9999, 17, 3, 17, 4242])
+    o = lo.LifOracle(block10k)
+    vs, ios, sps = [], [], []
+    for s in range(steps):
+        a, _ = o.step(z[s])
+        vs.append(o.V[idx].copy())
+        ios.append(o.i_bg[idx].copy())
+        sps.append(a[idx].copy())
+    with E.Engine.from_arrays(block10k, pull=True) as eng:
+        with pytest.raises(E.DtbError) as ei:
+            eng.run(5, sample_spike=True)
+        assert ei.value.status == E.UNSET_SAMPLE_FAILURE
+        eng.set_samples(idx)
+        eng.set_noise_injected(z)
+        r1 = eng.run(150, syn_mode=E.SYN_PUSH_EXACT, sample_spike=True, sample_v=True, sample_iou=True)
+        r2 = eng.run(150, syn_mode=E.SYN_PULL, sample_spike=True, sample_v=True, sample_iou=True)
+    sv = np.concatenate([r1.sample_v, r2.sample_v])
+    si = np.concatenate([r1.sample_iou, r2.sample_iou])
+    ss = np.concatenate([r1.sample_spike, r2.sample_spike])
+    assert np.array_equal(sv, np.array(vs))
+    assert np.array_equal(si, np.array(ios))
+    assert np.array_equal(ss.astype(bool), np.array(sps))
+    assert ss.sum() > 0
