@@ -385,7 +385,7 @@ def test_compact_spikes_operator(gpu, n):
 
 def test_samples_follow_oracle(gpu, block10k):
     """Updatesample + output_sample_*: per-step spike, V and OU current of chosen neurons."""
-    steps = 300
+    steps = 600
     z, _ = lo.torch_noise_stream(6, 10_000, steps, False)
     idx = np.array([5, 9999, 17, 3, 17, 4242])
     o = lo.LifOracle(block10k)
@@ -401,8 +401,8 @@ def test_samples_follow_oracle(gpu, block10k):
         assert ei.value.status == E.UNSET_SAMPLE_FAILURE
         eng.set_samples(idx)
         eng.set_noise_injected(z)
-        r1 = eng.run(150, syn_mode=E.SYN_PUSH_EXACT, sample_spike=True, sample_v=True, sample_iou=True)
-        r2 = eng.run(150, syn_mode=E.SYN_PULL, sample_spike=True, sample_v=True, sample_iou=True)
+        r1 = eng.run(300, syn_mode=E.SYN_PUSH_EXACT, sample_spike=True, sample_v=True, sample_iou=True)
+        r2 = eng.run(300, syn_mode=E.SYN_PULL, sample_spike=True, sample_v=True, sample_iou=True)
     sv = np.concatenate([r1.sample_v, r2.sample_v])
     si = np.concatenate([r1.sample_iou, r2.sample_iou])
     ss = np.concatenate([r1.sample_spike, r2.sample_spike])
