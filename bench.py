@@ -40,6 +40,8 @@ BYTES_STATE = 56          # V, J x4, i_ou, t_last read + written per neuron per 
 CSR_COL_BYTES = 4
 ACC_BYTES = 8             # one logical accumulator update (a float pair) per event
 ROW_BYTES = 12            # rowptr pair + spike-list entry per spiking row
+PUSH_KINDS = ["reg", "tma", "local"]
+PUSH_KERNELS = ["push_kernel", "push_tma_kernel", "push_kernel (cross-population) + push_local_kernel (windows)"]
 
 
 def parse():
@@ -53,7 +55,7 @@ def parse():
     p.add_argument("--neurons", type=int, default=N_NEURONS, help="network size (profiling runs use a small one)")
     p.add_argument("--pops", type=int, default=N_POPS)
     p.add_argument("--degree", type=int, default=IN_DEGREE)
-    p.add_argument("--push", default="auto", help="push kernel: auto (autotuned), reg:4|8|16, tma:256|512")
+    p.add_argument("--push", default="auto", help="push kernel: auto (autotuned), reg:4|8|16|1016|1008, tma:256|512, local:8|1016")
     p.add_argument("--form", default="plain", choices=["plain", "ensemble"],
                    help="plain: the 5M-neuron network; ensemble: 64 DA members batched (BF16) vs sequential (FP32)")
     p.add_argument("--members", type=int, default=64)
@@ -201,7 +203,7 @@ def run_ours(args):
     build_s = time.perf_counter() - t0
     if args.push != "auto":
         kind, param = args.push.split(":")
-        eng.set_push_variant({"reg": 0, "tma": 1}[kind], int(param))
+        eng.set_push_variant(PUSH_KINDS.index(kind), int(param))
     info = eng.info()
     stream = torch.cuda.ExternalStream(eng.stream(), device=dev)
     P = eng.n_pops
@@ -237,7 +239,7 @@ def run_ours(args):
     ms = start.elapsed_time(end)
 
     info = eng.info()
-    tuning = [{"kernel": ("reg" if k == 0 else "tma"), "param": p, "ms": m} for k, p, m in eng.tuning_report()]
+    tuning = [{"kernel": PUSH_KINDS[k], "param": p, "ms": m} for k, p, m in eng.tuning_report()]
     # per-kernel timing window (after the timed region)
     rk = eng.run(WINDOW, freq=True, out=(fr, None), time_kernels=True)
     lif_ms, push_ms = rk.kernel_ms[0] / WINDOW, rk.kernel_ms[1] / WINDOW
@@ -300,10 +302,11 @@ def run_ours(args):
                              f"{info.n_neurons * 56 / 1e6:.0f} MB neuron state)",
                        "device_bytes": int(info.device_bytes), "build_s": build_s,
                        "lif_ms_per_step": lif_ms, "push_ms_per_step": push_ms,
-                       "push_variant": ("reg" if info.push_kind == 0 else "tma") + f":{info.push_param}",
+                       "push_variant": PUSH_KINDS[info.push_kind] + f":{info.push_param}",
+                       "local_windows": int(info.local_windows),
                        "push_autotune": tuning,
                        "step_roofline_frac": step_bytes / ((lif_ms + push_ms) * 1e-3) / 1e9 / peak},
-            "roofline": {"bound": "hbm", "kernel": "push_kernel", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": PUSH_KERNELS[info.push_kind], "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "algorithmic_bytes_per_launch": push_bytes},
             "cpu_baseline": cpu,

@@ -10,7 +10,7 @@
 // nothing extra: tiles and spiking rows are distributed over the whole GPU.
 //
 // A window of steps of the float push mode is captured once into a CUDA graph
-// (2 kernel nodes per step) and replayed per window; the push variant is chosen by
+// (2 kernel nodes per step, 3 with the population-local push) and replayed per window; the push variant is chosen by
 // the same on-line autotuner as a single engine's, on the batch's own spike list.
 #include <algorithm>
 #include <cstring>
@@ -32,7 +32,7 @@ public:
     int sm_count = 148;
     uint32_t wtype = W_F32;
     NetView* d_views = nullptr;
-    uint32_t* d_prefix = nullptr;     // [lif n+1][pull n+1][vbase n+1]
+    uint32_t* d_prefix = nullptr;     // [lif n+1][pull n+1][vbase n+1][local windows n+1]
     uint32_t* list = nullptr;
     uint32_t* list_count = nullptr;
     uint32_t* list_ticket = nullptr;
@@ -40,6 +40,7 @@ public:
     PushCfg push_cfg{PUSH_REG, 8, 32};
     uint32_t push_ctas = 0;
     bool push_tuned[2] = {false, false};
+    bool autotune = true;
     TuneResult tune;
     bool use_graph = true;
     cudaGraphExec_t graph = nullptr;
@@ -75,7 +76,7 @@ int Batch::create(Engine* const* engines, uint32_t n) {
     DTB_CU(cudaEventCreate(&ev1));
     DTB_CU(cudaEventCreate(&tev[0]));
     DTB_CU(cudaEventCreate(&tev[1]));
-    std::vector<uint32_t> pre(3 * (n + 1), 0);
+    std::vector<uint32_t> pre(4 * (n + 1), 0);
     uint64_t total = 0;
     for (uint32_t i = 0; i < n; ++i) {
         pre[i + 1] = pre[i] + m[i]->n_pad / kLifTile;
@@ -83,6 +84,7 @@ int Batch::create(Engine* const* engines, uint32_t n) {
         total += m[i]->n_pad;
         if (total >= 0xFFFFFFFFull) return fail(DTB_UNSUPPORTED, "a batch holds at most 2^32 neurons");
         pre[2 * (n + 1) + i + 1] = static_cast<uint32_t>(total);
+        pre[3 * (n + 1) + i + 1] = pre[3 * (n + 1) + i] + m[i]->n_windows;
     }
     DTB_CU(cudaMalloc(reinterpret_cast<void**>(&d_views), sizeof(NetView) * n));
     DTB_CU(cudaMalloc(reinterpret_cast<void**>(&d_prefix), sizeof(uint32_t) * pre.size()));
@@ -102,6 +104,8 @@ int Batch::create(Engine* const* engines, uint32_t n) {
     lb.push_ctas = static_cast<uint32_t>(sm_count) * 8u;
     lb.lif_ctas = static_cast<uint32_t>(sm_count) * m[0]->lif_ctas_per_sm;
     lb.spikes = SpikeList{list, list_count, list_ticket, static_cast<uint32_t>(total)};
+    lb.win_prefix = d_prefix + 3 * (n + 1);
+    lb.windows_total = pre[3 * (n + 1) + n];
     DTB_CU(cudaStreamSynchronize(stream));
     return DTB_OK;
 }
@@ -159,7 +163,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
     uint64_t tune_at = ~0ull;
     if (rq.syn_mode != DTB_SYN_PULL) {
         DTB_CU(push_prepare(exact, wt, push_cfg, sm_count, &push_ctas));
-        if (!push_tuned[exact]) {
+        if (autotune && !push_tuned[exact]) {
             const uint64_t settle = 300;
             const uint64_t st = m[0]->steps;
             tune_at = st >= settle ? 1 : (settle - st < rq.iters ? settle - st : ~0ull);
@@ -207,7 +211,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
             }
             DTB_CU(cudaGraphLaunch(graph, stream));
             ++graph_launches;
-            launches += 2 * rows;
+            launches += (2 + push_extra_launches(lb, 0, push_cfg)) * rows;
         } else {
             for (uint32_t s = 0; s < rows; ++s) {
                 const bool first = (done + s) == 0;
@@ -230,7 +234,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
                     }
                 }
                 DTB_CU(launch_push(lb, exact, wt, push_cfg, push_ctas, stream));
-                launches += 2;
+                launches += 2 + push_extra_launches(lb, exact, push_cfg);
             }
         }
         if (done + rows == rq.iters) {
@@ -310,6 +314,21 @@ int32_t dtb_batch_run(void* batch, const dtb_run_request* req, dtb_run_output* o
 int32_t dtb_batch_set_graph(void* batch, int32_t enable) {
     if (!batch) return dtb::fail(DTB_INVALID_PARAMETER, "NULL batch");
     static_cast<Batch*>(batch)->use_graph = enable != 0;
+    return DTB_OK;
+}
+
+int32_t dtb_batch_set_push_variant(void* batch, int32_t kind, int32_t param) {
+    if (!batch) return dtb::fail(DTB_INVALID_PARAMETER, "NULL batch");
+    Batch* b = static_cast<Batch*>(batch);
+    if (kind < 0) {
+        b->autotune = true;
+        b->push_tuned[0] = b->push_tuned[1] = false;
+        return DTB_OK;
+    }
+    dtb::PushCfg cfg;
+    if (!dtb::push_cfg_from_abi(kind, param, cfg)) return dtb::fail(DTB_INVALID_PARAMETER, "unknown push variant");
+    b->push_cfg = cfg;
+    b->autotune = false;
     return DTB_OK;
 }
 

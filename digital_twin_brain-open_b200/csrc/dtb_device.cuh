@@ -26,6 +26,7 @@ constexpr int kLifTile = 1024;          // neurons per LIF CTA: 256 threads x 4 
 constexpr int kPullThreads = 256;
 constexpr int kPullTile = 256;          // neurons per pull CTA: 8 warps x 32 neurons
 constexpr int kPad = 1024;              // every per-neuron array is padded to a multiple of this
+constexpr uint32_t kLocalWin = 13312;   // neurons per local-push window: 4 receptor planes of 32-bit sums, 208 KiB
 constexpr uint32_t kKindBit = 0x80000000u;
 constexpr uint32_t kIndexMask = 0x7fffffffu;
 constexpr float kFixScale = 4294967296.0f;          // 2^32: fixed-point unit of dJ
@@ -119,6 +120,15 @@ struct NetView {
     uint8_t* hist_sspk;            // [hist_cap * n_samples] spike of each sampled neuron
     float* hist_sv;                // [hist_cap * n_samples] V after the step
     float* hist_siou;              // [hist_cap * n_samples] OU current after the step
+    // Population-local push (rows sorted by postsynaptic neuron).  A population
+    // with local windows is cut into pop_loc[a].x windows of pop_loc[a].y neurons;
+    // row j keeps, for each boundary k of its own population's windows, the offset
+    // inside the row of the first synapse at or past that boundary.
+    const uint2* own_seg;          // [n] own-population synapses of row j: [beg + x, beg + y); {0,0} = none local
+    const uint32_t* woff;          // row j of population a: woff[rb(a) + (j - pop_off[a]) * (k_a + 1) + k]
+    const uint4* pop_loc;          // [n_pops] {k_a, window width, rb(a) low word, rb(a) high word}
+    const uint4* win_tab;          // [n_windows] {population, first neuron, end neuron, window index | s << 16}
+    uint32_t n_windows;
 };
 
 // Batch-wide spike list written by the LIF kernel and consumed by the push kernel.

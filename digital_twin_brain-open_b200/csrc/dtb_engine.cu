@@ -205,6 +205,11 @@ int Engine::refresh_view() {
     v.hist_sspk = hist_sspk;
     v.hist_sv = hist_sv;
     v.hist_siou = hist_siou;
+    v.own_seg = own_seg;
+    v.woff = woff;
+    v.pop_loc = pop_loc;
+    v.win_tab = win_tab;
+    v.n_windows = n_windows;
     view = v;
     DTB_CU(cudaMemcpyAsync(view_dev, &view, sizeof(NetView), cudaMemcpyHostToDevice, stream));
     DTB_CU(cudaStreamSynchronize(stream));
@@ -223,7 +228,100 @@ LaunchBatch Engine::single_batch() const {
     b.push_ctas = static_cast<uint32_t>(sm_count) * 8u;
     b.lif_ctas = static_cast<uint32_t>(sm_count) * lif_ctas_per_sm;
     b.spikes = SpikeList{list, list_count, list_ticket, n_pad};
+    b.win_prefix = prefix_dev + 6;
+    b.windows_total = n_windows;
     return b;
+}
+
+// (kind, param) of dtb_set_push_variant -> one of the tuner's candidates;
+// param 1000 + lanes per row selects sub-warp rows.
+bool push_cfg_from_abi(int kind, int param, PushCfg& cfg) {
+    cfg = PushCfg{kind, param, 32};
+    if ((kind == PUSH_REG || kind == PUSH_LOCAL) && param >= 1000) {
+        cfg.param = 8;
+        cfg.lpr = param - 1000;
+    }
+    for (const PushCfg& c : kPushCands)
+        if (c.kind == cfg.kind && c.param == cfg.param && c.lpr == cfg.lpr) return true;
+    return false;
+}
+
+// Population-local push tables.  A population gets k = ceil(size / kLocalWin)
+// windows when its rows carry, on average, at least kLocalMinSpan own-population
+// synapses per window and its window sums fit 32-bit fixed point at a
+// resolution of 2^-kLocalMinShift or finer; other populations stay with the
+// scattered push.
+constexpr double kLocalMinSpan = 32.0;
+constexpr int kLocalMinShift = 16;
+constexpr int kLocalMaxShift = 60;
+
+int Engine::build_local_tables() {
+    if (!has_push || n == 0) return DTB_OK;
+    // pass 1: sortedness, own-population in-degree per neuron, max |w| per population
+    uint32_t* d_tmp = nullptr;
+    const size_t tmp_words = static_cast<size_t>(n) + P + 1;
+    DTB_CU(cudaMalloc(reinterpret_cast<void**>(&d_tmp), sizeof(uint32_t) * tmp_words));
+    std::vector<uint32_t> cnt(n), maxw(P);
+    uint32_t unsorted = 0;
+    auto pass1 = [&]() -> int {
+        DTB_CU(cudaMemsetAsync(d_tmp, 0, sizeof(uint32_t) * tmp_words, stream));
+        DTB_CU(build_local_offsets(out_ptr, out_col, out_w, static_cast<int>(wtype), pop_off_dev, P, n, nullptr, d_tmp,
+                                   d_tmp + n, nullptr, nullptr, d_tmp + n + P, stream));
+        DTB_CU(cudaMemcpyAsync(cnt.data(), d_tmp, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, stream));
+        DTB_CU(cudaMemcpyAsync(maxw.data(), d_tmp + n, sizeof(uint32_t) * P, cudaMemcpyDeviceToHost, stream));
+        DTB_CU(cudaMemcpyAsync(&unsorted, d_tmp + n + P, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        DTB_CU(cudaStreamSynchronize(stream));
+        return DTB_OK;
+    };
+    const int st = pass1();
+    cudaFree(d_tmp);
+    if (st != DTB_OK) return st;
+    if (unsorted) return DTB_OK;
+    std::vector<uint4> loc(P, make_uint4(0, 0, 0, 0));
+    std::vector<uint4> wins;
+    unsigned long long rb = 0;
+    for (uint32_t a = 0; a < P; ++a) {
+        const uint32_t size = pop_off[a + 1] - pop_off[a];
+        if (size == 0) continue;
+        uint64_t total = 0;
+        uint32_t deg = 0;
+        for (uint32_t i = pop_off[a]; i < pop_off[a + 1]; ++i) {
+            total += cnt[i];
+            deg = std::max(deg, cnt[i]);
+        }
+        const uint32_t k = (size + kLocalWin - 1) / kLocalWin;
+        if (static_cast<double>(total) / size / k < kLocalMinSpan) continue;
+        // largest s with max|w| * deg * 2^s + deg < 2^31 (each rounded weight adds at most 1/2)
+        float mw;
+        std::memcpy(&mw, &maxw[a], sizeof(float));
+        const double room = 2147483647.0 - deg;
+        int sh = kLocalMaxShift;
+        if (mw > 0.f) sh = std::min(kLocalMaxShift, static_cast<int>(std::floor(std::log2(room / (static_cast<double>(mw) * deg)))));
+        while (sh >= kLocalMinShift && static_cast<double>(mw) * deg * std::ldexp(1.0, sh) >= room) --sh;
+        if (sh < kLocalMinShift) continue;
+        const uint32_t width = (size + k - 1) / k;
+        loc[a] = make_uint4(k, width, static_cast<uint32_t>(rb), static_cast<uint32_t>(rb >> 32));
+        for (uint32_t w = 0; w < k; ++w) {
+            const uint32_t lo = std::min<uint64_t>(pop_off[a] + static_cast<uint64_t>(w) * width, pop_off[a + 1]);
+            const uint32_t hi = w + 1 == k ? pop_off[a + 1] : std::min<uint64_t>(lo + static_cast<uint64_t>(width), pop_off[a + 1]);
+            wins.push_back(make_uint4(a, lo, hi, w | (static_cast<uint32_t>(sh) << 16)));
+        }
+        rb += static_cast<unsigned long long>(size) * (k + 1);
+    }
+    if (wins.empty()) return DTB_OK;
+    DTB_TRY(dalloc(own_seg, n, false));
+    DTB_TRY(dalloc(woff, rb, false));
+    DTB_TRY(dalloc(pop_loc, P, false));
+    DTB_TRY(dalloc(win_tab, wins.size(), false));
+    DTB_CU(cudaMemcpyAsync(pop_loc, loc.data(), sizeof(uint4) * P, cudaMemcpyHostToDevice, stream));
+    DTB_CU(cudaMemcpyAsync(win_tab, wins.data(), sizeof(uint4) * wins.size(), cudaMemcpyHostToDevice, stream));
+    DTB_CU(build_local_offsets(out_ptr, out_col, out_w, static_cast<int>(wtype), pop_off_dev, P, n, pop_loc, nullptr,
+                               nullptr, own_seg, woff, nullptr, stream));
+    n_windows = static_cast<uint32_t>(wins.size());
+    const uint32_t wp[2] = {0u, n_windows};
+    DTB_CU(cudaMemcpyAsync(prefix_dev + 6, wp, sizeof(wp), cudaMemcpyHostToDevice, stream));
+    DTB_CU(cudaStreamSynchronize(stream));
+    return DTB_OK;
 }
 
 // Allocations every network needs, independent of its connectivity.
@@ -241,7 +339,7 @@ static int alloc_core(Engine& e) {
     DTB_TRY(e.dalloc(e.events, 1));
     DTB_TRY(e.dalloc(e.ticket, 1));
     DTB_TRY(e.dalloc(e.view_dev, 1));
-    DTB_TRY(e.dalloc(e.prefix_dev, 6));
+    DTB_TRY(e.dalloc(e.prefix_dev, 8));
     DTB_TRY(e.dalloc(e.list, e.n_pad, false));
     DTB_TRY(e.dalloc(e.list_count, 1));
     DTB_TRY(e.dalloc(e.list_ticket, 1));
@@ -389,6 +487,7 @@ int Engine::create_from_arrays(const dtb_network_arrays& a, const dtb_options& o
                             opt.build_push != 0, opt.build_pull != 0));
     DTB_TRY(upload_params());
     DTB_TRY(init_state());
+    DTB_TRY(build_local_tables());
     return refresh_view();
 }
 
@@ -463,6 +562,7 @@ int Engine::create_structured(const dtb_structured_spec& s, const dtb_options& o
     dev_bytes -= sizeof(uint32_t) * P + sizeof(unsigned long long) * P * P;
     DTB_TRY(upload_params());
     DTB_TRY(init_state());
+    DTB_TRY(build_local_tables());
     return refresh_view();
 }
 
@@ -701,6 +801,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
                         if (!push_tuned[0]) tune_at += 50;   // still quiet: retry later in this run
                     }
                     DTB_TRY(timed_launch(1, [&] { return launch_push(b, 0, static_cast<int>(wtype), push_cfg, push_ctas, stream); }));
+                    launches += push_extra_launches(b, 0, push_cfg);
                     break;
                 case DTB_SYN_PUSH_EXACT:
                     DTB_TRY(timed_launch(0, [&] { return launch_lif(b, first ? J_ASIS : J_FOLD, kflags, pm, stream); }));
@@ -793,6 +894,7 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
         LaunchBatch tb = b;
         tb.nets = tview;
         for (const PushCfg& c : kPushCands) {
+            if (c.kind == PUSH_LOCAL && (exact || b.windows_total == 0)) continue;
             uint32_t ctas = 0;
             DTB_CU(push_prepare(exact, wtype, c, sm_count, &ctas));
             float ms_min = 1e30f;
@@ -862,6 +964,7 @@ int Engine::info(dtb_engine_info& inf) const {
     inf.push_kind = static_cast<uint32_t>(push_cfg.kind);
     inf.push_param = static_cast<uint32_t>(push_cfg.lpr != 32 ? 1000 + push_cfg.lpr : push_cfg.param);
     inf.push_tuned_ms = tuned_ms;
+    inf.local_windows = n_windows;
     return DTB_OK;
 }
 
@@ -1284,15 +1387,8 @@ int32_t dtb_set_push_variant(void* engine, int32_t kind, int32_t param) {
         e->push_tuned[0] = e->push_tuned[1] = false;
         return DTB_OK;
     }
-    dtb::PushCfg cfg{kind, param, 32};
-    if (kind == dtb::PUSH_REG && param >= 1000) {   // 1000 + lanes per row: sub-warp rows
-        cfg.param = 8;
-        cfg.lpr = param - 1000;
-    }
-    bool ok = false;
-    for (const dtb::PushCfg& c : dtb::kPushCands)
-        ok = ok || (c.kind == cfg.kind && c.param == cfg.param && c.lpr == cfg.lpr);
-    if (!ok) return dtb::fail(DTB_INVALID_PARAMETER, "unknown push variant");
+    dtb::PushCfg cfg;
+    if (!dtb::push_cfg_from_abi(kind, param, cfg)) return dtb::fail(DTB_INVALID_PARAMETER, "unknown push variant");
     e->push_cfg = cfg;
     e->autotune = false;
     return DTB_OK;

@@ -28,6 +28,7 @@ struct TuneResult {
     float best_ms = 0.0f;
     std::vector<TuneEntry> report;
 };
+bool push_cfg_from_abi(int kind, int param, PushCfg& cfg);
 __global__ void set_u64_kernel(unsigned long long* p, unsigned long long v);
 __global__ void set_u32_kernel(uint32_t* p, uint32_t v);
 int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int exact, int wtype, int sm_count,
@@ -132,12 +133,19 @@ public:
     float* inj_z = nullptr;
     float* inj_u = nullptr;
     NetView* view_dev = nullptr;
-    uint32_t* prefix_dev = nullptr;   // [lif 2][pull 2][vbase 2]
+    uint32_t* prefix_dev = nullptr;   // [lif 2][pull 2][vbase 2][local windows 2]
     uint32_t* list = nullptr;
     uint32_t* list_count = nullptr;
     uint32_t* list_ticket = nullptr;
     uint32_t* tile_pop = nullptr;
     uint32_t lif_ctas_per_sm = 2;
+    // population-local push tables (built when every out-degree row is sorted)
+    uint2* own_seg = nullptr;
+    uint32_t* woff = nullptr;
+    uint4* pop_loc = nullptr;
+    uint4* win_tab = nullptr;
+    uint32_t n_windows = 0;
+    int build_local_tables();
 
     // push kernel variant (autotuned on the first active run)
     PushCfg push_cfg{PUSH_REG, 8, 32};

@@ -420,10 +420,11 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
 // ---------------------------------------------------------------------------
 // Push propagation: one warp per spiking row of the out-degree CSR
 // ---------------------------------------------------------------------------
-template <int ACC, int WT, int kPushUnroll, int LPR>
+template <int ACC, int WT, int kPushUnroll, int LPR, int LOCAL = 0>
 __global__ void __launch_bounds__(kPushThreads)
 push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase, uint32_t n_nets, SpikeList sl) {
-    // LPR lanes per row: 32 (a warp per row) or 16 / 8 (2 / 4 rows per warp, for short rows)
+    // LPR lanes per row: 32 (a warp per row) or 16 / 8 (2 / 4 rows per warp, for short rows).
+    // LOCAL: the own-population span of a row (own_seg) is left to push_local_kernel.
     constexpr uint32_t kGroups = 32 / LPR;
     const uint32_t count = *sl.count;
     const uint32_t lane = (threadIdx.x & 31u) % LPR;
@@ -434,6 +435,7 @@ push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase
     const void* wts = nets[0].out_w;
     float4* J = nets[0].J;
     long long* dJ = nets[0].dJ;
+    const uint2* own = LOCAL ? nets[0].own_seg : nullptr;
     uint32_t vb = 0;
     for (uint32_t r = gw; r < count; r += nw) {
         const uint32_t v = __ldg(sl.list + r);
@@ -445,24 +447,36 @@ push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase
             wts = nets[k].out_w;
             J = nets[k].J;
             dJ = nets[k].dJ;
+            if constexpr (LOCAL) own = nets[k].own_seg;
         }
         const uint32_t j = v - vb;
         const unsigned long long beg = __ldg(ptr + j), end = __ldg(ptr + j + 1);
-        for (unsigned long long e = beg + lane; e < end; e += static_cast<unsigned long long>(LPR) * kPushUnroll) {
+        // virtual positions [0, len): [0, len1) -> beg + x, [len1, len) -> beg2 + (x - len1)
+        unsigned long long len1 = end - beg, beg2 = end;
+        if constexpr (LOCAL) {
+            if (own) {
+                const uint2 o = __ldg(own + j);
+                len1 = o.x;
+                beg2 = beg + o.y;
+            }
+        }
+        const unsigned long long len = len1 + (end - beg2);
+        for (unsigned long long x = lane; x < len; x += static_cast<unsigned long long>(LPR) * kPushUnroll) {
             uint32_t c[kPushUnroll];
             float2 w[kPushUnroll];
 #pragma unroll
             for (int q = 0; q < kPushUnroll; ++q) {
-                const unsigned long long idx = e + static_cast<unsigned long long>(LPR) * q;
-                if (idx < end) {
+                const unsigned long long xq = x + static_cast<unsigned long long>(LPR) * q;
+                if (xq < len) {
+                    const unsigned long long idx = LOCAL ? (xq < len1 ? beg + xq : beg2 + (xq - len1)) : beg + xq;
                     c[q] = __ldcs(col + idx);
                     w[q] = load_weight<WT>(wts, idx);
                 }
             }
 #pragma unroll
             for (int q = 0; q < kPushUnroll; ++q) {
-                const unsigned long long idx = e + static_cast<unsigned long long>(LPR) * q;
-                if (idx < end) {
+                const unsigned long long xq = x + static_cast<unsigned long long>(LPR) * q;
+                if (xq < len) {
                     const uint32_t target = c[q] & kIndexMask;
                     const uint32_t kind = c[q] >> 31;
                     if constexpr (ACC == 0) {
@@ -483,6 +497,188 @@ push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase
             *sl.count = 0u;
             *sl.ticket = 0u;
             __threadfence();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Population-local push, phase B: one CTA per window of a population.  The CTA
+// zeroes four accumulator planes (AMPA, NMDA, GABAa, GABAb) for the neurons of
+// its window in shared memory, finds its population's spiking rows in the
+// propagated bitmap, adds each row's synapses into the window (the span between
+// two woff boundaries: contiguous, because rows are sorted by postsynaptic
+// neuron), and adds the window to J with coalesced 128-bit read-modify-writes.
+// Windows are disjoint and phase A (the cross-population spans) has finished, so
+// the write-back needs no atomics.
+//
+// The window sums are 32-bit fixed point: w is rounded to a multiple of 2^-s and
+// added with red.shared.add.u32 (native, fire-and-forget; a shared-memory float
+// atomic is a compare-and-swap loop whose latency stalls the warp).  s is chosen
+// per population when the tables are built so that max|w| x (largest own-
+// population in-degree) x 2^s + in-degree < 2^31: no sum can overflow, whatever
+// spikes.  The regional network gets s = 21 (resolution 4.8e-7, below the
+// rounding of float atomics onto J of order 10).
+// ---------------------------------------------------------------------------
+constexpr int kLocalThreads = 1024;
+constexpr int kLocalUnroll = 8;
+
+__device__ __forceinline__ void red_add_shared_u32(const void* p, uint32_t v) {
+    asm volatile("red.shared.add.u32 [%0], %1;" :: "r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))), "r"(v) : "memory");
+}
+
+constexpr size_t kLocalSmem = 4ull * kLocalWin * sizeof(int);
+
+template <int WT>
+__global__ void __launch_bounds__(kLocalThreads, 1)
+push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ win_prefix, uint32_t n_nets) {
+    // plane c of kLocalWin 32-bit sums: random targets spread over all 32 banks
+    extern __shared__ int acc[];
+    const uint32_t gwin = blockIdx.x;
+    const uint32_t net = n_nets > 1 ? find_net(win_prefix, n_nets, gwin) : 0u;
+    const NetView& nv = nets[net];
+    const uint4 wt = nv.win_tab[gwin - __ldg(win_prefix + net)];
+    const uint32_t a = wt.x, lo = wt.y, hi = wt.z, k = wt.w & 0xFFFFu;
+    const int sh = static_cast<int>(wt.w >> 16);                  // fixed-point exponent s, 16..60
+    const float scale = __int_as_float((127 + sh) << 23);         // 2^s
+    const float unscale = __int_as_float((127 - sh) << 23);       // 2^-s
+    const uint32_t width = hi - lo;
+    for (uint32_t i = threadIdx.x; i < 4 * kLocalWin; i += kLocalThreads) acc[i] = 0;
+    const uint4 pl = nv.pop_loc[a];
+    const uint32_t ka = pl.x;
+    const unsigned long long rb = static_cast<unsigned long long>(pl.z) | (static_cast<unsigned long long>(pl.w) << 32);
+    const uint32_t p_lo = __ldg(nv.pop_off + a), p_hi = __ldg(nv.pop_off + a + 1);
+    const uint32_t* bits = (nv.clock->n & 1ull) ? nv.bits1 : nv.bits0;
+    const unsigned long long* ptr = nv.out_ptr;
+    const uint32_t* col = nv.out_col;
+    const void* wts = nv.out_w;
+    const uint32_t* woff = nv.woff;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    constexpr uint32_t kWarps = kLocalThreads / 32;
+    const uint32_t w_lo = p_lo >> 5, w_hi = (p_hi + 31) >> 5;
+    __syncthreads();
+    // lane l of warp w reads word base + l * kWarps + w: every warp gets words
+    // spread over the whole population, so small populations still use all warps
+    for (uint32_t base = w_lo; base < w_hi; base += 32 * kWarps) {
+        const uint32_t wi = base + lane * kWarps + warp;
+        uint32_t m = 0;
+        if (wi < w_hi) {
+            m = bits[wi];
+            const uint32_t b0 = wi << 5;
+            if (b0 < p_lo) m &= ~0u << (p_lo - b0);
+            if (p_hi - b0 < 32u) m &= (1u << (p_hi - b0)) - 1u;
+        }
+        while (__any_sync(0xffffffffu, m != 0u)) {
+            // every lane with spikes left takes one row: its metadata loads overlap
+            uint32_t s0 = 0, s1 = 0;
+            unsigned long long rbeg = 0;
+            if (m) {
+                const uint32_t j = (wi << 5) + static_cast<uint32_t>(__ffs(m) - 1);
+                m &= m - 1u;
+                rbeg = __ldg(ptr + j);
+                const uint32_t* wo = woff + rb + static_cast<unsigned long long>(j - p_lo) * (ka + 1u) + k;
+                s0 = __ldg(wo);
+                s1 = __ldg(wo + 1);
+            }
+            uint32_t rows = __ballot_sync(0xffffffffu, s1 > s0);
+            while (rows) {
+                const int src = __ffs(rows) - 1;
+                rows &= rows - 1u;
+                const unsigned long long rbase = __shfl_sync(0xffffffffu, rbeg, src);
+                const unsigned long long e1 = rbase + __shfl_sync(0xffffffffu, s1, src);
+                for (unsigned long long e = rbase + __shfl_sync(0xffffffffu, s0, src) + lane; e < e1;
+                     e += 32ull * kLocalUnroll) {
+                    uint32_t c[kLocalUnroll];
+                    float2 w[kLocalUnroll];
+#pragma unroll
+                    for (int q = 0; q < kLocalUnroll; ++q) {
+                        const unsigned long long idx = e + 32ull * q;
+                        if (idx < e1) {
+                            c[q] = __ldcs(col + idx);
+                            w[q] = load_weight<WT>(wts, idx);
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < kLocalUnroll; ++q) {
+                        if (e + 32ull * q < e1) {
+                            const int* d = acc + (c[q] >> 31) * (2u * kLocalWin) + ((c[q] & kIndexMask) - lo);
+                            red_add_shared_u32(d, static_cast<uint32_t>(__float2int_rn(__fmul_rn(w[q].x, scale))));
+                            red_add_shared_u32(d + kLocalWin, static_cast<uint32_t>(__float2int_rn(__fmul_rn(w[q].y, scale))));
+                        }
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    float4* J = nv.J + lo;
+    for (uint32_t i = threadIdx.x; i < width; i += kLocalThreads) {
+        const int4 v = make_int4(acc[i], acc[kLocalWin + i], acc[2 * kLocalWin + i], acc[3 * kLocalWin + i]);
+        if (v.x | v.y | v.z | v.w) {
+            float4 x = J[i];
+            x.x = __fadd_rn(x.x, __fmul_rn(__int2float_rn(v.x), unscale));
+            x.y = __fadd_rn(x.y, __fmul_rn(__int2float_rn(v.y), unscale));
+            x.z = __fadd_rn(x.z, __fmul_rn(__int2float_rn(v.z), unscale));
+            x.w = __fadd_rn(x.w, __fmul_rn(__int2float_rn(v.w), unscale));
+            J[i] = x;
+        }
+    }
+}
+
+__device__ inline uint32_t row_lower_bound(const uint32_t* __restrict__ col, unsigned long long beg,
+                                           unsigned long long end, uint32_t target) {
+    unsigned long long lo = beg, hi = end;
+    while (lo < hi) {
+        const unsigned long long mid = (lo + hi) >> 1;
+        if ((__ldg(col + mid) & kIndexMask) < target) lo = mid + 1; else hi = mid;
+    }
+    return static_cast<uint32_t>(lo - beg);
+}
+
+// One warp per row.  Pass 1 (woff == nullptr): sortedness of every row, and per
+// own-population synapse its target's count (own_cnt) and its population's
+// largest |w| (maxw_bits, float bits of a non-negative value: ordered as
+// integers).  Pass 2: own_seg and the window boundaries of every row whose
+// population has local windows.
+template <int WT>
+__global__ void local_offsets_kernel(const unsigned long long* __restrict__ out_ptr, const uint32_t* __restrict__ col,
+                                     const void* __restrict__ wts, const uint32_t* __restrict__ pop_off, uint32_t n_pops,
+                                     uint32_t n, const uint4* __restrict__ pop_loc, uint32_t* own_cnt, uint32_t* maxw_bits,
+                                     uint2* own_seg, uint32_t* woff, uint32_t* unsorted) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < n; j += nw) {
+        const uint32_t a = find_pop(pop_off, n_pops, j);
+        const unsigned long long beg = out_ptr[j], end = out_ptr[j + 1];
+        const uint32_t p_lo = __ldg(pop_off + a), p_hi = __ldg(pop_off + a + 1);
+        if (woff == nullptr) {
+            bool bad = false;
+            for (unsigned long long e = beg + lane; e + 1 < end; e += 32)
+                bad |= (__ldg(col + e) & kIndexMask) > (__ldg(col + e + 1) & kIndexMask);
+            if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(unsorted, 1u);
+            const uint32_t s = row_lower_bound(col, beg, end, p_lo), t = row_lower_bound(col, beg, end, p_hi);
+            float mx = 0.f;
+            for (unsigned long long e = beg + s + lane; e < beg + t; e += 32) {
+                atomicAdd(own_cnt + (__ldg(col + e) & kIndexMask), 1u);
+                const float2 w = load_weight<WT>(wts, e);
+                mx = fmaxf(mx, fmaxf(fabsf(w.x), fabsf(w.y)));
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            if (lane == 0 && mx > 0.f) atomicMax(maxw_bits + a, __float_as_uint(mx));
+        } else {
+            const uint4 pl = pop_loc[a];
+            if (pl.x == 0) {
+                if (lane == 0) own_seg[j] = make_uint2(0u, 0u);
+                continue;
+            }
+            const unsigned long long rb = static_cast<unsigned long long>(pl.z) | (static_cast<unsigned long long>(pl.w) << 32);
+            uint32_t* wo = woff + rb + static_cast<unsigned long long>(j - p_lo) * (pl.x + 1u);
+            for (uint32_t k = lane; k <= pl.x; k += 32) {
+                const uint32_t bnd = k == pl.x ? p_hi : static_cast<uint32_t>(min(static_cast<unsigned long long>(p_lo) + static_cast<unsigned long long>(k) * pl.y,
+                                                                                   static_cast<unsigned long long>(p_hi)));
+                wo[k] = row_lower_bound(col, beg, end, bnd);
+            }
+            if (lane == 0) own_seg[j] = make_uint2(row_lower_bound(col, beg, end, p_lo), row_lower_bound(col, beg, end, p_hi));
         }
     }
 }
@@ -899,7 +1095,15 @@ cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop
 
 template <int ACC, int WT>
 static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint32_t ctas, cudaStream_t s) {
-    if (cfg.kind == PUSH_REG) {
+    if (cfg.kind == PUSH_LOCAL && ACC == 0) {
+        const dim3 grid(ctas), block(kPushThreads);
+        if (cfg.lpr == 16)
+            push_kernel<ACC, WT, 8, 16, 1><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes);
+        else
+            push_kernel<ACC, WT, 8, 32, 1><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes);
+        if (b.windows_total)
+            push_local_kernel<WT><<<b.windows_total, kLocalThreads, kLocalSmem, s>>>(b.nets, b.win_prefix, b.n_nets);
+    } else if (cfg.kind == PUSH_REG || cfg.kind == PUSH_LOCAL) {
         const dim3 grid(ctas), block(kPushThreads);
         if (cfg.lpr == 16) {
             push_kernel<ACC, WT, 8, 16><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes);
@@ -929,7 +1133,13 @@ template <int ACC, int WT>
 static cudaError_t push_prepare_wt(const PushCfg& cfg, int sm_count, uint32_t* ctas) {
     int per_sm = 0;
     cudaError_t e = cudaSuccess;
-    if (cfg.kind == PUSH_REG) {
+    if (cfg.kind == PUSH_LOCAL && ACC == 0) {
+        e = cudaFuncSetAttribute(push_local_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kLocalSmem));
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.lpr == 16 ? push_kernel<ACC, WT, 8, 16, 1> : push_kernel<ACC, WT, 8, 32, 1>,
+                                                              kPushThreads, 0);
+    } else if (cfg.kind == PUSH_REG || cfg.kind == PUSH_LOCAL) {
         if (cfg.lpr == 16) {
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, push_kernel<ACC, WT, 8, 16>, kPushThreads, 0);
         } else if (cfg.lpr == 8) {
@@ -969,7 +1179,8 @@ static cudaError_t push_launch_acc(const LaunchBatch& b, int wt, const PushCfg& 
 
 const PushCfg kPushCands[kPushCandidates] = {{PUSH_REG, 4, 32}, {PUSH_REG, 8, 32}, {PUSH_REG, 16, 32},
                                              {PUSH_REG, 8, 16}, {PUSH_REG, 8, 8},
-                                             {PUSH_TMA, 256, 32}, {PUSH_TMA, 512, 32}};
+                                             {PUSH_TMA, 256, 32}, {PUSH_TMA, 512, 32},
+                                             {PUSH_LOCAL, 8, 32}, {PUSH_LOCAL, 8, 16}};
 
 cudaError_t push_prepare(int exact, int wt, const PushCfg& cfg, int sm_count, uint32_t* ctas) {
     if (exact) {
@@ -990,6 +1201,21 @@ cudaError_t push_prepare(int exact, int wt, const PushCfg& cfg, int sm_count, ui
 
 cudaError_t launch_push(const LaunchBatch& b, int exact, int wt, const PushCfg& cfg, uint32_t ctas, cudaStream_t s) {
     return exact ? push_launch_acc<1>(b, wt, cfg, ctas, s) : push_launch_acc<0>(b, wt, cfg, ctas, s);
+}
+
+cudaError_t build_local_offsets(const unsigned long long* out_ptr, const uint32_t* out_col, const void* out_w, int wt,
+                                const uint32_t* pop_off, uint32_t n_pops, uint32_t n, const uint4* pop_loc,
+                                uint32_t* own_cnt, uint32_t* maxw_bits, uint2* own_seg, uint32_t* woff,
+                                uint32_t* unsorted, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const uint32_t blocks = std::min<uint32_t>((n + 7) / 8, 148u * 64u);
+    switch (wt) {
+        case W_F32: local_offsets_kernel<W_F32><<<blocks, 256, 0, s>>>(out_ptr, out_col, out_w, pop_off, n_pops, n, pop_loc, own_cnt, maxw_bits, own_seg, woff, unsorted); break;
+        case W_BF16: local_offsets_kernel<W_BF16><<<blocks, 256, 0, s>>>(out_ptr, out_col, out_w, pop_off, n_pops, n, pop_loc, own_cnt, maxw_bits, own_seg, woff, unsorted); break;
+        case W_F16: local_offsets_kernel<W_F16><<<blocks, 256, 0, s>>>(out_ptr, out_col, out_w, pop_off, n_pops, n, pop_loc, own_cnt, maxw_bits, own_seg, woff, unsorted); break;
+        default: local_offsets_kernel<W_U8><<<blocks, 256, 0, s>>>(out_ptr, out_col, out_w, pop_off, n_pops, n, pop_loc, own_cnt, maxw_bits, own_seg, woff, unsorted); break;
+    }
+    return cudaGetLastError();
 }
 
 template <int G>

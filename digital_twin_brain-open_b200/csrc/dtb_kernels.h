@@ -19,29 +19,46 @@ struct LaunchBatch {
     uint32_t pull_tiles_total;
     uint32_t push_ctas;
     uint32_t lif_ctas;            // persistent grid of the LIF kernel
+    const uint32_t* win_prefix;   // device [n_nets + 1] cumulative local-push windows
+    uint32_t windows_total;
     SpikeList spikes;
 };
 
 cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop_mode, cudaStream_t s);
 // Push kernel variants chosen by the autotuner.
-enum PushKind : int { PUSH_REG = 0, PUSH_TMA = 1 };
+enum PushKind : int { PUSH_REG = 0, PUSH_TMA = 1, PUSH_LOCAL = 2 };
 struct PushCfg {
     int kind;    // PUSH_REG: register-staged loads, param = synapses in flight per lane (4, 8, 16)
                  // PUSH_TMA: bulk-copy staged rows, param = synapses per stage (256, 512)
+                 // PUSH_LOCAL: own-population synapses summed per window in shared memory,
+                 //   the rest register-staged (param = synapses in flight per lane, 8)
     int param;
     int lpr = 32;  // PUSH_REG: lanes per row (32, 16, 8; sub-warp rows use 8 in flight per lane)
 };
 
 // Every variant the autotuner times.
-constexpr int kPushCandidates = 7;
+constexpr int kPushCandidates = 9;
 extern const PushCfg kPushCands[kPushCandidates];
 // Sets kernel attributes and returns the persistent grid (max resident CTAs).
 cudaError_t push_prepare(int exact, int weight_type, const PushCfg& cfg, int sm_count, uint32_t* ctas);
 cudaError_t launch_push(const LaunchBatch& b, int exact, int weight_type, const PushCfg& cfg, uint32_t ctas,
                         cudaStream_t s);
+// Kernels launch_push issues beyond the first (the local variant's window pass).
+inline uint32_t push_extra_launches(const LaunchBatch& b, int exact, const PushCfg& cfg) {
+    return (cfg.kind == PUSH_LOCAL && !exact && b.windows_total) ? 1u : 0u;
+}
 cudaError_t launch_pull(const LaunchBatch& b, int gather, int weight_type, uint32_t flags, int prop_mode, cudaStream_t s);
 cudaError_t launch_fold_finish(const LaunchBatch& b, cudaStream_t s);
 cudaError_t launch_gather_finish(const LaunchBatch& b, int weight_type, cudaStream_t s);
+
+// Population-local push tables (rows must be sorted by postsynaptic neuron;
+// *unsorted is set otherwise).  Pass 1 (woff == nullptr): per-neuron own-
+// population in-degree into own_cnt, per-population max |w| (float bits) into
+// maxw_bits; pass 2: own_seg and woff from pop_loc.
+cudaError_t build_local_offsets(const unsigned long long* out_ptr, const uint32_t* out_col, const void* out_w, int wt,
+                                const uint32_t* pop_off, uint32_t n_pops, uint32_t n, const uint4* pop_loc,
+                                uint32_t* own_cnt, uint32_t* maxw_bits, uint2* own_seg, uint32_t* woff,
+                                uint32_t* unsorted, cudaStream_t s);
 
 // ---- device network generator (dtb_generate.cu)
 struct GenSpec {

@@ -23,6 +23,7 @@ OUT_OF_MEMORY, CUDA_ERROR, DEVICE_FAULT, IO_ERROR, NO_DEVICE = 16, 17, 18, 19, 2
 W_F32, W_BF16, W_F16, W_U8, W_F64 = 0, 1, 2, 3, 4
 PROP_THRESHOLD, PROP_NOISE, PROP_OR = 0, 1, 2
 SYN_PUSH, SYN_PUSH_EXACT, SYN_PULL = 0, 1, 2
+PUSH_REG, PUSH_TMA, PUSH_LOCAL = 0, 1, 2
 NOISE_PHILOX, NOISE_INJECTED = 0, 1
 RUN_USE_OU, RUN_FREQ, RUN_VMEAN, RUN_RECORD_SPIKES, RUN_TIME_KERNELS = 1, 2, 4, 8, 16
 RUN_SAMPLE_SPIKE, RUN_SAMPLE_V, RUN_SAMPLE_IOU = 32, 64, 128
@@ -66,7 +67,7 @@ class EngineInfo(C.Structure):
                 ("device_bytes", C.c_uint64), ("step", C.c_uint64), ("t", C.c_float),
                 ("weight_type", C.c_uint32), ("has_push", C.c_uint32), ("has_pull", C.c_uint32),
                 ("per_neuron_params", C.c_uint32), ("push_kind", C.c_uint32), ("push_param", C.c_uint32),
-                ("push_tuned_ms", C.c_float)]
+                ("push_tuned_ms", C.c_float), ("local_windows", C.c_uint32)]
 
 
 class RunRequest(C.Structure):
@@ -118,6 +119,7 @@ SIGNATURES = {
     "dtb_batch_destroy": (_I32, [_P]),
     "dtb_batch_run": (_I32, [_P, _P, _P]),
     "dtb_batch_set_graph": (_I32, [_P, _I32]),
+    "dtb_batch_set_push_variant": (_I32, [_P, _I32, _I32]),
     "dtb_batch_info": (_I32, [_P, _P, _P, _P, _P]),
     "dtb_compact_spikes_noalloc": (_I32, [_P, _U32, _P, _P, _P]),
 }
@@ -281,7 +283,8 @@ class Engine:
         return inf
 
     def set_push_variant(self, kind, param=0):
-        """kind 0: register-staged (param 4/8/16), 1: TMA-staged (param 256/512), -1: autotune."""
+        """kind 0: register-staged (param 4/8/16, 1016/1008 sub-warp rows), 1: TMA-staged
+        (param 256/512), 2: population-local windows (param 8/1016), -1: autotune."""
         _check(LIB.dtb_set_push_variant(self._h, kind, param))
 
     def tuning_report(self):
@@ -421,6 +424,10 @@ class Batch:
 
     def set_graph(self, enable):
         _check(LIB.dtb_batch_set_graph(self._h, int(enable)))
+
+    def set_push_variant(self, kind, param=0):
+        """As Engine.set_push_variant, for the batch's shared push launch."""
+        _check(LIB.dtb_batch_set_push_variant(self._h, kind, param))
 
     def info(self):
         n, g, k, p = C.c_uint32(), C.c_uint32(), C.c_int32(), C.c_int32()

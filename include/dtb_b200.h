@@ -138,9 +138,11 @@ typedef struct dtb_engine_info {
     uint32_t weight_type;
     uint32_t has_push, has_pull;
     uint32_t per_neuron_params;  /* 1 once any parameter differs within a population        */
-    uint32_t push_kind;          /* push kernel in use: 0 register-staged, 1 TMA-staged rows   */
-    uint32_t push_param;         /* synapses in flight per lane (0) or per stage (1)          */
+    uint32_t push_kind;          /* push kernel in use: 0 register-staged, 1 TMA-staged rows,  */
+                                 /* 2 population-local windows + register-staged remainder     */
+    uint32_t push_param;         /* synapses in flight per lane (0, 2) or per stage (1)       */
     float push_tuned_ms;         /* push time of the chosen variant when it was tuned, ms     */
+    uint32_t local_windows;      /* population-local push windows (0: variant 2 = variant 0)  */
 } dtb_engine_info;
 
 /* RunRequest (snn.proto:63-77) flags. */
@@ -198,7 +200,11 @@ int32_t dtb_create_from_npz(const char* path, const dtb_options* opt, void** eng
 int32_t dtb_destroy(void* engine);
 int32_t dtb_info(void* engine, dtb_engine_info* info);
 /* Push kernel variant: kind 0 (register-staged, param 4/8/16 synapses in flight
- * per lane) or 1 (TMA bulk-copy staged rows, param 256/512 synapses per stage);
+ * per lane, or 1000 + lanes per row 16/8 for sub-warp rows), 1 (TMA bulk-copy
+ * staged rows, param 256/512 synapses per stage) or 2 (population-local: each
+ * row's own-population synapses are summed per window of its population in
+ * shared memory, the rest as kind 0; param 8 or 1016; float push mode only,
+ * the exact mode runs kind 0 instead);
  * kind < 0 re-enables the autotuner, which times every variant on a live spike
  * list of the first active run and keeps the fastest. */
 int32_t dtb_set_push_variant(void* engine, int32_t kind, int32_t param);
@@ -261,6 +267,8 @@ int32_t dtb_batch_destroy(void* batch);
 int32_t dtb_batch_run(void* batch, const dtb_run_request* req, dtb_run_output* outs);
 /* enable != 0: capture float-push windows into a CUDA graph (default). */
 int32_t dtb_batch_set_graph(void* batch, int32_t enable);
+/* The batch's push variant, as dtb_set_push_variant (kind < 0: autotune). */
+int32_t dtb_batch_set_push_variant(void* batch, int32_t kind, int32_t param);
 int32_t dtb_batch_info(void* batch, uint32_t* n_members, uint32_t* graph_launches, int32_t* push_kind,
                        int32_t* push_param);
 

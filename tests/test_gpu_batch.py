@@ -70,6 +70,33 @@ def test_batch_graph_window_and_solo_interleave(gpu):
         e.close()
 
 
+@pytest.mark.parametrize("graph", [False, True])
+def test_batch_local_push_step(gpu, graph):
+    """Batched population-local push: from saved mid-run member states, one float
+    step gives every member the exact push's spikes and V, and J within float rounding."""
+    specs = _members()
+    engines = [E.Engine.structured(s, seed=i) for i, s in enumerate(specs)]
+    assert all(e.info().local_windows > 0 for e in engines)
+    with E.Batch(engines, graph=graph) as b:
+        b.run(500, syn_mode=E.SYN_PUSH_EXACT)
+        blobs = [e.save_state() for e in engines]
+        ref = b.run(1, record_spikes=True, syn_mode=E.SYN_PUSH_EXACT)
+        v_ref = [e.read_state(E.STATE_V) for e in engines]
+        j_ref = [e.read_state(E.STATE_J) for e in engines]
+        for e, blob in zip(engines, blobs):
+            e.load_state(blob)
+        b.set_push_variant(E.PUSH_LOCAL, 8)
+        got = b.run(1, record_spikes=True, syn_mode=E.SYN_PUSH)
+        assert b.info()["push_kind"] == E.PUSH_LOCAL
+    for i, e in enumerate(engines):
+        assert np.array_equal(got[i].spikes, ref[i].spikes)
+        assert np.array_equal(e.read_state(E.STATE_V), v_ref[i])
+        assert np.allclose(e.read_state(E.STATE_J), j_ref[i], rtol=1e-5, atol=1e-5)
+    assert sum(int(r.spikes.sum()) for r in ref) > 0
+    for e in engines:
+        e.close()
+
+
 def test_batch_rejects_mixed_weight_types(gpu):
     a = E.Engine.structured(nw.structured_spec(3000, 3, 50, 1))
     b = E.Engine.structured(nw.structured_spec(3000, 3, 50, 2), weight_type=E.W_BF16)

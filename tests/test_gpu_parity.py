@@ -68,11 +68,13 @@ def test_deterministic_modes_bit_exact(gpu, syn, dyadic):
         assert r.events == expected_events
 
 
-def test_float_push_within_tolerance(gpu, block10k):
+@pytest.mark.parametrize("variant", [(E.PUSH_REG, 8), (E.PUSH_LOCAL, 8)])
+def test_float_push_within_tolerance(gpu, block10k, variant):
     steps = 400
     z, _ = lo.torch_noise_stream(0, 10_000, steps, False)
     o = lo.LifOracle(block10k)
     with E.Engine.from_arrays(block10k) as eng:
+        eng.set_push_variant(*variant)
         eng.set_noise_injected(z)
         div = None
         for s in range(steps):
@@ -355,7 +357,8 @@ def test_autotuner_picks_a_variant(gpu):
         r = eng.run(1000)
         assert r.freqs[-200:].sum() > 0.005 * 200 * spec.n
         rep = eng.tuning_report()
-        assert len(rep) == 7 and all(ms > 0 for _, _, ms in rep)
+        assert eng.info().local_windows > 0
+        assert len(rep) == 9 and all(ms > 0 for _, _, ms in rep)
         inf = eng.info()
         assert min(ms for _, _, ms in rep) == pytest.approx(inf.push_tuned_ms)
 
@@ -410,3 +413,63 @@ def test_samples_follow_oracle(gpu, block10k):
     assert np.array_equal(si, np.array(ios))
     assert np.array_equal(ss.astype(bool), np.array(sps))
     assert ss.sum() > 0
+
+
+# ---- population-local push -------------------------------------------------------
+LOCAL_WIN = 13312   # neurons per window (kLocalWin)
+
+
+def _local_spec():
+    """Three populations of 20k-35k neurons: two or three windows each."""
+    return nw.structured_spec(80_000, 3, 400, seed=21)
+
+
+def test_local_push_windows(gpu, block10k):
+    spec = _local_spec()
+    with E.Engine.structured(spec) as eng:
+        assert eng.info().local_windows == sum(-(-int(s) // LOCAL_WIN) for s in spec.pop_sizes)
+    with E.Engine.from_arrays(block10k) as eng:     # post-major input: rows sorted, one window
+        assert eng.info().local_windows == 1
+    perm = np.random.default_rng(0).permutation(block10k["input_neuron_idx"].shape[0])
+    shuffled = {k: (v[perm] if k != "property" else v) for k, v in block10k.items()}
+    with E.Engine.from_arrays(shuffled) as eng:     # rows not sorted by target: no windows
+        assert eng.info().local_windows == 0
+        eng.set_push_variant(E.PUSH_LOCAL, 8)       # runs as the register-staged push
+        assert eng.run(50).freqs.shape == (50, 1)
+
+
+@pytest.mark.parametrize("wt", [E.W_F32, E.W_BF16])
+def test_local_push_step_matches_exact_push(gpu, wt):
+    """One float step of the local push from a saved mid-run state: spikes and V equal
+    the exact push's bit for bit (they precede the push), J within float rounding of
+    the exact fixed-point sum."""
+    spec = _local_spec()
+    with E.Engine.structured(spec, weight_type=wt) as eng:
+        eng.run(600, syn_mode=E.SYN_PUSH_EXACT)
+        blob = eng.save_state()
+        r0 = eng.run(1, record_spikes=True, syn_mode=E.SYN_PUSH_EXACT)
+        v_ref, j_ref = eng.read_state(E.STATE_V), eng.read_state(E.STATE_J)
+        assert r0.spikes.sum() > 0.0005 * spec.n
+        for variant in ((E.PUSH_LOCAL, 8), (E.PUSH_LOCAL, 1016), (E.PUSH_REG, 8)):
+            eng.load_state(blob)
+            eng.set_push_variant(*variant)
+            r = eng.run(1, record_spikes=True, syn_mode=E.SYN_PUSH)
+            assert np.array_equal(r.spikes, r0.spikes), variant
+            assert np.array_equal(eng.read_state(E.STATE_V), v_ref), variant
+            j = eng.read_state(E.STATE_J)
+            assert np.allclose(j, j_ref, rtol=1e-5, atol=1e-5), (variant, np.abs(j - j_ref).max())
+            assert r.events == r0.events
+
+
+def test_local_push_rates_follow_exact_push(gpu):
+    """Over a long run the local float push keeps every population's rate within 3%
+    of the exact push's (float summation order only perturbs threshold crossings)."""
+    spec = _local_spec()
+    rates = {}
+    for syn, variant in ((E.SYN_PUSH_EXACT, (E.PUSH_REG, 8)), (E.SYN_PUSH, (E.PUSH_LOCAL, 8))):
+        with E.Engine.structured(spec) as eng:
+            eng.set_push_variant(*variant)
+            r = eng.run(1500, syn_mode=syn)
+            rates[syn] = r.freqs[500:].sum(0) / (1000 * spec.pop_sizes)
+    assert (rates[E.SYN_PUSH_EXACT] > 0.0005).all()
+    assert np.allclose(rates[E.SYN_PUSH], rates[E.SYN_PUSH_EXACT], rtol=0.03)
