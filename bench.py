@@ -56,9 +56,14 @@ def parse():
     p.add_argument("--pops", type=int, default=N_POPS)
     p.add_argument("--degree", type=int, default=IN_DEGREE)
     p.add_argument("--push", default="auto", help="push kernel: auto (autotuned), reg:4|8|16|1016|1008, tma:256|512, local:8|1016")
-    p.add_argument("--form", default="plain", choices=["plain", "ensemble"],
-                   help="plain: the 5M-neuron network; ensemble: 64 DA members batched (BF16) vs sequential (FP32)")
-    p.add_argument("--members", type=int, default=64)
+    p.add_argument("--form", default="plain", choices=["plain", "ensemble", "serve"],
+                   help="plain: the 5M-neuron network; ensemble: 64 DA members batched (BF16) vs sequential (FP32); "
+                        "serve: Poisson request stream, continuous batching (BF16) vs one at a time (FP32)")
+    p.add_argument("--requests", type=int, default=200, help="requests in the served trace (serve form)")
+    p.add_argument("--rate", type=float, default=40.0, help="request arrival rate, 1/s (serve form)")
+    p.add_argument("--slice", type=int, default=100, help="steps per continuous-batching slice (serve form)")
+    p.add_argument("--hbm-cap-gb", type=float, default=150.0, help="HBM cap of the resident networks (serve form)")
+    p.add_argument("--members", type=int, default=None, help="ensemble members (64) or served networks (128)")
     p.add_argument("--window", type=int, default=800, help="steps per assimilation window (ensemble form)")
     return p.parse_args()
 
@@ -346,7 +351,7 @@ def run_ensemble(args):
     from dtb_b200 import engine as E
     from dtb_b200 import network as nw
 
-    specs = nw.ensemble_specs(n_members=args.members, seed=3)
+    specs = nw.ensemble_specs(n_members=args.members or 64, seed=3)
     windows, W = args.steps, args.window
     rng_hp = np.random.default_rng(11)
     # per-window DA hyper-parameter factors (mul_property_by_subblk of g_AMPA per population)
@@ -445,6 +450,71 @@ def run_ensemble(args):
     }
 
 
+def run_serve(args):
+    """Served form: Poisson request stream over 128 resident networks, continuous batching
+    (BF16) vs the plain single-network path one request at a time (FP32)."""
+    import torch
+    import __graft_entry__
+    __graft_entry__.load_package()
+    from dtb_b200 import engine as E
+    from dtb_b200 import network as nw
+
+    specs = nw.ensemble_specs(n_members=args.members or 128, seed=4)
+    rng = np.random.default_rng(12)
+    t, reqs = 0.0, []
+    for _ in range(args.requests):
+        t += float(rng.exponential(1.0 / args.rate))
+        net = int(rng.integers(len(specs)))
+        P = specs[net].n_pops
+        ou = (rng.uniform(0.55, 0.65, P).astype(np.float32), rng.uniform(0.18, 0.22, P).astype(np.float32),
+              np.full(P, 10.0, np.float32))
+        reqs.append(dict(net=net, iters=args.window, arrival_s=t, ou=ou))
+    warm = [dict(net=i, iters=args.slice, arrival_s=0.0, ou=None) for i in range(len(specs))]
+
+    def serve(wt, policy):
+        t0 = time.perf_counter()
+        srv = E.Server(hbm_cap_bytes=args.hbm_cap_gb * 1e9, slice_steps=args.slice, max_batch=64,
+                       syn_mode=E.SYN_PUSH, autotune=False)
+        for i, sp in enumerate(specs):
+            srv.add_structured(sp, weight_type=wt, seed=200 + i)
+        build_s = time.perf_counter() - t0
+        srv.play(warm, policy)
+        torch.cuda.synchronize()
+        got = srv.play(reqs, policy)
+        info = srv.info()
+        srv.close()
+        lat = np.array([g["latency_s"] for g in got]) * 1e3
+        svc = np.array([g["finish_s"] - g["start_s"] for g in got]) * 1e3
+        span = max(g["finish_s"] for g in got) - reqs[0]["arrival_s"]
+        ev = sum(g["events"] for g in got)
+        rates = np.concatenate([g["freqs"].sum(0) / (args.window * specs[r["net"]].pop_sizes) * 1e4
+                                for g, r in zip(got, reqs)])
+        return {"latency_ms": {"p50": float(np.percentile(lat, 50)), "p90": float(np.percentile(lat, 90)),
+                               "p99": float(np.percentile(lat, 99)), "mean": float(lat.mean()), "max": float(lat.max())},
+                "in_service_ms_mean": float(svc.mean()), "events_per_s": ev / span, "span_s": span,
+                "requests_per_s": len(got) / span, "build_s": build_s,
+                "mean_requests_per_slice": info["batch_members_sum"] / max(1, info["slices"]),
+                "evictions": info["evictions"], "resident_gb": info["resident_bytes"] / 1e9}, rates
+
+    batched, rates_b = serve(E.W_BF16, E.SERVE_BATCHED)
+    plain, rates_s = serve(E.W_F32, E.SERVE_SEQUENTIAL)
+    rel = np.abs(rates_b - rates_s) / np.maximum(rates_s, 1e-9)
+    return {
+        "metric": METRIC, "form": "serve", "value": batched["latency_ms"]["p99"], "unit": "ms p99 request latency",
+        "n_gpus": 1, "steps": args.requests, "warmup": 1, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16-weights/f32-state (batched), f32 (plain)",
+        "data": "synthetic (128 seeded networks of the ensemble distribution generated on the device)",
+        "config": {"workload": f"Poisson arrivals {args.rate}/s, {args.requests} requests of {args.window} steps with "
+                               f"new per-population OU parameters, {len(specs)} resident networks, "
+                               f"HBM cap {args.hbm_cap_gb} GB, slices of {args.slice} steps",
+                   "neurons": int(sum(s.n for s in specs)), "synapses": int(sum(s.n_edges for s in specs))},
+        "batched_bf16": batched, "plain_sequential_f32": plain,
+        "p50_ratio_plain_over_batched": plain["latency_ms"]["p50"] / batched["latency_ms"]["p50"],
+        "p99_ratio_plain_over_batched": plain["latency_ms"]["p99"] / batched["latency_ms"]["p99"],
+        "population_rate_rel_diff_median": float(np.median(rel)),
+    }
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -470,6 +540,8 @@ def main():
         out = run_reference(args)
     elif args.form == "ensemble":
         out = run_ensemble(args)
+    elif args.form == "serve":
+        out = run_serve(args)
     else:
         out = run_ours(args)
     if out is not None:

@@ -15,38 +15,9 @@
 #include <algorithm>
 #include <cstring>
 
-#include "dtb_engine.h"
+#include "dtb_batch.h"
 
 namespace dtb {
-
-class Batch {
-public:
-    ~Batch();
-    int create(Engine* const* engines, uint32_t n);
-    int run(const dtb_run_request& rq, dtb_run_output* outs);
-    int refresh_views();
-
-    std::vector<Engine*> m;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev[2] = {nullptr, nullptr};
-    int sm_count = 148;
-    uint32_t wtype = W_F32;
-    NetView* d_views = nullptr;
-    uint32_t* d_prefix = nullptr;     // [lif n+1][pull n+1][vbase n+1][local windows n+1]
-    uint32_t* list = nullptr;
-    uint32_t* list_count = nullptr;
-    uint32_t* list_ticket = nullptr;
-    LaunchBatch lb{};
-    PushCfg push_cfg{PUSH_REG, 8, 32};
-    uint32_t push_ctas = 0;
-    bool push_tuned[2] = {false, false};
-    bool autotune = true;
-    TuneResult tune;
-    bool use_graph = true;
-    cudaGraphExec_t graph = nullptr;
-    uint64_t graph_key[6] = {0, 0, 0, 0, 0, 0};
-    uint32_t graph_launches = 0;
-};
 
 Batch::~Batch() {
     if (stream) cudaStreamSynchronize(stream);
@@ -60,22 +31,30 @@ Batch::~Batch() {
 }
 
 int Batch::create(Engine* const* engines, uint32_t n) {
-    if (n == 0) return fail(DTB_INVALID_PARAMETER, "empty batch");
-    m.assign(engines, engines + n);
-    for (uint32_t i = 0; i < n; ++i) {
-        if (!m[i]) return fail(DTB_INVALID_PARAMETER, "NULL engine in batch");
-        for (uint32_t j = 0; j < i; ++j)
-            if (m[j] == m[i]) return fail(DTB_INVALID_PARAMETER, "an engine appears twice in the batch");
-        if (m[i]->wtype != m[0]->wtype) return fail(DTB_UNSUPPORTED, "batch members must share the weight type");
-        if (m[i]->device != m[0]->device) return fail(DTB_UNSUPPORTED, "batch members must share the device");
-    }
-    wtype = m[0]->wtype;
-    sm_count = m[0]->sm_count;
     DTB_CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     DTB_CU(cudaEventCreate(&ev0));
     DTB_CU(cudaEventCreate(&ev1));
     DTB_CU(cudaEventCreate(&tev[0]));
     DTB_CU(cudaEventCreate(&tev[1]));
+    return set_members(engines, n);
+}
+
+// (Re)define the members.  Device tables grow when needed and are reused
+// otherwise, so a serving loop can change membership between slices cheaply;
+// a captured graph is dropped because it holds the old tables' sizes.
+int Batch::set_members(Engine* const* engines, uint32_t n) {
+    if (n == 0) return fail(DTB_INVALID_PARAMETER, "empty batch");
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!engines[i]) return fail(DTB_INVALID_PARAMETER, "NULL engine in batch");
+        for (uint32_t j = 0; j < i; ++j)
+            if (engines[j] == engines[i]) return fail(DTB_INVALID_PARAMETER, "an engine appears twice in the batch");
+        if (engines[i]->wtype != engines[0]->wtype) return fail(DTB_UNSUPPORTED, "batch members must share the weight type");
+        if (engines[i]->device != engines[0]->device) return fail(DTB_UNSUPPORTED, "batch members must share the device");
+    }
+    if (!m.empty() && engines[0]->wtype != wtype) push_tuned[0] = push_tuned[1] = false;
+    m.assign(engines, engines + n);
+    wtype = m[0]->wtype;
+    sm_count = m[0]->sm_count;
     std::vector<uint32_t> pre(4 * (n + 1), 0);
     uint64_t total = 0;
     for (uint32_t i = 0; i < n; ++i) {
@@ -86,11 +65,26 @@ int Batch::create(Engine* const* engines, uint32_t n) {
         pre[2 * (n + 1) + i + 1] = static_cast<uint32_t>(total);
         pre[3 * (n + 1) + i + 1] = pre[3 * (n + 1) + i] + m[i]->n_windows;
     }
-    DTB_CU(cudaMalloc(reinterpret_cast<void**>(&d_views), sizeof(NetView) * n));
-    DTB_CU(cudaMalloc(reinterpret_cast<void**>(&d_prefix), sizeof(uint32_t) * pre.size()));
-    DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list), sizeof(uint32_t) * total));
-    DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_count), sizeof(uint32_t)));
-    DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_ticket), sizeof(uint32_t)));
+    DTB_CU(cudaStreamSynchronize(stream));
+    if (n > cap_members) {
+        if (d_views) cudaFree(d_views);
+        if (d_prefix) cudaFree(d_prefix);
+        d_views = nullptr;
+        d_prefix = nullptr;
+        DTB_CU(cudaMalloc(reinterpret_cast<void**>(&d_views), sizeof(NetView) * n));
+        DTB_CU(cudaMalloc(reinterpret_cast<void**>(&d_prefix), sizeof(uint32_t) * pre.size()));
+        cap_members = n;
+    }
+    if (total > cap_neurons) {
+        if (list) cudaFree(list);
+        list = nullptr;
+        DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list), sizeof(uint32_t) * total));
+        cap_neurons = total;
+    }
+    if (!list_count) {
+        DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_count), sizeof(uint32_t)));
+        DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_ticket), sizeof(uint32_t)));
+    }
     DTB_CU(cudaMemsetAsync(list_count, 0, sizeof(uint32_t), stream));
     DTB_CU(cudaMemsetAsync(list_ticket, 0, sizeof(uint32_t), stream));
     DTB_CU(cudaMemcpyAsync(d_prefix, pre.data(), sizeof(uint32_t) * pre.size(), cudaMemcpyHostToDevice, stream));
@@ -106,6 +100,11 @@ int Batch::create(Engine* const* engines, uint32_t n) {
     lb.spikes = SpikeList{list, list_count, list_ticket, static_cast<uint32_t>(total)};
     lb.win_prefix = d_prefix + 3 * (n + 1);
     lb.windows_total = pre[3 * (n + 1) + n];
+    if (graph) {
+        cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    }
+    std::memset(graph_key, 0, sizeof(graph_key));
     DTB_CU(cudaStreamSynchronize(stream));
     return DTB_OK;
 }

@@ -1,0 +1,42 @@
+// The batched form: several engines advanced by one launch of each per-step kernel.
+#pragma once
+
+#include <vector>
+
+#include "dtb_engine.h"
+
+namespace dtb {
+
+class Batch {
+public:
+    ~Batch();
+    int create(Engine* const* engines, uint32_t n);
+    int set_members(Engine* const* engines, uint32_t n);
+    int run(const dtb_run_request& rq, dtb_run_output* outs);
+    int refresh_views();
+
+    std::vector<Engine*> m;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev[2] = {nullptr, nullptr};
+    int sm_count = 148;
+    uint32_t wtype = W_F32;
+    NetView* d_views = nullptr;
+    uint32_t* d_prefix = nullptr;     // [lif n+1][pull n+1][vbase n+1][local windows n+1]
+    uint32_t* list = nullptr;
+    uint32_t* list_count = nullptr;
+    uint32_t* list_ticket = nullptr;
+    uint32_t cap_members = 0;         // capacity of d_views / d_prefix
+    uint64_t cap_neurons = 0;         // capacity of the spike list
+    LaunchBatch lb{};
+    PushCfg push_cfg{PUSH_REG, 8, 32};
+    uint32_t push_ctas = 0;
+    bool push_tuned[2] = {false, false};
+    bool autotune = true;
+    TuneResult tune;
+    bool use_graph = true;
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_key[6] = {0, 0, 0, 0, 0, 0};
+    uint32_t graph_launches = 0;
+};
+
+}  // namespace dtb

@@ -122,6 +122,13 @@ SIGNATURES = {
     "dtb_batch_set_push_variant": (_I32, [_P, _I32, _I32]),
     "dtb_batch_info": (_I32, [_P, _P, _P, _P, _P]),
     "dtb_compact_spikes_noalloc": (_I32, [_P, _U32, _P, _P, _P]),
+    "dtb_server_default_options": (None, [_P]),
+    "dtb_server_create": (_I32, [_P, C.POINTER(C.c_void_p)]),
+    "dtb_server_destroy": (_I32, [_P]),
+    "dtb_server_add_structured": (_I32, [_P, _P, _P, _P]),
+    "dtb_server_add_npz": (_I32, [_P, C.c_char_p, _P, _P]),
+    "dtb_server_play": (_I32, [_P, _U32, _P, _U32]),
+    "dtb_server_info": (_I32, [_P, _P]),
 }
 
 
@@ -193,6 +200,28 @@ def compact_spikes(d_bits, n, d_indices, d_count, stream=0):
     """Device spike bitmap -> ascending device index list (all pointers are device addresses)."""
     _check(LIB.dtb_compact_spikes(C.c_void_p(d_bits), n, C.c_void_p(d_indices), C.c_void_p(d_count),
                                   C.c_void_p(stream) if stream else None))
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [("hbm_cap_bytes", C.c_uint64), ("slice_steps", C.c_uint32), ("max_batch", C.c_uint32),
+                ("syn_mode", C.c_uint32), ("flags", C.c_uint32), ("autotune", C.c_uint32),
+                ("reserved", C.c_uint32 * 3)]
+
+
+class Request(C.Structure):
+    _fields_ = [("net", C.c_uint32), ("iters", C.c_uint32), ("arrival_s", C.c_double),
+                ("ou_mean", C.c_void_p), ("ou_sigma", C.c_void_p), ("ou_tau", C.c_void_p),
+                ("freqs", C.c_void_p), ("start_s", C.c_double), ("finish_s", C.c_double),
+                ("events", C.c_uint64), ("status", C.c_int32), ("reserved", C.c_uint32)]
+
+
+class ServerInfo(C.Structure):
+    _fields_ = [("n_nets", C.c_uint32), ("resident", C.c_uint32), ("resident_bytes", C.c_uint64),
+                ("evictions", C.c_uint64), ("restores", C.c_uint64), ("slices", C.c_uint64),
+                ("batch_members_sum", C.c_uint64)]
+
+
+SERVE_BATCHED, SERVE_SEQUENTIAL = 0, 1
 
 
 @dataclasses.dataclass
@@ -409,6 +438,91 @@ class Engine:
     def load_state(self, blob):
         blob = np.ascontiguousarray(blob, np.uint8)
         _check(LIB.dtb_load_state(self._h, _ptr(blob), blob.shape[0]))
+
+
+def _structured_c(spec, pop_id_base=0):
+    """The C spec of a network.StructuredSpec plus the arrays it points into (keep them alive)."""
+    keep = (_u32(spec.pop_sizes), _u32(spec.pop_exc), np.ascontiguousarray(spec.src_cdf, np.uint64),
+            np.ascontiguousarray(spec.property_rows(), np.float32))
+    s = StructuredSpecC(spec.n_pops, keep[0].ctypes.data, keep[1].ctypes.data, keep[2].ctypes.data,
+                        keep[3].ctypes.data, pop_id_base, spec.in_degree, spec.seed, int(spec.dyadic_weights))
+    return s, keep
+
+
+class Server:
+    """A pool of networks under an HBM cap serving a trace of simulate-window requests
+    (dtb_server_*): continuous batching or one request at a time."""
+
+    def __init__(self, hbm_cap_bytes=None, slice_steps=100, max_batch=64, syn_mode=SYN_PUSH, use_ou=True,
+                 autotune=True):
+        o = ServerOptions()
+        LIB.dtb_server_default_options(C.byref(o))
+        if hbm_cap_bytes is not None:
+            o.hbm_cap_bytes = int(hbm_cap_bytes)
+        o.slice_steps, o.max_batch, o.syn_mode = slice_steps, max_batch, syn_mode
+        o.flags = RUN_USE_OU if use_ou else 0
+        o.autotune = int(autotune)
+        h = C.c_void_p()
+        _check(LIB.dtb_server_create(C.byref(o), C.byref(h)))
+        self._h = h
+        self.n_pops = []
+
+    def add_structured(self, spec, **opts):
+        s, keep = _structured_c(spec)
+        o = default_options(**opts)
+        nid = C.c_uint32()
+        _check(LIB.dtb_server_add_structured(self._h, C.byref(s), C.byref(o), C.byref(nid)))
+        self.n_pops.append(spec.n_pops)
+        return nid.value
+
+    def add_npz(self, path, n_pops, **opts):
+        o = default_options(**opts)
+        nid = C.c_uint32()
+        _check(LIB.dtb_server_add_npz(self._h, os.fsencode(path), C.byref(o), C.byref(nid)))
+        self.n_pops.append(n_pops)
+        return nid.value
+
+    def play(self, requests, policy=SERVE_BATCHED):
+        """requests: dicts {net, iters, arrival_s, ou: (mean, sigma, tau) arrays or None}, sorted by
+        arrival.  Returns dicts with freqs [iters, P], start_s, finish_s, latency_s, events."""
+        arr = (Request * len(requests))()
+        keep, freqs = [], []
+        for i, r in enumerate(requests):
+            P = self.n_pops[r["net"]] if 0 <= r["net"] < len(self.n_pops) else 1   # the library rejects unknown ids
+            fr = np.zeros((r["iters"], P), np.int32)
+            freqs.append(fr)
+            arr[i].net, arr[i].iters, arr[i].arrival_s = r["net"], r["iters"], float(r["arrival_s"])
+            arr[i].freqs = fr.ctypes.data
+            if r.get("ou") is not None:
+                m, sd, tau = (np.ascontiguousarray(x, np.float32) for x in r["ou"])
+                keep.extend((m, sd, tau))
+                arr[i].ou_mean, arr[i].ou_sigma, arr[i].ou_tau = m.ctypes.data, sd.ctypes.data, tau.ctypes.data
+        _check(LIB.dtb_server_play(self._h, len(requests), arr, policy))
+        return [dict(freqs=freqs[i], start_s=arr[i].start_s, finish_s=arr[i].finish_s,
+                     latency_s=arr[i].finish_s - arr[i].arrival_s, events=int(arr[i].events), status=arr[i].status)
+                for i in range(len(requests))]
+
+    def info(self):
+        inf = ServerInfo()
+        _check(LIB.dtb_server_info(self._h, C.byref(inf)))
+        return {f: getattr(inf, f) for f, _ in ServerInfo._fields_}
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            _check(LIB.dtb_server_destroy(self._h))
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 class Batch:

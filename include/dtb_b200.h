@@ -272,6 +272,62 @@ int32_t dtb_batch_set_push_variant(void* batch, int32_t kind, int32_t param);
 int32_t dtb_batch_info(void* batch, uint32_t* n_members, uint32_t* graph_launches, int32_t* push_kind,
                        int32_t* push_param);
 
+/* --- serving form -----------------------------------------------------------
+ * No reference counterpart: the reference serves one network per process group,
+ * one Run RPC at a time (dist_simulator.cpp:3217-3451).  A server holds a pool of
+ * networks under an HBM cap and replays a trace of simulate-window requests in
+ * real time, either with continuous batching or one request at a time. */
+#define DTB_SERVE_BATCHED    0u  /* continuous batching over slices of slice_steps  */
+#define DTB_SERVE_SEQUENTIAL 1u  /* arrival order, one request at a time (dtb_run)   */
+
+typedef struct dtb_server_options {
+    uint64_t hbm_cap_bytes;  /* device memory of resident networks; idle ones beyond it are evicted to host */
+    uint32_t slice_steps;    /* steps per continuous-batching slice                               */
+    uint32_t max_batch;      /* most requests in flight together                                  */
+    uint32_t syn_mode;       /* DTB_SYN_* of every run                                            */
+    uint32_t flags;          /* DTB_RUN_USE_OU etc.; DTB_RUN_FREQ is always on                    */
+    uint32_t autotune;       /* 1: the batch autotunes its push variant once                      */
+    uint32_t reserved[3];
+} dtb_server_options;
+
+/* One request: Updateoubackgroundparam (optional) followed by Run(iter=iters)
+ * on one network, with RunResponse.freq of every step as the output. */
+typedef struct dtb_request {
+    uint32_t net;            /* id from dtb_server_add_*                                     */
+    uint32_t iters;          /* steps to simulate                                            */
+    double arrival_s;        /* seconds after the replay starts; non-decreasing over a trace */
+    const float* ou_mean;    /* [P] per population, or NULL to keep the current parameters   */
+    const float* ou_sigma;   /* [P]                                                          */
+    const float* ou_tau;     /* [P]                                                          */
+    int32_t* freqs;          /* [iters * P] per-step population spike counts, or NULL        */
+    double start_s;          /* out: first step issued (seconds after the replay starts)     */
+    double finish_s;         /* out: last step finished                                      */
+    uint64_t events;         /* out: synaptic events delivered                               */
+    int32_t status;          /* out: DTB_OK once served                                      */
+    uint32_t reserved;
+} dtb_request;
+
+typedef struct dtb_server_stats {
+    uint32_t n_nets;
+    uint32_t resident;           /* networks in HBM                         */
+    uint64_t resident_bytes;
+    uint64_t evictions;          /* networks moved to the host              */
+    uint64_t restores;           /* networks rebuilt from the host          */
+    uint64_t slices;             /* batched slices (or runs, sequentially)  */
+    uint64_t batch_members_sum;  /* sum over slices of requests in flight   */
+} dtb_server_stats;
+
+void dtb_server_default_options(dtb_server_options* opt);
+int32_t dtb_server_create(const dtb_server_options* opt, void** server);
+int32_t dtb_server_destroy(void* server);
+/* Add a network (built resident; idle networks are evicted if the cap requires). */
+int32_t dtb_server_add_structured(void* server, const dtb_structured_spec* spec, const dtb_options* opt,
+                                  uint32_t* net_id);
+int32_t dtb_server_add_npz(void* server, const char* path, const dtb_options* opt, uint32_t* net_id);
+/* Serve the n requests (sorted by arrival) under `policy`; fills their outputs. */
+int32_t dtb_server_play(void* server, uint32_t n, dtb_request* reqs, uint32_t policy);
+int32_t dtb_server_info(void* server, dtb_server_stats* info);
+
 /* --- state access (tests, checkpoint, serving eviction) ------------------ */
 #define DTB_STATE_V      0  /* float [n]                                       */
 #define DTB_STATE_J      1  /* float [n*4] (AMPA, NMDA, GABAa, GABAb per neuron) */

@@ -91,3 +91,21 @@ def test_host_csr_edge_cases():
     assert list(rows) == [7] and list(ptr) == [0, 4] and list(post) == [1, 0, 3, 1] and list(kind) == [0, 1, 0, 1]
     with pytest.raises(E.DtbError):
         E.build_out_csr_host(5, np.array([5]), np.array([0]), np.array([0]))
+
+
+def test_server_rejects_bad_traces_without_a_device():
+    """Trace validation happens before any device work."""
+    with E.Server() as srv:
+        with pytest.raises(E.DtbError) as ei:
+            srv.play([dict(net=0, iters=10, arrival_s=0.0)])     # no such network
+        assert ei.value.status == E.INVALID_PARAMETER
+        srv.n_pops.append(3)                                       # pretend a network of 3 populations
+        with pytest.raises(E.DtbError):
+            srv.play([dict(net=0, iters=10, arrival_s=0.0)])     # still unknown to the library
+    import ctypes as C
+    o = E.ServerOptions()
+    E.LIB.dtb_server_default_options(C.byref(o))
+    assert o.slice_steps == 100 and o.max_batch == 64 and o.hbm_cap_bytes == 150 * 10**9
+    o.slice_steps = 0
+    h = C.c_void_p()
+    assert E.LIB.dtb_server_create(C.byref(o), C.byref(h)) == E.INVALID_PARAMETER
