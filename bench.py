@@ -56,9 +56,10 @@ def parse():
     p.add_argument("--pops", type=int, default=N_POPS)
     p.add_argument("--degree", type=int, default=IN_DEGREE)
     p.add_argument("--push", default="auto", help="push kernel: auto (autotuned), reg:4|8|16|1016|1008, tma:256|512, local:8|1016")
-    p.add_argument("--form", default="plain", choices=["plain", "ensemble", "serve"],
+    p.add_argument("--form", default="plain", choices=["plain", "ensemble", "serve", "precision"],
                    help="plain: the 5M-neuron network; ensemble: 64 DA members batched (BF16) vs sequential (FP32); "
-                        "serve: Poisson request stream, continuous batching (BF16) vs one at a time (FP32)")
+                        "serve: Poisson request stream, continuous batching (BF16) vs one at a time (FP32); "
+                        "precision: bf16 + pull vs the FP64 oracle on a 200k-neuron network")
     p.add_argument("--requests", type=int, default=200, help="requests in the served trace (serve form)")
     p.add_argument("--rate", type=float, default=40.0, help="request arrival rate, 1/s (serve form)")
     p.add_argument("--slice", type=int, default=100, help="steps per continuous-batching slice (serve form)")
@@ -515,6 +516,90 @@ def run_serve(args):
     }
 
 
+def spike_agreement(a, b):
+    """First step where two rasters differ, and |A and B| / |A or B| over all steps."""
+    bad = np.nonzero((a != b).any(axis=1))[0]
+    inter = np.logical_and(a, b).sum()
+    union = np.logical_or(a, b).sum()
+    return (int(bad[0]) if bad.size else None), float(inter / max(union, 1))
+
+
+def run_precision(args):
+    """Precision form: bf16 weights + the deterministic pull kernel (and the float32 /
+    float-push variants) against the FP64 restatement of block_new on a 200k-neuron
+    network of the regional construction, with the float32 CPU model beside them."""
+    import __graft_entry__
+    __graft_entry__.load_package()
+    from dtb_b200 import engine as E
+    from dtb_b200 import network as nw
+    from oracle import c_oracle as cc
+
+    n = args.neurons if args.neurons != N_NEURONS else 200_000
+    pops = max(1, round(n / 25_000)) if args.pops == N_POPS else args.pops
+    steps, n_v = args.window, 64
+    warm = 200
+    spec = nw.structured_spec(n, pops, args.degree, SPEC_SEED)
+    net = cc.structured_edges(spec)
+    z = np.random.default_rng(7).standard_normal((steps, n), dtype=np.float32)
+    t0 = time.perf_counter()
+    sp64, cnt64, ev64, v64 = cc.COracle64(net).run(z, n_v=n_v)
+    t64 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sp32, _, _ = cc.COracle(net).run(z)
+    t32 = time.perf_counter() - t0
+    sp64c, _, _, _ = cc.COracle64(net).run(z, clock32=True)
+    del net
+    pop_of = np.repeat(np.arange(pops), spec.pop_sizes)
+
+    def pop_rates(sp):
+        return np.bincount(pop_of, weights=sp[warm:].sum(0), minlength=pops) / (spec.pop_sizes * (steps - warm)) * 1e4
+
+    r64 = pop_rates(sp64)
+
+    r32 = pop_rates(sp32)
+
+    def compare(sp, vt=None):
+        first, jac = spike_agreement(sp, sp64)
+        r = pop_rates(sp)
+        rel = np.abs(r - r64) / np.maximum(r64, 1e-9)
+        rel32 = np.abs(r - r32) / np.maximum(r32, 1e-9)
+        first32, jac32 = spike_agreement(sp, sp32)
+        out = {"first_divergence_step": first, "spike_jaccard": jac,
+               "rate_hz": float(sp[warm:].mean() * 1e4), "pop_rate_rel_err_median": float(np.median(rel)),
+               "pop_rate_rel_err_max": float(rel.max()),
+               "vs_f32_block_new": {"first_divergence_step": first32, "spike_jaccard": jac32,
+                                    "pop_rate_rel_diff_max": float(rel32.max())}}
+        if vt is not None:
+            upto = first if first is not None else steps
+            if upto > 0:
+                d = np.abs(vt[:upto] - v64[:upto]) / np.abs(v64[:upto])
+                out["v_rel_err_max_before_divergence"] = float(d.max())
+        return out
+
+    res = {"cpu_f32_block_new": compare(sp32), "cpu_fp64_with_float32_clock": compare(sp64c)}
+    idx = np.arange(n_v, dtype=np.uint32)
+    for name, wt, syn in (("gpu_bf16_pull", E.W_BF16, E.SYN_PULL), ("gpu_f32_pull", E.W_F32, E.SYN_PULL),
+                          ("gpu_bf16_push", E.W_BF16, E.SYN_PUSH), ("gpu_f32_push", E.W_F32, E.SYN_PUSH)):
+        with E.Engine.structured(spec, weight_type=wt, push=syn != E.SYN_PULL, pull=syn == E.SYN_PULL) as eng:
+            eng.set_noise_injected(z)
+            eng.set_samples(idx)
+            r = eng.run(steps, record_spikes=True, sample_v=True, syn_mode=syn)
+            res[name] = compare(r.spikes, r.sample_v)
+            res[name]["device_ms_per_step"] = r.device_ms / steps
+    return {
+        "metric": METRIC, "form": "precision", "value": res["gpu_bf16_pull"]["pop_rate_rel_err_median"],
+        "unit": "median relative error of population rates vs FP64", "n_gpus": 1, "steps": steps, "warmup": 0,
+        "higher_is_better": False, "dtype": "bf16-weights/f32-state",
+        "data": "synthetic (seeded regional network, replayed on the host for the oracles)",
+        "config": {"workload": f"{n}-neuron regional network, {pops} populations, in-degree {args.degree}, "
+                               f"{steps} steps, injected float32 normal draws shared by every run, "
+                               f"rates over steps {warm}-{steps}",
+                   "neurons": n, "synapses": int(spec.n_edges), "fp64_oracle_s": t64, "f32_oracle_s": t32,
+                   "fp64_rate_hz": float(sp64[warm:].mean() * 1e4), "fp64_events": ev64},
+        "vs_fp64": res,
+    }
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -542,6 +627,8 @@ def main():
         out = run_ensemble(args)
     elif args.form == "serve":
         out = run_serve(args)
+    elif args.form == "precision":
+        out = run_precision(args)
     else:
         out = run_ours(args)
     if out is not None:

@@ -50,6 +50,9 @@ def lib():
                                                  C.c_int32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
                                                  C.c_void_p]
         _lib.oracle_threads.restype = C.c_int32
+        _lib.oracle_run_f64.restype = C.c_int64
+        _lib.oracle_run_f64.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_int32, C.c_int32]
     return _lib
 
 
@@ -131,3 +134,60 @@ class COracle:
         ev = lib().oracle_run(C.byref(self._s), steps, self.dt, z.ctypes.data, None if u is None else u.ctypes.data,
                               self.prop_mode, None if sp is None else sp.ctypes.data, counts.ctypes.data)
         return (None if sp is None else sp.astype(bool)), counts, int(ev)
+
+
+class _Net64(C.Structure):
+    _fields_ = [("n", C.c_int32)] + [(f, C.c_void_p) for f in (
+        "in_ptr", "in_pre", "in_kind", "w0", "w1", "dtC", "neg_gL", "V_L", "V_th", "V_reset", "T_ref", "I_ext",
+        "g", "Vu", "decay", "ou_mean", "ou_f1", "ou_f2s", "V", "i_bg", "t_last", "J", "I_syn", "t", "active")]
+
+
+class COracle64:
+    """The FP64 restatement (block_new in float64): constants from
+    ``LifOracle(dtype=float64)``, state and arithmetic in double, threshold
+    propagation.  The normal draws are the float32 stream every run shares."""
+
+    def __init__(self, net, dt=0.1, ou=(0.6, 0.2, 10.0)):
+        ref = lo.LifOracle(dict(property=net["property"], input_neuron_idx=np.zeros(0, np.uint32),
+                                output_neuron_idx=np.zeros(0, np.uint32),
+                                input_channel_offset=np.zeros(0, np.uint8), weight=np.zeros((0, 2), np.float32)),
+                           dt=dt, ou=ou, dtype=np.float64)
+        self.n = n = ref.n
+        self.dt = dt
+        post = np.asarray(net["output_neuron_idx"], np.int64)
+        order = np.argsort(post, kind="stable")
+        self.in_ptr = np.concatenate([[0], np.cumsum(np.bincount(post, minlength=n))]).astype(np.int64)
+        self.in_pre = np.ascontiguousarray(np.asarray(net["input_neuron_idx"], np.uint32)[order])
+        self.in_kind = np.ascontiguousarray((np.asarray(net["input_channel_offset"]) != 0)[order].astype(np.uint8))
+        w = np.asarray(net["weight"], np.float32)[order]
+        self.w0 = np.ascontiguousarray(w[:, 0], np.float64)
+        self.w1 = np.ascontiguousarray(w[:, 1], np.float64)
+        f64 = lambda a: np.ascontiguousarray(np.broadcast_to(a, (n,)), np.float64)  # noqa: E731
+        self.consts = [f64(ref.dtC), f64(ref.neg_gL), f64(ref.V_L), f64(ref.V_th), f64(ref.V_reset), f64(ref.T_ref),
+                       f64(ref.i_ext), np.ascontiguousarray(ref.g_u, np.float64),
+                       np.ascontiguousarray(ref.V_u, np.float64), np.ascontiguousarray(ref.decay, np.float64),
+                       f64(ref.ou_mean), f64(ref.ou_f1), f64(ref.ou_f2s)]
+        self.V = f64(ref.V).copy()
+        self.i_bg = f64(ref.i_bg).copy()
+        self.t_last = f64(ref.t_last).copy()
+        self.J = np.zeros((4, n), np.float64)
+        self.I_syn = np.zeros(n, np.float64)
+        self.t = np.zeros(1, np.float64)
+        self._active = np.zeros(n, np.uint8)
+        self._s = _Net64(n, *(a.ctypes.data for a in (
+            [self.in_ptr, self.in_pre, self.in_kind, self.w0, self.w1] + self.consts +
+            [self.V, self.i_bg, self.t_last, self.J, self.I_syn, self.t, self._active])))
+
+    def run(self, z, record=True, n_v=0, clock32=False):
+        """Run z.shape[0] steps; returns (spikes [steps, n] bool or None, counts [steps], events,
+        V of the first n_v neurons after every step as float32 [steps, n_v]).  clock32 keeps the
+        clock in float32 (block_new's time) and everything else in double."""
+        z = np.ascontiguousarray(z, np.float32)
+        steps = z.shape[0]
+        sp = np.zeros((steps, self.n), np.uint8) if record else None
+        counts = np.zeros(steps, np.int64)
+        vt = np.zeros((steps, n_v), np.float32) if n_v else None
+        ev = lib().oracle_run_f64(C.byref(self._s), steps, self.dt, z.ctypes.data,
+                                  None if sp is None else sp.ctypes.data, counts.ctypes.data,
+                                  None if vt is None else vt.ctypes.data, n_v, int(clock32))
+        return (None if sp is None else sp.astype(bool)), counts, int(ev), vt

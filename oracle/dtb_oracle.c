@@ -130,6 +130,98 @@ int64_t oracle_run(oracle_net* s, int32_t steps, float dt, const float* z, const
     return events;
 }
 
+/* ---- FP64 restatement ---------------------------------------------------
+ * The same step in double precision throughout (constants derived in double by
+ * lif_oracle.LifOracle(dtype=float64); weights widened exactly; the normal draws
+ * widened from the float32 stream every run shares).  This is block_new under
+ * torch.set_default_dtype(torch.float64), the reference for precision
+ * statements about float32 and bf16 runs. */
+typedef struct {
+    int32_t n;
+    const int64_t* in_ptr;
+    const uint32_t* in_pre;
+    const uint8_t* in_kind;
+    const double* w0;
+    const double* w1;
+    const double* dtC;
+    const double* neg_gL;
+    const double* V_L;
+    const double* V_th;
+    const double* V_reset;
+    const double* T_ref;
+    const double* I_ext;
+    const double* g;          /* [4*n] channel-major */
+    const double* Vu;
+    const double* decay;
+    const double* ou_mean;
+    const double* ou_f1;
+    const double* ou_f2s;
+    double* V;
+    double* i_bg;
+    double* t_last;
+    double* J;
+    double* I_syn;
+    double* t;
+    uint8_t* active;
+} oracle_net64;
+
+/* Threshold propagation only.  V_out [steps*n_v] receives V of the first n_v
+ * neurons after every step when non-NULL.  clock32 != 0 rounds the clock to
+ * float32 after every `t += dt` (block_new's float32 time) and keeps everything
+ * else in double: it isolates the part of a float32 run's difference that the
+ * refractory test `t >= t_last + T_ref` makes. */
+int64_t oracle_run_f64(oracle_net64* s, int32_t steps, double dt, const float* z, uint8_t* spikes_out,
+                       int64_t* counts_out, float* V_out, int32_t n_v, int32_t clock32) {
+    const int32_t n = s->n;
+    int64_t events = 0;
+    for (int32_t st = 0; st < steps; ++st) {
+        const float* zs = z + (int64_t)st * n;
+        const double t = clock32 ? (double)(float)(*s->t + dt) : *s->t + dt;
+        *s->t = t;
+        int64_t cnt = 0;
+#pragma omp parallel for schedule(static) reduction(+ : cnt)
+        for (int32_t i = 0; i < n; ++i) {
+            const double ib = s->i_bg[i] + (s->ou_f1[i] * (s->ou_mean[i] - s->i_bg[i]) + s->ou_f2s[i] * (double)zs[i]);
+            s->i_bg[i] = ib;
+            const double cd = ((s->neg_gL[i] * (s->V[i] - s->V_L[i]) + s->I_syn[i]) + s->I_ext[i]) + ib;
+            const double vn = s->V[i] + s->dtC[i] * cd;
+            const double v = t >= s->t_last[i] + s->T_ref[i] ? vn : s->V_reset[i];
+            const uint8_t a = v >= s->V_th[i];
+            s->V[i] = v < s->V_th[i] ? v : s->V_th[i];
+            s->active[i] = a;
+            cnt += a;
+        }
+        int64_t ev = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : ev)
+        for (int32_t i = 0; i < n; ++i) {
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int64_t e = s->in_ptr[i]; e < s->in_ptr[i + 1]; ++e) {
+                if (s->active[s->in_pre[e]]) {
+                    const int c = s->in_kind[e] ? 2 : 0;
+                    acc[c] += s->w0[e];
+                    acc[c + 1] += s->w1[e];
+                    ++ev;
+                }
+            }
+            double I = 0.0;
+            for (int c = 0; c < 4; ++c) {
+                const int64_t k = (int64_t)c * n + i;
+                const double j = s->J[k] * s->decay[k] + acc[c];
+                s->J[k] = j;
+                I += s->g[k] * (s->Vu[k] - s->V[i]) * j;
+            }
+            s->I_syn[i] = I;
+            if (s->active[i]) s->t_last[i] = t;
+        }
+        events += ev;
+        if (spikes_out) memcpy(spikes_out + (int64_t)st * n, s->active, (size_t)n);
+        if (counts_out) counts_out[st] = cnt;
+        if (V_out)
+            for (int32_t i = 0; i < n_v; ++i) V_out[(int64_t)st * n_v + i] = (float)s->V[i];
+    }
+    return events;
+}
+
 /* ---- Philox4x32-10 and the regional-network edge stream ---------------- */
 static void philox(uint32_t c[4], uint32_t k0, uint32_t k1) {
     for (int r = 0; r < 10; ++r) {
