@@ -23,7 +23,7 @@ Batch::~Batch() {
     if (stream) cudaStreamSynchronize(stream);
     if (graph) cudaGraphExecDestroy(graph);
     for (void* p : {static_cast<void*>(d_views), static_cast<void*>(d_prefix), static_cast<void*>(list),
-                    static_cast<void*>(list_count), static_cast<void*>(list_ticket)})
+                    static_cast<void*>(list_count), static_cast<void*>(list_ticket), static_cast<void*>(local_scratch)})
         if (p) cudaFree(p);
     for (cudaEvent_t e : {ev0, ev1, tev[0], tev[1]})
         if (e) cudaEventDestroy(e);
@@ -81,6 +81,13 @@ int Batch::set_members(Engine* const* engines, uint32_t n) {
         DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list), sizeof(uint32_t) * total));
         cap_neurons = total;
     }
+    const uint32_t windows = pre[3 * (n + 1) + n];
+    if (windows > cap_windows) {
+        if (local_scratch) cudaFree(local_scratch);
+        local_scratch = nullptr;
+        DTB_CU(cudaMalloc(reinterpret_cast<void**>(&local_scratch), sizeof(uint32_t) * (2ull * windows + 2)));
+        cap_windows = windows;
+    }
     if (!list_count) {
         DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_count), sizeof(uint32_t)));
         DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_ticket), sizeof(uint32_t)));
@@ -99,7 +106,9 @@ int Batch::set_members(Engine* const* engines, uint32_t n) {
     lb.lif_ctas = static_cast<uint32_t>(sm_count) * m[0]->lif_ctas_per_sm;
     lb.spikes = SpikeList{list, list_count, list_ticket, static_cast<uint32_t>(total)};
     lb.win_prefix = d_prefix + 3 * (n + 1);
-    lb.windows_total = pre[3 * (n + 1) + n];
+    lb.windows_total = windows;
+    lb.local_scratch = local_scratch;
+    lb.sm_count = static_cast<uint32_t>(sm_count);
     if (graph) {
         cudaGraphExecDestroy(graph);
         graph = nullptr;

@@ -230,6 +230,8 @@ LaunchBatch Engine::single_batch() const {
     b.spikes = SpikeList{list, list_count, list_ticket, n_pad};
     b.win_prefix = prefix_dev + 6;
     b.windows_total = n_windows;
+    b.local_scratch = local_scratch;
+    b.sm_count = static_cast<uint32_t>(sm_count);
     return b;
 }
 
@@ -313,6 +315,7 @@ int Engine::build_local_tables() {
     DTB_TRY(dalloc(woff, rb, false));
     DTB_TRY(dalloc(pop_loc, P, false));
     DTB_TRY(dalloc(win_tab, wins.size(), false));
+    DTB_TRY(dalloc(local_scratch, 2 * wins.size() + 2));
     DTB_CU(cudaMemcpyAsync(pop_loc, loc.data(), sizeof(uint4) * P, cudaMemcpyHostToDevice, stream));
     DTB_CU(cudaMemcpyAsync(win_tab, wins.data(), sizeof(uint4) * wins.size(), cudaMemcpyHostToDevice, stream));
     DTB_CU(build_local_offsets(out_ptr, out_col, out_w, static_cast<int>(wtype), pop_off_dev, P, n, pop_loc, nullptr,

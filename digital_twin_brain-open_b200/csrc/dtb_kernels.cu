@@ -502,14 +502,23 @@ push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase
 }
 
 // ---------------------------------------------------------------------------
-// Population-local push, phase B: one CTA per window of a population.  The CTA
-// zeroes four accumulator planes (AMPA, NMDA, GABAa, GABAb) for the neurons of
-// its window in shared memory, finds its population's spiking rows in the
-// propagated bitmap, adds each row's synapses into the window (the span between
-// two woff boundaries: contiguous, because rows are sorted by postsynaptic
-// neuron), and adds the window to J with coalesced 128-bit read-modify-writes.
-// Windows are disjoint and phase A (the cross-population spans) has finished, so
-// the write-back needs no atomics.
+// Population-local push, phase B.  Each population with local windows is cut
+// into windows of at most kLocalWin neurons; a row's synapses into one window
+// are a contiguous span (rows are sorted by postsynaptic neuron) between two
+// woff boundaries.  The work of a step is split into units of up to
+// kLocalUnitRows spiking rows of one window's population:
+//
+//   local_count_kernel   spiking rows of each window's population (bitmap popcount)
+//   local_scan_kernel    units per window -> exclusive prefix; resets the unit counter
+//   push_local_kernel    persistent, one 1024-thread CTA per SM: takes units from an
+//                        atomic counter, finds the unit's rows by a block-wide prefix
+//                        over the population's bitmap, sums their window spans into
+//                        shared memory, and flushes the window to J with coalesced
+//                        red.global.add.v4.f32 when it moves to another window.
+//
+// A bursting population becomes many units spread over every SM, so the step is
+// balanced whatever the activity pattern; the L2 sees one 16-byte reduction per
+// touched neuron per flush instead of one per synapse.
 //
 // The window sums are 32-bit fixed point: w is rounded to a multiple of 2^-s and
 // added with red.shared.add.u32 (native, fire-and-forget; a shared-memory float
@@ -521,107 +530,233 @@ push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase
 // ---------------------------------------------------------------------------
 constexpr int kLocalThreads = 1024;
 constexpr int kLocalUnroll = 8;
+constexpr uint32_t kLocalUnitRows = 512;
+constexpr size_t kLocalSmem = 4ull * kLocalWin * sizeof(int) + kLocalUnitRows * (2 * sizeof(uint32_t) + sizeof(unsigned long long));
 
 __device__ __forceinline__ void red_add_shared_u32(const void* p, uint32_t v) {
     asm volatile("red.shared.add.u32 [%0], %1;" :: "r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))), "r"(v) : "memory");
 }
+__device__ __forceinline__ void red_add_f32x4(float4* addr, float4 v) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" :: "l"(addr), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+                 : "memory");
+}
 
-constexpr size_t kLocalSmem = 4ull * kLocalWin * sizeof(int);
+// Spiking-row bitmap word wi of the population [p_lo, p_hi), bits outside masked off.
+__device__ __forceinline__ uint32_t pop_word(const uint32_t* bits, uint32_t wi, uint32_t p_lo, uint32_t p_hi) {
+    uint32_t m = bits[wi];
+    const uint32_t b0 = wi << 5;
+    if (b0 < p_lo) m &= ~0u << (p_lo - b0);
+    if (p_hi - b0 < 32u) m &= (1u << (p_hi - b0)) - 1u;
+    return m;
+}
+
+// Exclusive prefix of v over the block (blockDim.x a multiple of 32); *total = sum.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s_warp, uint32_t* total) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= static_cast<uint32_t>(o)) incl += y;
+    }
+    __syncthreads();
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t x = lane < nw ? s_warp[lane] : 0u;
+        uint32_t xi = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, xi, o);
+            if (lane >= static_cast<uint32_t>(o)) xi += y;
+        }
+        if (lane < nw) s_warp[lane] = xi - x;
+        if (lane == 31) s_warp[32] = xi;
+    }
+    __syncthreads();
+    *total = s_warp[32];
+    return s_warp[warp] + incl - v;
+}
+
+struct LocalWindow {
+    const NetView* nv;
+    uint32_t a, lo, hi, k, ka1, p_lo, p_hi;
+    unsigned long long rb_k;
+    float scale, unscale;
+};
+
+__device__ __forceinline__ void load_window(const NetView* __restrict__ nets, const uint32_t* __restrict__ win_prefix,
+                                            uint32_t n_nets, uint32_t gwin, LocalWindow& W) {
+    const uint32_t net = n_nets > 1 ? find_net(win_prefix, n_nets, gwin) : 0u;
+    W.nv = nets + net;
+    const uint4 wt = W.nv->win_tab[gwin - __ldg(win_prefix + net)];
+    W.a = wt.x;
+    W.lo = wt.y;
+    W.hi = wt.z;
+    W.k = wt.w & 0xFFFFu;
+    const int sh = static_cast<int>(wt.w >> 16);     // fixed-point exponent s, 16..60
+    W.scale = __int_as_float((127 + sh) << 23);      // 2^s
+    W.unscale = __int_as_float((127 - sh) << 23);    // 2^-s
+    const uint4 pl = W.nv->pop_loc[W.a];
+    W.ka1 = pl.x + 1u;
+    W.rb_k = (static_cast<unsigned long long>(pl.z) | (static_cast<unsigned long long>(pl.w) << 32)) + W.k;
+    W.p_lo = __ldg(W.nv->pop_off + W.a);
+    W.p_hi = __ldg(W.nv->pop_off + W.a + 1);
+}
+
+// scratch: [windows] spiking rows of each window's population, [windows + 1]
+// unit prefix, [1] unit counter.
+__global__ void __launch_bounds__(256)
+local_count_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ win_prefix, uint32_t n_nets,
+                   uint32_t* scratch) {
+    __shared__ uint32_t s_warp[33];
+    LocalWindow W;
+    load_window(nets, win_prefix, n_nets, blockIdx.x, W);
+    const uint32_t* bits = (W.nv->clock->n & 1ull) ? W.nv->bits1 : W.nv->bits0;
+    uint32_t c = 0;
+    for (uint32_t wi = (W.p_lo >> 5) + threadIdx.x; wi < ((W.p_hi + 31) >> 5); wi += blockDim.x)
+        c += __popc(pop_word(bits, wi, W.p_lo, W.p_hi));
+    uint32_t total;
+    block_exclusive_scan(c, s_warp, &total);
+    if (threadIdx.x == 0) scratch[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024)
+local_scan_kernel(uint32_t* scratch, uint32_t windows) {
+    __shared__ uint32_t s_warp[33];
+    uint32_t* upre = scratch + windows;
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < windows; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t u = i < windows ? (scratch[i] + kLocalUnitRows - 1) / kLocalUnitRows : 0u;
+        uint32_t total;
+        const uint32_t ex = block_exclusive_scan(u, s_warp, &total);
+        if (i < windows) upre[i] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) {
+        upre[windows] = carry;
+        upre[windows + 1] = 0u;      // the unit counter
+    }
+}
+
+// Add the window's fixed-point sums to J (coalesced 16-byte reductions of the
+// touched neurons) and clear them.
+__device__ __forceinline__ void local_flush(const LocalWindow& W, int* acc) {
+    __syncthreads();
+    float4* J = W.nv->J + W.lo;
+    const uint32_t width = W.hi - W.lo;
+    for (uint32_t i = threadIdx.x; i < width; i += kLocalThreads) {
+        const int4 v = make_int4(acc[i], acc[kLocalWin + i], acc[2 * kLocalWin + i], acc[3 * kLocalWin + i]);
+        if (v.x | v.y | v.z | v.w) {
+            red_add_f32x4(J + i, make_float4(__fmul_rn(__int2float_rn(v.x), W.unscale), __fmul_rn(__int2float_rn(v.y), W.unscale),
+                                             __fmul_rn(__int2float_rn(v.z), W.unscale), __fmul_rn(__int2float_rn(v.w), W.unscale)));
+            acc[i] = 0;
+            acc[kLocalWin + i] = 0;
+            acc[2 * kLocalWin + i] = 0;
+            acc[3 * kLocalWin + i] = 0;
+        }
+    }
+    __syncthreads();
+}
 
 template <int WT>
 __global__ void __launch_bounds__(kLocalThreads, 1)
-push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ win_prefix, uint32_t n_nets) {
+push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ win_prefix, uint32_t n_nets,
+                  uint32_t windows, uint32_t* scratch) {
     // plane c of kLocalWin 32-bit sums: random targets spread over all 32 banks
     extern __shared__ int acc[];
-    const uint32_t gwin = blockIdx.x;
-    const uint32_t net = n_nets > 1 ? find_net(win_prefix, n_nets, gwin) : 0u;
-    const NetView& nv = nets[net];
-    const uint4 wt = nv.win_tab[gwin - __ldg(win_prefix + net)];
-    const uint32_t a = wt.x, lo = wt.y, hi = wt.z, k = wt.w & 0xFFFFu;
-    const int sh = static_cast<int>(wt.w >> 16);                  // fixed-point exponent s, 16..60
-    const float scale = __int_as_float((127 + sh) << 23);         // 2^s
-    const float unscale = __int_as_float((127 - sh) << 23);       // 2^-s
-    const uint32_t width = hi - lo;
-    for (uint32_t i = threadIdx.x; i < 4 * kLocalWin; i += kLocalThreads) acc[i] = 0;
-    const uint4 pl = nv.pop_loc[a];
-    const uint32_t ka = pl.x;
-    const unsigned long long rb = static_cast<unsigned long long>(pl.z) | (static_cast<unsigned long long>(pl.w) << 32);
-    const uint32_t p_lo = __ldg(nv.pop_off + a), p_hi = __ldg(nv.pop_off + a + 1);
-    const uint32_t* bits = (nv.clock->n & 1ull) ? nv.bits1 : nv.bits0;
-    const unsigned long long* ptr = nv.out_ptr;
-    const uint32_t* col = nv.out_col;
-    const void* wts = nv.out_w;
-    const uint32_t* woff = nv.woff;
+    uint32_t* s_rows = reinterpret_cast<uint32_t*>(acc + 4 * kLocalWin);
+    uint32_t* s_len = s_rows + kLocalUnitRows;
+    unsigned long long* s_start = reinterpret_cast<unsigned long long*>(s_len + kLocalUnitRows);
+    __shared__ uint32_t s_warp[33];
+    __shared__ uint32_t s_unit;
+    const uint32_t* rows_of = scratch;
+    const uint32_t* upre = scratch + windows;
+    uint32_t* counter = scratch + 2 * windows + 1;
+    const uint32_t total_units = upre[windows];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    constexpr uint32_t kWarps = kLocalThreads / 32;
-    const uint32_t w_lo = p_lo >> 5, w_hi = (p_hi + 31) >> 5;
-    __syncthreads();
-    // lane l of warp w reads word base + l * kWarps + w: every warp gets words
-    // spread over the whole population, so small populations still use all warps
-    for (uint32_t base = w_lo; base < w_hi; base += 32 * kWarps) {
-        const uint32_t wi = base + lane * kWarps + warp;
-        uint32_t m = 0;
-        if (wi < w_hi) {
-            m = bits[wi];
-            const uint32_t b0 = wi << 5;
-            if (b0 < p_lo) m &= ~0u << (p_lo - b0);
-            if (p_hi - b0 < 32u) m &= (1u << (p_hi - b0)) - 1u;
+    for (uint32_t i = threadIdx.x; i < 4 * kLocalWin; i += kLocalThreads) acc[i] = 0;
+    LocalWindow W{};
+    uint32_t cur = 0xFFFFFFFFu;
+    for (;;) {
+        if (threadIdx.x == 0) s_unit = atomicAdd(counter, 1u);
+        __syncthreads();
+        const uint32_t u = s_unit;
+        if (u >= total_units) break;
+        // the unit's window: the last w with upre[w] <= u (windows without units repeat a value)
+        uint32_t lo_w = 0, hi_w = windows - 1;
+        while (lo_w < hi_w) {
+            const uint32_t mid = (lo_w + hi_w + 1) >> 1;
+            if (upre[mid] <= u) lo_w = mid; else hi_w = mid - 1;
         }
-        while (__any_sync(0xffffffffu, m != 0u)) {
-            // every lane with spikes left takes one row: its metadata loads overlap
-            uint32_t s0 = 0, s1 = 0;
-            unsigned long long rbeg = 0;
-            if (m) {
+        const uint32_t gw = lo_w;
+        if (gw != cur) {
+            if (cur != 0xFFFFFFFFu) local_flush(W, acc);
+            load_window(nets, win_prefix, n_nets, gw, W);
+            cur = gw;
+        }
+        const uint32_t r_lo = (u - upre[gw]) * kLocalUnitRows;
+        const uint32_t r_hi = min(r_lo + kLocalUnitRows, rows_of[gw]);
+        // rows with population rank in [r_lo, r_hi): block prefix over the bitmap
+        const uint32_t* bits = (W.nv->clock->n & 1ull) ? W.nv->bits1 : W.nv->bits0;
+        const uint32_t w_lo = W.p_lo >> 5, w_hi = (W.p_hi + 31) >> 5;
+        const uint32_t per = (w_hi - w_lo + kLocalThreads - 1) / kLocalThreads;
+        const uint32_t my_lo = min(w_lo + threadIdx.x * per, w_hi), my_hi = min(my_lo + per, w_hi);
+        uint32_t c = 0;
+        for (uint32_t wi = my_lo; wi < my_hi; ++wi) c += __popc(pop_word(bits, wi, W.p_lo, W.p_hi));
+        uint32_t total;
+        uint32_t rank = block_exclusive_scan(c, s_warp, &total);
+        for (uint32_t wi = my_lo; wi < my_hi && rank < r_hi; ++wi) {
+            uint32_t m = pop_word(bits, wi, W.p_lo, W.p_hi);
+            if (rank + __popc(m) <= r_lo) { rank += __popc(m); continue; }
+            while (m && rank < r_hi) {
                 const uint32_t j = (wi << 5) + static_cast<uint32_t>(__ffs(m) - 1);
                 m &= m - 1u;
-                rbeg = __ldg(ptr + j);
-                const uint32_t* wo = woff + rb + static_cast<unsigned long long>(j - p_lo) * (ka + 1u) + k;
-                s0 = __ldg(wo);
-                s1 = __ldg(wo + 1);
+                if (rank >= r_lo) s_rows[rank - r_lo] = j;
+                ++rank;
             }
-            uint32_t rows = __ballot_sync(0xffffffffu, s1 > s0);
-            while (rows) {
-                const int src = __ffs(rows) - 1;
-                rows &= rows - 1u;
-                const unsigned long long rbase = __shfl_sync(0xffffffffu, rbeg, src);
-                const unsigned long long e1 = rbase + __shfl_sync(0xffffffffu, s1, src);
-                for (unsigned long long e = rbase + __shfl_sync(0xffffffffu, s0, src) + lane; e < e1;
-                     e += 32ull * kLocalUnroll) {
-                    uint32_t c[kLocalUnroll];
-                    float2 w[kLocalUnroll];
+        }
+        __syncthreads();
+        const uint32_t nrows = r_hi - r_lo;
+        // span of every row of the unit: [out_ptr[j] + woff[k], out_ptr[j] + woff[k + 1])
+        const NetView& nv = *W.nv;
+        for (uint32_t r = threadIdx.x; r < nrows; r += kLocalThreads) {
+            const uint32_t j = s_rows[r];
+            const uint32_t* wo = nv.woff + W.rb_k + static_cast<unsigned long long>(j - W.p_lo) * W.ka1;
+            const uint32_t s0 = __ldg(wo), s1 = __ldg(wo + 1);
+            s_start[r] = __ldg(nv.out_ptr + j) + s0;
+            s_len[r] = s1 - s0;
+        }
+        __syncthreads();
+        const uint32_t* col = nv.out_col;
+        const void* wts = nv.out_w;
+        for (uint32_t r = warp; r < nrows; r += kLocalThreads / 32) {
+            const unsigned long long e0 = s_start[r], e1 = e0 + s_len[r];
+            for (unsigned long long e = e0 + lane; e < e1; e += 32ull * kLocalUnroll) {
+                uint32_t cc[kLocalUnroll];
+                float2 w[kLocalUnroll];
 #pragma unroll
-                    for (int q = 0; q < kLocalUnroll; ++q) {
-                        const unsigned long long idx = e + 32ull * q;
-                        if (idx < e1) {
-                            c[q] = __ldcs(col + idx);
-                            w[q] = load_weight<WT>(wts, idx);
-                        }
+                for (int q = 0; q < kLocalUnroll; ++q) {
+                    const unsigned long long idx = e + 32ull * q;
+                    if (idx < e1) {
+                        cc[q] = __ldcs(col + idx);
+                        w[q] = load_weight<WT>(wts, idx);
                     }
+                }
 #pragma unroll
-                    for (int q = 0; q < kLocalUnroll; ++q) {
-                        if (e + 32ull * q < e1) {
-                            const int* d = acc + (c[q] >> 31) * (2u * kLocalWin) + ((c[q] & kIndexMask) - lo);
-                            red_add_shared_u32(d, static_cast<uint32_t>(__float2int_rn(__fmul_rn(w[q].x, scale))));
-                            red_add_shared_u32(d + kLocalWin, static_cast<uint32_t>(__float2int_rn(__fmul_rn(w[q].y, scale))));
-                        }
+                for (int q = 0; q < kLocalUnroll; ++q) {
+                    if (e + 32ull * q < e1) {
+                        const int* d = acc + (cc[q] >> 31) * (2u * kLocalWin) + ((cc[q] & kIndexMask) - W.lo);
+                        red_add_shared_u32(d, static_cast<uint32_t>(__float2int_rn(__fmul_rn(w[q].x, W.scale))));
+                        red_add_shared_u32(d + kLocalWin, static_cast<uint32_t>(__float2int_rn(__fmul_rn(w[q].y, W.scale))));
                     }
                 }
             }
         }
+        __syncthreads();
     }
-    __syncthreads();
-    float4* J = nv.J + lo;
-    for (uint32_t i = threadIdx.x; i < width; i += kLocalThreads) {
-        const int4 v = make_int4(acc[i], acc[kLocalWin + i], acc[2 * kLocalWin + i], acc[3 * kLocalWin + i]);
-        if (v.x | v.y | v.z | v.w) {
-            float4 x = J[i];
-            x.x = __fadd_rn(x.x, __fmul_rn(__int2float_rn(v.x), unscale));
-            x.y = __fadd_rn(x.y, __fmul_rn(__int2float_rn(v.y), unscale));
-            x.z = __fadd_rn(x.z, __fmul_rn(__int2float_rn(v.z), unscale));
-            x.w = __fadd_rn(x.w, __fmul_rn(__int2float_rn(v.w), unscale));
-            J[i] = x;
-        }
-    }
+    if (cur != 0xFFFFFFFFu) local_flush(W, acc);
 }
 
 __device__ inline uint32_t row_lower_bound(const uint32_t* __restrict__ col, unsigned long long beg,
@@ -1101,8 +1236,12 @@ static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint
             push_kernel<ACC, WT, 8, 16, 1><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes);
         else
             push_kernel<ACC, WT, 8, 32, 1><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes);
-        if (b.windows_total)
-            push_local_kernel<WT><<<b.windows_total, kLocalThreads, kLocalSmem, s>>>(b.nets, b.win_prefix, b.n_nets);
+        if (b.windows_total) {
+            local_count_kernel<<<b.windows_total, 256, 0, s>>>(b.nets, b.win_prefix, b.n_nets, b.local_scratch);
+            local_scan_kernel<<<1, 1024, 0, s>>>(b.local_scratch, b.windows_total);
+            push_local_kernel<WT><<<b.sm_count, kLocalThreads, kLocalSmem, s>>>(b.nets, b.win_prefix, b.n_nets,
+                                                                                 b.windows_total, b.local_scratch);
+        }
     } else if (cfg.kind == PUSH_REG || cfg.kind == PUSH_LOCAL) {
         const dim3 grid(ctas), block(kPushThreads);
         if (cfg.lpr == 16) {

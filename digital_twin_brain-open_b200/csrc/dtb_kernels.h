@@ -21,6 +21,8 @@ struct LaunchBatch {
     uint32_t lif_ctas;            // persistent grid of the LIF kernel
     const uint32_t* win_prefix;   // device [n_nets + 1] cumulative local-push windows
     uint32_t windows_total;
+    uint32_t* local_scratch;      // device [2 * windows_total + 2]: rows per window, unit prefix, unit counter
+    uint32_t sm_count;
     SpikeList spikes;
 };
 
@@ -43,9 +45,9 @@ extern const PushCfg kPushCands[kPushCandidates];
 cudaError_t push_prepare(int exact, int weight_type, const PushCfg& cfg, int sm_count, uint32_t* ctas);
 cudaError_t launch_push(const LaunchBatch& b, int exact, int weight_type, const PushCfg& cfg, uint32_t ctas,
                         cudaStream_t s);
-// Kernels launch_push issues beyond the first (the local variant's window pass).
+// Kernels launch_push issues beyond the first (the local variant's count, scan and window passes).
 inline uint32_t push_extra_launches(const LaunchBatch& b, int exact, const PushCfg& cfg) {
-    return (cfg.kind == PUSH_LOCAL && !exact && b.windows_total) ? 1u : 0u;
+    return (cfg.kind == PUSH_LOCAL && !exact && b.windows_total) ? 3u : 0u;
 }
 cudaError_t launch_pull(const LaunchBatch& b, int gather, int weight_type, uint32_t flags, int prop_mode, cudaStream_t s);
 cudaError_t launch_fold_finish(const LaunchBatch& b, cudaStream_t s);
