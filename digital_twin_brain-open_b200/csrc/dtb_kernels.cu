@@ -19,6 +19,7 @@
 // a binary search over the batch's tile prefix; every network keeps its own clock,
 // and the last CTA of a network to finish (ticket counter) advances that clock.
 #include <algorithm>
+#include <atomic>
 
 #include "dtb_device.cuh"
 #include "dtb_kernels.h"
@@ -187,57 +188,138 @@ __device__ inline void advance_clock(const NetView& nv, uint32_t tiles, float t,
     }
 }
 
+// mbarrier and bulk-copy helpers (cp.async.bulk, no multicast).
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    uint64_t g;
+    asm volatile("cvta.to.global.u64 %0, %1;" : "=l"(g) : "l"(src));
+    asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_addr(dst)), "l"(g), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                 : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// Bounded wait on one mbarrier phase; false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (uint32_t it = 0; it < kWaitLimit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 // ---------------------------------------------------------------------------
 // Fused LIF step (push and exact-push modes): a persistent grid walks the
-// batch's 1024-neuron tiles.  Per tile, every thread issues its state loads
-// first (V, i_ou, t_last, J, noise draws), then steps its 4 neurons.
+// batch's 1024-neuron tiles.  A tile's state (V, i_ou, t_last: 4 KiB each; J:
+// 16 KiB) moves by bulk copies (cp.async.bulk, no multicast) through a
+// two-stage ring in shared memory: the copies of the next tile are in flight
+// while the CTA steps the current one, each thread steps its quad of neurons
+// one neuron at a time in the stage, and the finished tile leaves by bulk
+// stores.  Two CTA barriers per tile: one before the stage of the next tile is
+// refilled, one before the finished stage is stored.  Spike-list slots are
+// taken per warp; the device clock's ticket is taken once per CTA and network.
+// Every mbarrier wait is bounded; a wait that runs out raises kErrTimeout (the
+// host turns it into DTB_DEVICE_FAULT) after one more bounded wait.
 // ---------------------------------------------------------------------------
+constexpr uint32_t kLifStageFloats = 3 * kLifTile + 4 * kLifTile;   // V | i_ou | t_last | J (float4)
+constexpr size_t kLifSmem = 2ull * kLifStageFloats * sizeof(float);
+
+__device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, uint32_t bytes) {
+    uint64_t g;
+    asm volatile("cvta.to.global.u64 %0, %1;" : "=l"(g) : "l"(gdst));
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                 :: "l"(g), "r"(smem_addr(ssrc)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// thread 0: issue the copies of tile `gt` into stage `stg`
+__device__ __forceinline__ void lif_prefetch(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_prefix,
+                                             uint32_t n_nets, uint32_t gt, float* stage, uint64_t* bar) {
+    const uint32_t net = n_nets > 1 ? find_net(tile_prefix, n_nets, gt) : 0u;
+    const NetView* nv = nets + net;
+    const size_t first = static_cast<size_t>(gt - __ldg(tile_prefix + net)) * kLifTile;
+    mbar_expect_tx(bar, static_cast<uint32_t>(kLifStageFloats * sizeof(float)));
+    bulk_load(stage, nv->V + first, kLifTile * sizeof(float), bar);
+    bulk_load(stage + kLifTile, nv->iou + first, kLifTile * sizeof(float), bar);
+    bulk_load(stage + 2 * kLifTile, nv->tlast + first, kLifTile * sizeof(float), bar);
+    bulk_load(stage + 3 * kLifTile, nv->J + first, kLifTile * sizeof(float4), bar);
+}
+
+// thread 0: the CTA finished `cnt` tiles of `nv`; the last CTA of the network advances its clock
+__device__ __forceinline__ void lif_ticket(const NetView& nv, uint32_t cnt, float t, unsigned long long n) {
+    __threadfence();
+    const uint32_t k = atomicAdd(nv.ticket, cnt);
+    if (k + cnt == nv.lif_tiles) {
+        nv.clock->t = t;
+        nv.clock->n = n;
+        *nv.ticket = 0u;
+        __threadfence();
+    }
+}
+
 template <int JM>
-__global__ void __launch_bounds__(kLifThreads, 2)
+__global__ void __launch_bounds__(kLifThreads, 3)
 lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_prefix,
            const uint32_t* __restrict__ vbase, uint32_t n_nets, uint32_t total_tiles, SpikeList sl, uint32_t flags,
            int prop_mode) {
+    extern __shared__ __align__(128) float lsm[];
+    __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ NetView s_nv;
-    __shared__ uint32_t s_base;
-    __shared__ uint32_t s_warp[kLifThreads / 32];
-    __shared__ unsigned long long s_events;
     __shared__ int s_cnt[kStatSlots];
     __shared__ long long s_vs[kStatSlots];
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
     uint32_t cur_net = 0xFFFFFFFFu;
     const bool use_ou = (flags & kFlagUseOU) != 0;
     const bool need_u = prop_mode != PROP_THRESHOLD;
     const bool injected = (flags & kFlagInjected) != 0;
+    uint32_t late = 0;                 // a bulk-copy wait ran out
+    uint32_t done_here = 0;            // tiles of cur_net this CTA finished (thread 0's ticket)
+    float t_last_tile = 0.f;
+    unsigned long long n_last_tile = 0;
+    if (tid < kStatSlots) { s_cnt[tid] = 0; s_vs[tid] = 0; }
+    if (tid == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        if (blockIdx.x < total_tiles) lif_prefetch(nets, tile_prefix, n_nets, blockIdx.x, lsm, &s_bar[0]);
+    }
+    __syncthreads();
 
-    for (uint32_t gt = blockIdx.x; gt < total_tiles; gt += gridDim.x) {
+    uint32_t it = 0;
+    for (uint32_t gt = blockIdx.x; gt < total_tiles; gt += gridDim.x, ++it) {
         const uint32_t net = n_nets > 1 ? find_net(tile_prefix, n_nets, gt) : 0u;
+        const uint32_t stg = it & 1u;
         if (net != cur_net) {
+            // hand in the previous network's tiles, then switch views
+            if (tid == 0 && done_here) lif_ticket(s_nv, done_here, t_last_tile, n_last_tile);
+            done_here = 0;
             __syncthreads();
             load_netview(s_nv, nets + net);
             cur_net = net;
         }
-        if (tid < kStatSlots) { s_cnt[tid] = 0; s_vs[tid] = 0; }
-        if (tid == 0) s_events = 0ull;
+        // barrier A: the other stage's readers (previous tile) are done and its
+        // store has been issued; refill it with the tile after this one
+        if (tid == 0 && gt + gridDim.x < total_tiles) {
+            bulk_wait_read();
+            lif_prefetch(nets, tile_prefix, n_nets, gt + gridDim.x, lsm + (stg ^ 1u) * kLifStageFloats, &s_bar[stg ^ 1u]);
+        }
         __syncthreads();
         const NetView& nv = s_nv;
         const uint32_t tile = gt - __ldg(tile_prefix + net);
         const uint32_t tile_first = tile * kLifTile;
         const uint32_t i0 = tile_first + tid * 4;
-
-        // ---- state loads first: 128-bit per array, 4 neurons per thread
-        float4 V4 = *reinterpret_cast<const float4*>(nv.V + i0);
-        float4 I4 = *reinterpret_cast<const float4*>(nv.iou + i0);
-        float4 T4 = *reinterpret_cast<const float4*>(nv.tlast + i0);
-        float4 J4[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) J4[k] = nv.J[i0 + k];
-        longlong2 D[8];
-        if constexpr (JM == J_FOLD) {
-            const longlong2* dsrc = reinterpret_cast<const longlong2*>(nv.dJ + static_cast<size_t>(i0) * 4);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) D[k] = dsrc[k];
-        }
         const float t_prev = nv.clock->t;
         const unsigned long long n_prev = nv.clock->n;
         const unsigned long long run_base = nv.clock->run_base;
@@ -256,10 +338,18 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
         StatAcc sa{s_cnt, s_vs, p_tile};
         float z[4], u[4] = {1.f, 1.f, 1.f, 1.f};
         draw_noise(nv, i0, n, inj_base, injected, need_u, z, u, err);
+        longlong2* dq = reinterpret_cast<longlong2*>(nv.dJ + static_cast<size_t>(i0) * 4);   // J_FOLD: this quad's sums
+        if (!mbar_wait_bounded(&s_bar[stg], (it >> 1) & 1u)) {
+            late = 1;
+            mbar_wait_bounded(&s_bar[stg], (it >> 1) & 1u);
+        }
+        if (late) err |= kErrTimeout;
+        float* st = lsm + stg * kLifStageFloats;
+        float* sV = st + tid * 4;
+        float* sI = st + kLifTile + tid * 4;
+        float* sT = st + 2 * kLifTile + tid * 4;
+        float4* sJ = reinterpret_cast<float4*>(st + 3 * kLifTile) + tid * 4;
 
-        float* Vv = reinterpret_cast<float*>(&V4);
-        float* Iv = reinterpret_cast<float*>(&I4);
-        float* Tv = reinterpret_cast<float*>(&T4);
         uint32_t nib_prop = 0, nib_act = 0;
         unsigned long long ev = 0;
         uint32_t p = p_tile;
@@ -269,41 +359,46 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
         bool uniform = true;
         int cnt_acc = 0;
         long long vs_acc = 0;
+        float v_out[4], i_out[4];
         PopParams pp;
         load_pop_params(nv, p, i_first, pp);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const uint32_t i = i0 + k;
-            if (i >= nv.n) { uniform = false; continue; }
+            if (i >= nv.n) { uniform = false; v_out[k] = 0.f; i_out[k] = 0.f; continue; }
             if (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) {
                 while (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) ++p;
                 uniform = false;
                 if (!nv.per_neuron) load_pop_params(nv, p, i, pp);
             }
             if (nv.per_neuron && k > 0) load_pop_params(nv, p, i, pp);
-            float* Jk = reinterpret_cast<float*>(&J4[k]);
+            const float4 Jk = sJ[k];
             NeuronIn in;
-            in.V = Vv[k];
-            in.iou = Iv[k];
-            in.tlast = Tv[k];
+            in.V = sV[k];
+            in.iou = sI[k];
+            in.tlast = sT[k];
             if constexpr (JM == J_FOLD) {
-                const long long* dk = reinterpret_cast<const long long*>(&D[2 * k]);
-#pragma unroll
-                for (int c = 0; c < 4; ++c) in.J[c] = decay_add(Jk[c], pp.decay[c], fix_to_float(dk[c]));
+                const longlong2 d01 = dq[2 * k], d23 = dq[2 * k + 1];
+                in.J[0] = decay_add(Jk.x, pp.decay[0], fix_to_float(d01.x));
+                in.J[1] = decay_add(Jk.y, pp.decay[1], fix_to_float(d01.y));
+                in.J[2] = decay_add(Jk.z, pp.decay[2], fix_to_float(d23.x));
+                in.J[3] = decay_add(Jk.w, pp.decay[3], fix_to_float(d23.y));
+                dq[2 * k] = make_longlong2(0, 0);
+                dq[2 * k + 1] = make_longlong2(0, 0);
             } else {
-#pragma unroll
-                for (int c = 0; c < 4; ++c) in.J[c] = Jk[c];
+                in.J[0] = Jk.x; in.J[1] = Jk.y; in.J[2] = Jk.z; in.J[3] = Jk.w;
             }
             const NeuronOut o = lif_update(pp, in, t, z[k], use_ou);
-            Vv[k] = o.V;
-            Iv[k] = o.iou;
-            Tv[k] = o.tlast;
+            sV[k] = o.V;
+            sI[k] = o.iou;
+            sT[k] = o.tlast;
+            v_out[k] = o.V;
+            i_out[k] = o.iou;
             if constexpr (JM == J_DIRECT) {
-#pragma unroll
-                for (int c = 0; c < 4; ++c) Jk[c] = __fmul_rn(in.J[c], pp.decay[c]);
+                sJ[k] = make_float4(__fmul_rn(in.J[0], pp.decay[0]), __fmul_rn(in.J[1], pp.decay[1]),
+                                    __fmul_rn(in.J[2], pp.decay[2]), __fmul_rn(in.J[3], pp.decay[3]));
             } else if constexpr (JM == J_FOLD) {
-#pragma unroll
-                for (int c = 0; c < 4; ++c) Jk[c] = in.J[c];
+                sJ[k] = make_float4(in.J[0], in.J[1], in.J[2], in.J[3]);
             }
             const bool sp = propagated(prop_mode, o.active, u[k], pp.noise_rate);
             nib_prop |= static_cast<uint32_t>(sp) << k;
@@ -318,20 +413,6 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
                     stat_add(nv, sa, row, p, o.active, v_fix(o.V));
                 }
             }
-        }
-
-        // ---- state stores
-        *reinterpret_cast<float4*>(nv.V + i0) = V4;
-        *reinterpret_cast<float4*>(nv.iou + i0) = I4;
-        *reinterpret_cast<float4*>(nv.tlast + i0) = T4;
-        if constexpr (JM != J_ASIS) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) nv.J[i0 + k] = J4[k];
-        }
-        if constexpr (JM == J_FOLD) {
-            longlong2* ddst = reinterpret_cast<longlong2*>(nv.dJ + static_cast<size_t>(i0) * 4);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) ddst[k] = make_longlong2(0, 0);
         }
 
         // ---- spike bitmaps (propagated: parity buffer; threshold: history row)
@@ -356,14 +437,13 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
                     if ((sb >> k) & 1u) {
                         const size_t o = static_cast<size_t>(row) * nv.n_samples + slot;
                         nv.hist_sspk[o] = static_cast<uint8_t>((nib_act >> k) & 1u);
-                        nv.hist_sv[o] = Vv[k];
-                        nv.hist_siou[o] = Iv[k];
+                        nv.hist_sv[o] = v_out[k];
+                        nv.hist_siou[o] = i_out[k];
                         ++slot;
                     }
                 }
             }
         }
-
         // ---- population statistics: warp-uniform fast path, else per-thread slots
         if (stats) {
             const uint32_t pl = __shfl_sync(0xffffffffu, p_first, 0);
@@ -376,33 +456,39 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
                 stat_add(nv, sa, row, p_first, cnt_acc, vs_acc);
             }
         }
-
-        // ---- spike list (push modes): CTA-aggregated, ascending within the tile
+        // ---- spike list (push modes): one slot range per warp, ascending within it
         const uint32_t my_cnt = __popc(nib_prop);
         uint32_t incl = my_cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
+            if (lane >= static_cast<uint32_t>(o)) incl += y;
         }
-        if (lane == 31) s_warp[warp] = incl;
+        const uint32_t wtotal = __shfl_sync(0xffffffffu, incl, 31);
+        if ((flags & kFlagList) && wtotal) {
+            uint32_t base = 0;
+            if (lane == 31) base = atomicAdd(sl.count, wtotal);
+            base = __shfl_sync(0xffffffffu, base, 31);
+            if (my_cnt) {
+                uint32_t pos = base + incl - my_cnt;
+                const uint32_t vb = __ldg(vbase + net);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if ((nib_prop >> k) & 1u) sl.list[pos++] = vb + i0 + k;
+            }
+        }
         const unsigned long long wev = warp_sum_ull(ev);
-        if (lane == 0 && wev) atomicAdd(&s_events, wev);
+        if (lane == 0 && wev) atomicAdd(nv.events, wev);
+
+        // barrier B: the stage holds the finished tile; store it, flush statistics
         __syncthreads();
         if (tid == 0) {
-            uint32_t total = 0;
-#pragma unroll
-            for (int w = 0; w < kLifThreads / 32; ++w) { const uint32_t c = s_warp[w]; s_warp[w] = total; total += c; }
-            s_base = ((flags & kFlagList) && total) ? atomicAdd(sl.count, total) : 0u;
-            if (s_events) atomicAdd(nv.events, s_events);
-        }
-        __syncthreads();
-        if ((flags & kFlagList) && my_cnt) {
-            uint32_t pos = s_base + s_warp[warp] + incl - my_cnt;
-            const uint32_t vb = __ldg(vbase + net);
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if ((nib_prop >> k) & 1u) sl.list[pos++] = vb + i0 + k;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            bulk_store(nv.V + tile_first, st, kLifTile * sizeof(float));
+            bulk_store(nv.iou + tile_first, st + kLifTile, kLifTile * sizeof(float));
+            bulk_store(nv.tlast + tile_first, st + 2 * kLifTile, kLifTile * sizeof(float));
+            if constexpr (JM != J_ASIS) bulk_store(nv.J + tile_first, st + 3 * kLifTile, kLifTile * sizeof(float4));
+            bulk_commit();
         }
         if (stats && tid < kStatSlots) {
             const int c = s_cnt[tid];
@@ -411,9 +497,22 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
                 const size_t o = static_cast<size_t>(row) * nv.n_pops + (p_tile + tid);
                 if (c) atomicAdd(nv.hist_cnt + o, c);
                 atomicAdd(reinterpret_cast<unsigned long long*>(nv.hist_vsum + o), static_cast<unsigned long long>(v));
+                s_cnt[tid] = 0;
+                s_vs[tid] = 0;
             }
         }
-        advance_clock(nv, nv.lif_tiles, t, n, err);
+        err = __reduce_or_sync(0xffffffffu, err);
+        if (lane == 0 && err) atomicOr(&nv.clock->err, err);
+        if (tid == 0) {
+            t_last_tile = t;
+            n_last_tile = n;
+            ++done_here;
+        }
+    }
+    // the CTA's last stores complete before its tiles count towards the clock
+    if (tid == 0) {
+        bulk_wait_all();
+        if (done_here) lif_ticket(s_nv, done_here, t_last_tile, n_last_tile);
     }
 }
 
@@ -828,34 +927,6 @@ __global__ void local_offsets_kernel(const unsigned long long* __restrict__ out_
 // Every mbarrier wait is bounded: on timeout the kernel raises an error bit,
 // waits (bounded) for its other copy in flight, and stops.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_addr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_addr(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    uint64_t g;
-    asm volatile("cvta.to.global.u64 %0, %1;" : "=l"(g) : "l"(src));
-    asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 :: "r"(smem_addr(dst)), "l"(g), "r"(bytes), "r"(smem_addr(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-                 : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
-    return ok != 0;
-}
-// Bounded wait on one mbarrier phase; false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (uint32_t it = 0; it < kWaitLimit; ++it)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
 template <int WT> struct WBytes { static constexpr int v = 4; };
 template <> struct WBytes<W_F32> { static constexpr int v = 8; };
 template <> struct WBytes<W_U8> { static constexpr int v = 2; };
@@ -1218,12 +1289,25 @@ gather_finish_kernel(const NetView* __restrict__ nets, const uint32_t* __restric
 // ---------------------------------------------------------------------------
 cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop_mode, cudaStream_t s) {
     if (b.lif_tiles_total == 0) return cudaSuccess;
+    // dynamic shared memory above 48 KiB needs an opt-in per kernel and device
+    static std::atomic<uint32_t> attr_set{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint32_t bit = 1u << (dev & 31);
+    if (!(attr_set.load() & bit)) {
+        for (auto fn : {lif_kernel<J_DIRECT>, lif_kernel<J_FOLD>, lif_kernel<J_ASIS>}) {
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kLifSmem));
+            if (e != cudaSuccess) return e;
+        }
+        attr_set.fetch_or(bit);
+    }
     const dim3 grid(std::min(b.lif_tiles_total, b.lif_ctas)), block(kLifThreads);
     const uint32_t T = b.lif_tiles_total;
     switch (jmode) {
-        case J_DIRECT: lif_kernel<J_DIRECT><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode); break;
-        case J_FOLD: lif_kernel<J_FOLD><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode); break;
-        default: lif_kernel<J_ASIS><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode); break;
+        case J_DIRECT: lif_kernel<J_DIRECT><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode); break;
+        case J_FOLD: lif_kernel<J_FOLD><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode); break;
+        default: lif_kernel<J_ASIS><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode); break;
     }
     return cudaGetLastError();
 }
