@@ -134,12 +134,19 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
     const bool record = (rq.flags & DTB_RUN_RECORD_SPIKES) != 0;
     const int exact = rq.syn_mode == DTB_SYN_PUSH_EXACT ? 1 : 0;
     const bool samples = (rq.flags & (DTB_RUN_SAMPLE_SPIKE | DTB_RUN_SAMPLE_V | DTB_RUN_SAMPLE_IOU)) != 0;
+    const bool imean = (rq.flags & DTB_RUN_IMEAN) != 0, rimean = (rq.flags & DTB_RUN_RECEPTOR_IMEAN) != 0;
+    const bool sisyn = (rq.flags & DTB_RUN_SAMPLE_ISYN) != 0;
+    if ((imean || rimean || sisyn) && rq.syn_mode == DTB_SYN_PULL)
+        return fail(DTB_UNSUPPORTED, "synaptic-current outputs need a push mode (the pull kernel completes J one step later)");
+    const bool isyn_any = imean || rimean || sisyn;
     bool injected = false;
     for (size_t i = 0; i < m.size(); ++i) {
         Engine& e = *m[i];
         if (rq.syn_mode != DTB_SYN_PULL && !e.has_push) return fail(DTB_UNSUPPORTED, "a member has no out-degree CSR");
         if (rq.syn_mode == DTB_SYN_PULL && !e.has_pull) return fail(DTB_UNSUPPORTED, "a member has no in-degree CSR");
-        if ((freq && !outs[i].freqs) || (vmean && !outs[i].vmeans) || (record && !outs[i].spike_bits))
+        if ((freq && !outs[i].freqs) || (vmean && !outs[i].vmeans) || (record && !outs[i].spike_bits) ||
+            (imean && !outs[i].imeans) || (rimean && !outs[i].receptor_imeans) ||
+            (sisyn && !e.sample_order.empty() && !outs[i].sample_isyn))
             return fail(DTB_INVALID_PARAMETER, "requested output buffer is NULL");
         const bool inj = e.noise_src == DTB_NOISE_INJECTED;
         if (i > 0 && inj != injected) return fail(DTB_UNSUPPORTED, "batch members must share the noise source");
@@ -157,6 +164,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
     for (Engine* e : m) {
         if (exact) DTB_TRY(e->ensure_dj());
         DTB_TRY(e->ensure_hist(cap, record, samples));
+        if (isyn_any) DTB_TRY(e->ensure_isum(cap, sisyn));
     }
     DTB_TRY(refresh_views());
     uint32_t kflags = 0;
@@ -166,6 +174,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
     if (rq.syn_mode != DTB_SYN_PULL) kflags |= kFlagList;
     if (injected) kflags |= kFlagInjected;
     if (samples) kflags |= kFlagSample;
+    if (isyn_any) kflags |= kFlagIsyn;
     const int pm = static_cast<int>(rq.prop_mode);
     const int wt = static_cast<int>(wtype);
     uint64_t tune_at = ~0ull;
@@ -190,6 +199,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
                 DTB_CU(cudaMemsetAsync(e->hist_cnt, 0, sizeof(int) * rows * e->P, stream));
                 DTB_CU(cudaMemsetAsync(e->hist_vsum, 0, sizeof(long long) * rows * e->P, stream));
             }
+            if (isyn_any) DTB_CU(cudaMemsetAsync(e->hist_isum, 0, sizeof(long long) * rows * e->P * 5, stream));
             ++launches;
         }
         DTB_CU(cudaEventRecord(ev0, stream));
@@ -208,6 +218,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
                 for (uint32_t s = 0; s < rows && ce == cudaSuccess; ++s) {
                     ce = launch_lif(lb, J_DIRECT, kflags, pm, stream);
                     if (ce == cudaSuccess) ce = launch_push(lb, 0, wt, push_cfg, push_ctas, stream);
+                    if (ce == cudaSuccess && isyn_any) ce = launch_stat_isyn(lb, 0, sm_count, stream);
                 }
                 const cudaError_t ee = cudaStreamEndCapture(stream, &g);
                 if (ce != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(ce, "graph capture"); }
@@ -219,7 +230,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
             }
             DTB_CU(cudaGraphLaunch(graph, stream));
             ++graph_launches;
-            launches += (2 + push_extra_launches(lb, 0, push_cfg)) * rows;
+            launches += (2 + push_extra_launches(lb, 0, push_cfg) + (isyn_any ? 1u : 0u)) * rows;
         } else {
             for (uint32_t s = 0; s < rows; ++s) {
                 const bool first = (done + s) == 0;
@@ -243,6 +254,10 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
                 }
                 DTB_CU(launch_push(lb, exact, wt, push_cfg, push_ctas, stream));
                 launches += 2 + push_extra_launches(lb, exact, push_cfg);
+                if (isyn_any) {
+                    DTB_CU(launch_stat_isyn(lb, exact, sm_count, stream));
+                    ++launches;
+                }
             }
         }
         if (done + rows == rq.iters) {
@@ -263,6 +278,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
             e.steps += rows;
             DTB_TRY(e.finish_hist(rows, done, outs[i], freq, vmean, record));
             if (samples && !e.sample_order.empty()) DTB_TRY(e.finish_samples(rows, done, outs[i]));
+            if (isyn_any) DTB_TRY(e.finish_isum(rows, done, outs[i], imean, rimean, sisyn && !e.sample_order.empty()));
         }
         done += rows;
     }

@@ -56,6 +56,7 @@ constexpr uint32_t kFlagRecord = 4u;
 constexpr uint32_t kFlagList = 8u;       // write the spike list for the push kernel
 constexpr uint32_t kFlagInjected = 16u;
 constexpr uint32_t kFlagSample = 32u;     // record the sampled neurons
+constexpr uint32_t kFlagIsyn = 64u;       // synaptic-current statistics after the push (host-side marker)
 
 // Derived per-population constants (host computes them once per property change).
 struct __align__(16) PopParams {
@@ -110,6 +111,8 @@ struct NetView {
     unsigned long long inj_rows;
     int* hist_cnt;                 // [hist_cap * n_pops]
     long long* hist_vsum;          // [hist_cap * n_pops] fixed point, scale 2^24
+    long long* hist_isum;          // [isum_cap * n_pops * 5] I_syn, I_AMPA, I_NMDA, I_GABAa, I_GABAb sums, scale 2^24
+    uint32_t isum_cap;
     unsigned long long* events;    // cumulative synaptic events
     uint32_t* ticket;              // last-tile counter of the per-step kernels
     const uint32_t* tile_pop;      // [lif_tiles] population of each LIF tile's first neuron
@@ -120,6 +123,7 @@ struct NetView {
     uint8_t* hist_sspk;            // [hist_cap * n_samples] spike of each sampled neuron
     float* hist_sv;                // [hist_cap * n_samples] V after the step
     float* hist_siou;              // [hist_cap * n_samples] OU current after the step
+    float* hist_sisyn;             // [isum_cap * n_samples] I_syn at the end of the step
     // Population-local push (rows sorted by postsynaptic neuron).  A population
     // with local windows is cut into pop_loc[a].x windows of pop_loc[a].y neurons;
     // row j keeps, for each boundary k of its own population's windows, the offset

@@ -49,6 +49,7 @@ Engine::~Engine() {
     for (void* p : allocs) cudaFree(p);
     if (h_cnt) cudaFreeHost(h_cnt);
     if (h_vsum) cudaFreeHost(h_vsum);
+    if (h_isum) cudaFreeHost(h_isum);
     for (cudaEvent_t e : tev) cudaEventDestroy(e);
     if (tune_ev[0]) cudaEventDestroy(tune_ev[0]);
     if (tune_ev[1]) cudaEventDestroy(tune_ev[1]);
@@ -195,6 +196,8 @@ int Engine::refresh_view() {
     v.inj_rows = inj_rows;
     v.hist_cnt = hist_cnt;
     v.hist_vsum = hist_vsum;
+    v.hist_isum = hist_isum;
+    v.isum_cap = isum_cap;
     v.events = events;
     v.ticket = ticket;
     v.lif_tiles = n_pad / kLifTile;
@@ -205,6 +208,7 @@ int Engine::refresh_view() {
     v.hist_sspk = hist_sspk;
     v.hist_sv = hist_sv;
     v.hist_siou = hist_siou;
+    v.hist_sisyn = hist_sisyn;
     v.own_seg = own_seg;
     v.woff = woff;
     v.pop_loc = pop_loc;
@@ -666,6 +670,62 @@ int Engine::ensure_hist(uint32_t rows, bool record, bool samples) {
     return DTB_OK;
 }
 
+// Device and pinned host buffers of the synaptic-current sums.
+int Engine::ensure_isum(uint32_t rows, bool sample) {
+    bool changed = false;
+    if (rows > isum_cap) {
+        dfree(hist_isum);
+        hist_isum = nullptr;
+        DTB_TRY(dalloc(hist_isum, static_cast<size_t>(rows) * P * 5));
+        if (h_isum) cudaFreeHost(h_isum);
+        h_isum = nullptr;
+        DTB_CU(cudaMallocHost(&h_isum, sizeof(long long) * rows * P * 5));
+        isum_cap = rows;
+        changed = true;
+    }
+    if (sample && n_samples && sisyn_cap < isum_cap) {
+        dfree(hist_sisyn);
+        hist_sisyn = nullptr;
+        DTB_TRY(dalloc(hist_sisyn, static_cast<size_t>(isum_cap) * n_samples));
+        sisyn_cap = isum_cap;
+        changed = true;
+    }
+    return changed ? refresh_view() : DTB_OK;
+}
+
+// Means of the chunk's synaptic-current sums into the caller's buffers.
+int Engine::finish_isum(uint32_t rows, uint32_t out_row0, const dtb_run_output& out, bool imean, bool receptor,
+                        bool sample) {
+    std::vector<float> si;
+    if (sample && n_samples) {
+        si.resize(static_cast<size_t>(rows) * n_samples);
+        DTB_CU(cudaMemcpyAsync(si.data(), hist_sisyn, si.size() * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    }
+    if (imean || receptor)
+        DTB_CU(cudaMemcpyAsync(h_isum, hist_isum, sizeof(long long) * rows * P * 5, cudaMemcpyDeviceToHost, stream));
+    DTB_CU(cudaStreamSynchronize(stream));
+    if (!si.empty()) {
+        const size_t K = sample_order.size();
+        for (uint32_t r = 0; r < rows; ++r)
+            for (size_t k = 0; k < K; ++k)
+                out.sample_isyn[static_cast<size_t>(out_row0 + r) * K + k] = si[static_cast<size_t>(r) * n_samples + sample_order[k]];
+    }
+    for (uint32_t r = 0; r < rows && (imean || receptor); ++r) {
+        for (uint32_t p = 0; p < P; ++p) {
+            const uint32_t cnt = pop_off[p + 1] - pop_off[p] - excl_count[p];
+            const long long* q = h_isum + (static_cast<size_t>(r) * P + p) * 5;
+            auto mean = [&](long long v) {
+                return cnt ? static_cast<float>(static_cast<double>(v) / kVsumScale / static_cast<double>(cnt)) : 0.0f;
+            };
+            const size_t row = static_cast<size_t>(out_row0 + r);
+            if (imean) out.imeans[row * P + p] = mean(q[0]);
+            if (receptor)
+                for (int c = 0; c < 4; ++c) out.receptor_imeans[(row * 4 + c) * P + p] = mean(q[1 + c]);
+        }
+    }
+    return DTB_OK;
+}
+
 int Engine::begin_run_chunk(uint64_t run_base, uint32_t rows, bool stats) {
     set_u64_kernel<<<1, 1, 0, stream>>>(&clock->run_base, run_base);
     DTB_CU(cudaGetLastError());
@@ -734,13 +794,21 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     if ((freq && !out.freqs) || (vmean && !out.vmeans) || (record && !out.spike_bits))
         return fail(DTB_INVALID_PARAMETER, "requested output buffer is NULL");
     const bool samples = (rq.flags & (DTB_RUN_SAMPLE_SPIKE | DTB_RUN_SAMPLE_V | DTB_RUN_SAMPLE_IOU)) != 0;
-    if (samples && sample_order.empty())
+    const bool sisyn = (rq.flags & DTB_RUN_SAMPLE_ISYN) != 0;
+    if ((samples || sisyn) && sample_order.empty())
         return fail(DTB_UNSET_SAMPLE_FAILURE, "sample outputs requested but no samples are set");
+    if (sisyn && !out.sample_isyn) return fail(DTB_INVALID_PARAMETER, "requested sample buffer is NULL");
     if (((rq.flags & DTB_RUN_SAMPLE_SPIKE) && !out.sample_spike) || ((rq.flags & DTB_RUN_SAMPLE_V) && !out.sample_v) ||
         ((rq.flags & DTB_RUN_SAMPLE_IOU) && !out.sample_iou))
         return fail(DTB_INVALID_PARAMETER, "requested sample buffer is NULL");
     if ((rq.flags & DTB_RUN_SAMPLE_IOU) && !(rq.flags & DTB_RUN_USE_OU))
         return fail(DTB_INVALID_PARAMETER, "sample_iou needs use_ou_background");
+    const bool imean = (rq.flags & DTB_RUN_IMEAN) != 0, rimean = (rq.flags & DTB_RUN_RECEPTOR_IMEAN) != 0;
+    if ((imean && !out.imeans) || (rimean && !out.receptor_imeans))
+        return fail(DTB_INVALID_PARAMETER, "requested imean buffer is NULL");
+    if ((imean || rimean || sisyn) && rq.syn_mode == DTB_SYN_PULL)
+        return fail(DTB_UNSUPPORTED, "synaptic-current outputs need a push mode (the pull kernel completes J one step later)");
+    const bool isyn_any = imean || rimean || sisyn;
     const bool injected = noise_src == DTB_NOISE_INJECTED;
     if (injected) {
         const uint64_t used = steps - inj_first;
@@ -751,6 +819,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     uint32_t cap = std::min<uint32_t>(rq.iters, 4096u);
     if (record) cap = std::min<uint32_t>(cap, std::max<uint32_t>(1u, static_cast<uint32_t>((512ull << 20) / (4ull * n_words))));
     DTB_TRY(ensure_hist(cap, record, samples));
+    if (isyn_any) DTB_TRY(ensure_isum(cap, sisyn));
     uint32_t kflags = 0;
     if (samples) kflags |= kFlagSample;
     if (rq.flags & DTB_RUN_USE_OU) kflags |= kFlagUseOU;
@@ -780,9 +849,10 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     while (done < rq.iters) {
         const uint32_t rows = std::min(cap, rq.iters - done);
         DTB_TRY(begin_run_chunk(steps, rows, freq || vmean));
+        if (isyn_any) DTB_CU(cudaMemsetAsync(hist_isum, 0, sizeof(long long) * rows * P * 5, stream));
         ++launches;
         std::vector<std::pair<int, size_t>> timed;   // (kernel class, event pair index)
-        if (time_k) DTB_TRY(ensure_timing_events(4 * static_cast<size_t>(rows) + 4));   // 2 events x (2 launches per step + 1)
+        if (time_k) DTB_TRY(ensure_timing_events(6 * static_cast<size_t>(rows) + 4));   // 2 events x (3 launches per step + 1)
         auto timed_launch = [&](int cls, auto&& fn) -> int {
             if (time_k) DTB_CU(cudaEventRecord(tev[2 * timed.size()], stream));
             DTB_CU(fn());
@@ -805,6 +875,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
                     }
                     DTB_TRY(timed_launch(1, [&] { return launch_push(b, 0, static_cast<int>(wtype), push_cfg, push_ctas, stream); }));
                     launches += push_extra_launches(b, 0, push_cfg);
+                    if (isyn_any) DTB_TRY(timed_launch(3, [&] { return launch_stat_isyn(b, 0, sm_count, stream); }));
                     break;
                 case DTB_SYN_PUSH_EXACT:
                     DTB_TRY(timed_launch(0, [&] { return launch_lif(b, first ? J_ASIS : J_FOLD, kflags, pm, stream); }));
@@ -813,6 +884,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
                         if (!push_tuned[1]) tune_at += 50;
                     }
                     DTB_TRY(timed_launch(1, [&] { return launch_push(b, 1, static_cast<int>(wtype), push_cfg, push_ctas, stream); }));
+                    if (isyn_any) DTB_TRY(timed_launch(3, [&] { return launch_stat_isyn(b, 1, sm_count, stream); }));
                     break;
                 default:
                     DTB_TRY(timed_launch(2, [&] { return launch_pull(b, first ? 0 : 1, static_cast<int>(wtype), kflags, pm, stream); }));
@@ -842,6 +914,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
         steps += rows;
         DTB_TRY(finish_hist(rows, done, out, freq, vmean, record));
         if (samples) DTB_TRY(finish_samples(rows, done, out));
+        if (isyn_any) DTB_TRY(finish_isum(rows, done, out, imean, rimean, sisyn));
         done += rows;
     }
     for (int k = 0; k < 4; ++k) out.kernel_ms[k] = kms[k];
@@ -1125,9 +1198,11 @@ int Engine::set_samples(uint32_t count, const uint32_t* idx) {
         dfree(hist_sspk);
         dfree(hist_sv);
         dfree(hist_siou);
+        dfree(hist_sisyn);
         hist_sspk = nullptr;
-        hist_sv = hist_siou = nullptr;
+        hist_sv = hist_siou = hist_sisyn = nullptr;
         sample_cap = 0;
+        sisyn_cap = 0;
     }
     n_samples = total;
     return refresh_view();

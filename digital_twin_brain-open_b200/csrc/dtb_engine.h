@@ -68,6 +68,8 @@ public:
     int begin_run_chunk(uint64_t run_base, uint32_t rows, bool stats);
     int finish_hist(uint32_t rows, uint32_t out_row0, const dtb_run_output& out, bool freq, bool vmean, bool record);
     int finish_samples(uint32_t rows, uint32_t out_row0, const dtb_run_output& out);
+    int ensure_isum(uint32_t rows, bool sample);
+    int finish_isum(uint32_t rows, uint32_t out_row0, const dtb_run_output& out, bool imean, bool receptor, bool sample);
 
     // identity
     int device = 0;
@@ -121,6 +123,9 @@ public:
     uint32_t* ticket = nullptr;
     int* hist_cnt = nullptr;
     long long* hist_vsum = nullptr;
+    long long* hist_isum = nullptr;      // [isum_cap * P * 5] synaptic-current sums (imean outputs)
+    uint32_t isum_cap = 0;
+    long long* h_isum = nullptr;
     uint32_t* rec_bits = nullptr;
     uint32_t hist_cap = 0, rec_cap = 0;
     uint32_t n_samples = 0, sample_cap = 0;
@@ -129,6 +134,8 @@ public:
     uint8_t* hist_sspk = nullptr;
     float* hist_sv = nullptr;
     float* hist_siou = nullptr;
+    float* hist_sisyn = nullptr;         // [isum_cap * sample_cap slots] sampled end-of-step I_syn
+    uint32_t sisyn_cap = 0;
     std::vector<uint32_t> sample_order;   // sample slot -> position in the caller's list
     float* inj_z = nullptr;
     float* inj_u = nullptr;

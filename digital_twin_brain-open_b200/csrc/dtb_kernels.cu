@@ -1285,6 +1285,109 @@ gather_finish_kernel(const NetView* __restrict__ nets, const uint32_t* __restric
 }
 
 // ---------------------------------------------------------------------------
+// End-of-step synaptic currents per population: output_imean and
+// output_receptor_imeas (stat_result.cpp:269-380; block_new.py:152-156, the
+// mean_psc of every population).  Runs after the step's push, when J is
+// complete: I_u = g_u (V_u - V) J_u and I_syn = ((I_0 + I_1) + I_2) + I_3 in
+// the LIF step's operation order, V after the step.  Sums are fixed point
+// (2^24, like the V sums) so batches and reruns agree bit for bit; neurons
+// excluded from statistics are skipped.
+// ---------------------------------------------------------------------------
+template <int JM>
+__global__ void __launch_bounds__(256)
+stat_isyn_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_prefix, uint32_t n_nets,
+                 uint32_t total_tiles) {
+    __shared__ unsigned long long s_is[kStatSlots][5];
+    const uint32_t tid = threadIdx.x, lane = tid & 31u;
+    for (uint32_t gt = blockIdx.x; gt < total_tiles; gt += gridDim.x) {
+        const uint32_t net = n_nets > 1 ? find_net(tile_prefix, n_nets, gt) : 0u;
+        const NetView& nv = nets[net];
+        const long long row = static_cast<long long>(nv.clock->n - nv.clock->run_base) - 1;
+        if (nv.hist_isum == nullptr || row < 0 || row >= static_cast<long long>(nv.isum_cap)) continue;
+        const bool sampled = nv.hist_sisyn != nullptr && nv.n_samples != 0;
+        for (uint32_t q = tid; q < kStatSlots * 5; q += blockDim.x) (&s_is[0][0])[q] = 0ull;
+        __syncthreads();
+        const uint32_t tile = gt - __ldg(tile_prefix + net);
+        const uint32_t p_tile = __ldg(nv.tile_pop + tile);
+        const uint32_t i0 = tile * kLifTile + tid * 4;
+        uint32_t p = p_tile;
+        const uint32_t i_first = min(i0, nv.n - 1);
+        while (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i_first) ++p;
+        const uint32_t p_first = p;
+        PopParams pp;
+        load_pop_params(nv, p, i_first, pp);
+        long long acc[5] = {0, 0, 0, 0, 0};
+        bool uniform = true;
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t i = i0 + k;
+            if (i >= nv.n) { uniform = false; continue; }
+            if (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) {
+                while (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) ++p;
+                if (!nv.per_neuron) load_pop_params(nv, p, i, pp);
+            }
+            if (nv.per_neuron && k > 0) load_pop_params(nv, p, i, pp);
+            if (excluded(nv, i)) { uniform = false; continue; }
+            const float V = nv.V[i];
+            const float4 Jv = nv.J[i];
+            float J[4] = {Jv.x, Jv.y, Jv.z, Jv.w};
+            if constexpr (JM == J_FOLD) {
+                const long long* d = nv.dJ + static_cast<size_t>(i) * 4;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) J[c] = decay_add(J[c], pp.decay[c], fix_to_float(d[c]));
+            }
+            float I[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) I[c] = __fmul_rn(__fmul_rn(pp.g[c], __fsub_rn(pp.Vu[c], V)), J[c]);
+            const float isyn = __fadd_rn(__fadd_rn(__fadd_rn(I[0], I[1]), I[2]), I[3]);
+            if (sampled) {
+                const uint32_t sw = __ldg(nv.sample_bits + (i >> 5)), sb = 1u << (i & 31);
+                if (sw & sb)
+                    nv.hist_sisyn[static_cast<size_t>(row) * nv.n_samples + __ldg(nv.sample_pre + (i >> 5)) + __popc(sw & (sb - 1u))] = isyn;
+            }
+            long long q[5] = {v_fix(isyn), v_fix(I[0]), v_fix(I[1]), v_fix(I[2]), v_fix(I[3])};
+            if (p == p_first) {
+#pragma unroll
+                for (int c = 0; c < 5; ++c) acc[c] += q[c];
+            } else {
+                uniform = false;
+                const uint32_t slot = p - p_tile;
+#pragma unroll
+                for (int c = 0; c < 5; ++c) {
+                    if (slot < static_cast<uint32_t>(kStatSlots)) atomicAdd(&s_is[slot][c], static_cast<unsigned long long>(q[c]));
+                    else atomicAdd(reinterpret_cast<unsigned long long*>(nv.hist_isum) + (static_cast<size_t>(row) * nv.n_pops + p) * 5 + c,
+                                   static_cast<unsigned long long>(q[c]));
+                }
+            }
+        }
+        const uint32_t pl = __shfl_sync(0xffffffffu, p_first, 0);
+        const bool wuni = __all_sync(0xffffffffu, uniform && p_first == pl);
+        if (wuni) {
+#pragma unroll
+            for (int c = 0; c < 5; ++c) acc[c] = warp_sum_ll(acc[c]);
+        }
+        if ((wuni && lane == 0) || (!wuni && i0 < nv.n)) {
+            const uint32_t slot = (wuni ? pl : p_first) - p_tile;
+            const uint32_t pp_ = wuni ? pl : p_first;
+#pragma unroll
+            for (int c = 0; c < 5; ++c) {
+                if (!acc[c]) continue;
+                if (slot < static_cast<uint32_t>(kStatSlots)) atomicAdd(&s_is[slot][c], static_cast<unsigned long long>(acc[c]));
+                else atomicAdd(reinterpret_cast<unsigned long long*>(nv.hist_isum) + (static_cast<size_t>(row) * nv.n_pops + pp_) * 5 + c,
+                               static_cast<unsigned long long>(acc[c]));
+            }
+        }
+        __syncthreads();
+        for (uint32_t q = tid; q < kStatSlots * 5; q += blockDim.x) {
+            const uint32_t slot = q / 5, c = q % 5;
+            const unsigned long long v = s_is[slot][c];
+            if (v && p_tile + slot < nv.n_pops)
+                atomicAdd(reinterpret_cast<unsigned long long*>(nv.hist_isum) + (static_cast<size_t>(row) * nv.n_pops + p_tile + slot) * 5 + c, v);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Host-side launchers
 // ---------------------------------------------------------------------------
 cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop_mode, cudaStream_t s) {
@@ -1455,6 +1558,14 @@ static void pull_dispatch(const LaunchBatch& b, int wt, uint32_t flags, int prop
 cudaError_t launch_pull(const LaunchBatch& b, int gather, int wt, uint32_t flags, int prop_mode, cudaStream_t s) {
     if (b.pull_tiles_total == 0) return cudaSuccess;
     if (gather) pull_dispatch<1>(b, wt, flags, prop_mode, s); else pull_dispatch<0>(b, wt, flags, prop_mode, s);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stat_isyn(const LaunchBatch& b, int exact, int sm_count, cudaStream_t s) {
+    if (b.lif_tiles_total == 0) return cudaSuccess;
+    const dim3 grid(std::min<uint32_t>(b.lif_tiles_total, static_cast<uint32_t>(sm_count) * 8u)), block(256);
+    if (exact) stat_isyn_kernel<J_FOLD><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.n_nets, b.lif_tiles_total);
+    else stat_isyn_kernel<J_DIRECT><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.n_nets, b.lif_tiles_total);
     return cudaGetLastError();
 }
 

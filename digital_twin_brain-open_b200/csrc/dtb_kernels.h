@@ -51,6 +51,9 @@ inline uint32_t push_extra_launches(const LaunchBatch& b, int exact, const PushC
 }
 cudaError_t launch_pull(const LaunchBatch& b, int gather, int weight_type, uint32_t flags, int prop_mode, cudaStream_t s);
 cudaError_t launch_fold_finish(const LaunchBatch& b, cudaStream_t s);
+// Per-population sums of the end-of-step synaptic currents (after the push of
+// the step; exact = J still holds its folded form plus dJ).
+cudaError_t launch_stat_isyn(const LaunchBatch& b, int exact, int sm_count, cudaStream_t s);
 cudaError_t launch_gather_finish(const LaunchBatch& b, int weight_type, cudaStream_t s);
 
 // Population-local push tables (rows must be sorted by postsynaptic neuron;

@@ -27,6 +27,7 @@ PUSH_REG, PUSH_TMA, PUSH_LOCAL = 0, 1, 2
 NOISE_PHILOX, NOISE_INJECTED = 0, 1
 RUN_USE_OU, RUN_FREQ, RUN_VMEAN, RUN_RECORD_SPIKES, RUN_TIME_KERNELS = 1, 2, 4, 8, 16
 RUN_SAMPLE_SPIKE, RUN_SAMPLE_V, RUN_SAMPLE_IOU = 32, 64, 128
+RUN_IMEAN, RUN_RECEPTOR_IMEAN, RUN_SAMPLE_ISYN = 256, 512, 1024
 STATE_V, STATE_J, STATE_I_OU, STATE_T_LAST = 0, 1, 2, 3
 
 # snn.proto PropType
@@ -79,7 +80,8 @@ class RunOutput(C.Structure):
     _fields_ = [("freqs", C.c_void_p), ("vmeans", C.c_void_p), ("spike_bits", C.c_void_p),
                 ("events", C.c_uint64), ("device_ms", C.c_double), ("kernel_ms", C.c_double * 4),
                 ("launches", C.c_uint32), ("reserved", C.c_uint32), ("sample_spike", C.c_void_p),
-                ("sample_v", C.c_void_p), ("sample_iou", C.c_void_p)]
+                ("sample_v", C.c_void_p), ("sample_iou", C.c_void_p), ("imeans", C.c_void_p),
+                ("receptor_imeans", C.c_void_p), ("sample_isyn", C.c_void_p)]
 
 
 _P = C.c_void_p
@@ -236,6 +238,9 @@ class RunResult:
     sample_spike: np.ndarray | None = None   # uint8 [iters, n_samples]
     sample_v: np.ndarray | None = None
     sample_iou: np.ndarray | None = None
+    imeans: np.ndarray | None = None             # float [iters, P] mean I_syn at the end of each step
+    receptor_imeans: np.ndarray | None = None    # float [iters, 4, P] mean I_AMPA, I_NMDA, I_GABAa, I_GABAb
+    sample_isyn: np.ndarray | None = None        # float [iters, n_samples] end-of-step I_syn
 
 
 class Engine:
@@ -371,7 +376,8 @@ class Engine:
     # ---- stepping
     def run(self, iters, use_ou=True, freq=True, vmean=False, record_spikes=False,
             prop_mode=PROP_THRESHOLD, syn_mode=SYN_PUSH, time_kernels=False, out=None,
-            sample_spike=False, sample_v=False, sample_iou=False):
+            sample_spike=False, sample_v=False, sample_iou=False, imean=False, receptor_imean=False,
+            sample_isyn=False):
         """Advance ``iters`` steps (RunRequest, snn.proto:63-77).
 
         ``out`` may pass preallocated (freqs, vmeans) host arrays of shape [iters, P].
@@ -379,11 +385,16 @@ class Engine:
         flags = (RUN_USE_OU if use_ou else 0) | (RUN_FREQ if freq else 0) | \
                 (RUN_VMEAN if vmean else 0) | (RUN_RECORD_SPIKES if record_spikes else 0) | \
                 (RUN_TIME_KERNELS if time_kernels else 0) | (RUN_SAMPLE_SPIKE if sample_spike else 0) | \
-                (RUN_SAMPLE_V if sample_v else 0) | (RUN_SAMPLE_IOU if sample_iou else 0)
+                (RUN_SAMPLE_V if sample_v else 0) | (RUN_SAMPLE_IOU if sample_iou else 0) | \
+                (RUN_IMEAN if imean else 0) | (RUN_RECEPTOR_IMEAN if receptor_imean else 0) | \
+                (RUN_SAMPLE_ISYN if sample_isyn else 0)
+        im = np.zeros((iters, self.n_pops), np.float32) if imean else None
+        rim = np.zeros((iters, 4, self.n_pops), np.float32) if receptor_imean else None
         ns = getattr(self, "n_sample_list", 0)
         ss = np.zeros((iters, ns), np.uint8) if sample_spike else None
         sv = np.zeros((iters, ns), np.float32) if sample_v else None
         si = np.zeros((iters, ns), np.float32) if sample_iou else None
+        sy = np.zeros((iters, ns), np.float32) if sample_isyn else None
         rq = RunRequest(iters, flags, prop_mode, syn_mode)
         if out is not None:
             fr, vm = out
@@ -397,12 +408,15 @@ class Engine:
         res.sample_spike = None if ss is None else ss.ctypes.data
         res.sample_v = None if sv is None else sv.ctypes.data
         res.sample_iou = None if si is None else si.ctypes.data
+        res.imeans = None if im is None else im.ctypes.data
+        res.receptor_imeans = None if rim is None else rim.ctypes.data
+        res.sample_isyn = None if sy is None else sy.ctypes.data
         _check(LIB.dtb_run(self._h, C.byref(rq), C.byref(res)))
         spikes = None
         if sb is not None:
             spikes = np.unpackbits(sb.view(np.uint8), axis=1, bitorder="little")[:, :self.n].astype(bool)
         return RunResult(fr, vm, spikes, int(res.events), float(res.device_ms), tuple(res.kernel_ms), int(res.launches),
-                         ss, sv, si)
+                         ss, sv, si, im, rim, sy)
 
     # ---- state
     def read_state(self, which):

@@ -166,9 +166,11 @@ class SnnService(pbg.SnnServicer):
             status = pb.SNN_INVALID_PARAMETER
         elif request.t_steps > 1 and not request.use_ou_background:
             status = pb.SNN_INVALID_PARAMETER
-        elif (request.t_steps > 1 or request.output_imean or request.output_receptor_imeas
-              or request.output_sample_isynaptic):
+        elif request.t_steps > 1:
             status = pb.SNN_UNSUPPORTED
+        elif ((request.output_imean or request.output_receptor_imeas or request.output_sample_isynaptic)
+              and self.syn_mode == E.SYN_PULL):
+            status = pb.SNN_UNSUPPORTED     # the pull kernel completes J one step later
         if status != pb.SNN_OK:
             yield pb.RunResponse(status=status)
             return
@@ -180,7 +182,9 @@ class SnnService(pbg.SnnServicer):
                 r = self.eng.run(it, use_ou=request.use_ou_background, freq=request.output_freq,
                                  vmean=request.output_vmean, syn_mode=self.syn_mode,
                                  sample_spike=request.output_sample_spike, sample_v=request.output_sample_vmemb,
-                                 sample_iou=request.output_sample_iou)
+                                 sample_iou=request.output_sample_iou, imean=request.output_imean,
+                                 receptor_imean=request.output_receptor_imeas,
+                                 sample_isyn=request.output_sample_isynaptic)
                 for k in range(it):
                     resp = pb.RunResponse(status=pb.SNN_OK)
                     if request.output_freq:
@@ -199,6 +203,16 @@ class SnnService(pbg.SnnServicer):
                         resp.sample_vmemb.append(r.sample_v[k].tobytes())
                     if request.output_sample_iou:
                         resp.sample_iou.append(r.sample_iou[k].tobytes())
+                    if request.output_sample_isynaptic:
+                        resp.sample_isynaptic.append(r.sample_isyn[k].tobytes())
+                    if request.output_imean:
+                        resp.imean.append(r.imeans[k].astype(np.float32).tobytes())
+                    if request.output_receptor_imeas:
+                        ri = r.receptor_imeans[k]
+                        resp.ampa_imean.append(ri[0].tobytes())
+                        resp.nmda_imean.append(ri[1].tobytes())
+                        resp.gabaa_imean.append(ri[2].tobytes())
+                        resp.gabab_imean.append(ri[3].tobytes())
                     yield resp
                 done += it
             self.iterations += request.iter

@@ -154,6 +154,9 @@ typedef struct dtb_engine_info {
 #define DTB_RUN_SAMPLE_SPIKE  (1u << 5)  /* output_sample_spike: spikes of the sampled neurons */
 #define DTB_RUN_SAMPLE_V      (1u << 6)  /* output_sample_vmemb                                 */
 #define DTB_RUN_SAMPLE_IOU    (1u << 7)  /* output_sample_iou (needs DTB_RUN_USE_OU)            */
+#define DTB_RUN_IMEAN         (1u << 8)  /* output_imean: per-population mean I_syn (push modes) */
+#define DTB_RUN_RECEPTOR_IMEAN (1u << 9) /* output_receptor_imeas: mean I_u per receptor        */
+#define DTB_RUN_SAMPLE_ISYN   (1u << 10) /* output_sample_isynaptic: end-of-step I_syn (push)   */
 
 typedef struct dtb_run_request {
     uint32_t iters;      /* RunRequest.iter; > 0                                                */
@@ -177,6 +180,10 @@ typedef struct dtb_run_output {
     uint8_t* sample_spike;  /* [iters * n_samples] in the order given to dtb_set_samples          */
     float* sample_v;        /* [iters * n_samples]                                               */
     float* sample_iou;      /* [iters * n_samples]                                               */
+    float* imeans;          /* [iters * n_pops] mean I_syn at the end of each step (DTB_RUN_IMEAN)  */
+    float* receptor_imeans; /* [iters * 4 * n_pops] mean I_AMPA, I_NMDA, I_GABAa, I_GABAb per step,
+                               receptor-major within a step (DTB_RUN_RECEPTOR_IMEAN)            */
+    float* sample_isyn;     /* [iters * n_samples] end-of-step I_syn of the sampled neurons        */
 } dtb_run_output;
 
 /* --- version and errors ------------------------------------------------- */

@@ -102,9 +102,14 @@ def test_against_block_new_golden(gpu, case):
         eng.set_noise_injected(z, u)
         done = 0
         for s_end in sorted(int(x.split("_")[-1]) for x in g.files if x.startswith("v_full_")):
-            r = eng.run(s_end - done, freq=True, record_spikes=True, prop_mode=pm, syn_mode=E.SYN_PUSH_EXACT)
+            r = eng.run(s_end - done, freq=True, record_spikes=True, prop_mode=pm, syn_mode=E.SYN_PUSH_EXACT,
+                        imean=True, receptor_imean=True)
             assert first_divergence(r.spikes, ref[done:s_end]) is None, f"spikes differ in steps {done}..{s_end}"
             assert np.allclose(r.freqs[:, 0] / n, g["mean_act"][done:s_end], rtol=0, atol=1e-7)
+            # block_new's mean_psc (torch float32 means of I_u over the population)
+            psc = g["mean_psc"][done:s_end]
+            assert np.allclose(r.receptor_imeans[:, :, 0], psc, rtol=1e-4, atol=1e-4)
+            assert np.allclose(r.imeans[:, 0], psc.astype(np.float64).sum(1), rtol=1e-4, atol=1e-4)
             v = eng.read_state(E.STATE_V)
             if dyadic:
                 assert np.array_equal(v, g[f"v_full_{s_end}"])
@@ -392,20 +397,24 @@ def test_samples_follow_oracle(gpu, block10k):
     z, _ = lo.torch_noise_stream(6, 10_000, steps, False)
     idx = np.array([5, 9999, 17, 3, 17, 4242])
     o = lo.LifOracle(block10k)
-    vs, ios, sps = [], [], []
+    vs, ios, sps, isy = [], [], [], []
     for s in range(steps):
         a, _ = o.step(z[s])
         vs.append(o.V[idx].copy())
         ios.append(o.i_bg[idx].copy())
         sps.append(a[idx].copy())
+        isy.append(o.I_syn[idx].copy())
     with E.Engine.from_arrays(block10k, pull=True) as eng:
         with pytest.raises(E.DtbError) as ei:
             eng.run(5, sample_spike=True)
         assert ei.value.status == E.UNSET_SAMPLE_FAILURE
         eng.set_samples(idx)
         eng.set_noise_injected(z)
-        r1 = eng.run(300, syn_mode=E.SYN_PUSH_EXACT, sample_spike=True, sample_v=True, sample_iou=True)
+        r1 = eng.run(300, syn_mode=E.SYN_PUSH_EXACT, sample_spike=True, sample_v=True, sample_iou=True,
+                     sample_isyn=True)
         r2 = eng.run(300, syn_mode=E.SYN_PULL, sample_spike=True, sample_v=True, sample_iou=True)
+    # output_sample_isynaptic: end-of-step I_syn, bit-exact in the deterministic push mode
+    assert np.array_equal(r1.sample_isyn, np.array(isy[:300]))
     sv = np.concatenate([r1.sample_v, r2.sample_v])
     si = np.concatenate([r1.sample_iou, r2.sample_iou])
     ss = np.concatenate([r1.sample_spike, r2.sample_spike])
@@ -510,3 +519,39 @@ def test_bf16_pull_precision_against_fp64():
     assert upto > 20
     assert np.max(np.abs(r.sample_v[:upto] - v64[:upto]) / np.abs(v64[:upto])) < 1e-4
     assert np.all(np.abs(rates(r.spikes) - r32) < 0.01 * r32)
+
+
+def test_imeans_follow_oracle():
+    """output_imean / output_receptor_imeas in exact mode: the population means of the
+    oracle's end-of-step I_u and I_syn (bit-exact per neuron here), within the 2^-24
+    fixed-point quantum of the sums; float push within float tolerance; pull refuses."""
+    spec = nw.structured_spec(12_000, 5, 200, seed=8)
+    net = co.structured_edges(spec)
+    steps = 300
+    z, _ = lo.torch_noise_stream(2, spec.n, steps, False)
+    o = lo.LifOracle(net)
+    pops = np.unique(o.pop)
+    ref_i = np.zeros((steps, spec.n_pops))
+    ref_u = np.zeros((steps, 4, spec.n_pops))
+    for s in range(steps):
+        o.step(z[s])
+        for k, p in enumerate(pops):
+            m = o.pop == p
+            ref_u[s, :, k] = o.I_u[:, m].astype(np.float64).mean(1)
+            ref_i[s, k] = o.I_syn[m].astype(np.float64).mean()
+    with E.Engine.structured(spec, pull=True) as eng:
+        eng.set_noise_injected(z)
+        r = eng.run(120, syn_mode=E.SYN_PUSH_EXACT, imean=True, receptor_imean=True)
+        r2 = eng.run(steps - 120, syn_mode=E.SYN_PUSH_EXACT, imean=True, receptor_imean=True)
+        rec = np.concatenate([r.receptor_imeans, r2.receptor_imeans])
+        im = np.concatenate([r.imeans, r2.imeans])
+        assert np.abs(ref_u).max() > 1.0
+        assert np.allclose(rec, ref_u, rtol=0, atol=1e-6)
+        assert np.allclose(im, ref_i, rtol=0, atol=1e-6)
+        with pytest.raises(E.DtbError) as ei:
+            eng.run(5, syn_mode=E.SYN_PULL, imean=True)
+        assert ei.value.status == E.UNSUPPORTED
+    with E.Engine.structured(spec) as eng:
+        eng.set_noise_injected(z)
+        r = eng.run(20, syn_mode=E.SYN_PUSH, receptor_imean=True)
+        assert np.allclose(r.receptor_imeans, ref_u[:20], rtol=1e-4, atol=1e-4)

@@ -57,7 +57,9 @@ def test_server_matches_direct_engine(gpu, tmp_path):
         assert stub.Updatesample(iter([pb.UpdateSampleRequest(block_id=0, sample_idx=[1, 2, 3]),
                                        pb.UpdateSampleRequest(block_id=1, sample_idx=[0, 7])])).success
         r2 = _run(stub, iter=200, output_freq=True, freq_char=True, use_ou_background=True,
-                  output_sample_spike=True, output_sample_vmemb=True)
+                  output_sample_spike=True, output_sample_vmemb=True, output_imean=True,
+                  output_receptor_imeas=True, output_sample_isynaptic=True)
+        assert _run(stub, iter=5, t_steps=2, use_ou_background=True)[0].status == pb.SNN_UNSUPPORTED
         assert not stub.Updatedopaminecurrentparam(iter([pb.UpdateDopamineCurrentParamRequest(block_id=0)])).success
         assert stub.Shutdown(pb.ShutdownRequest()).shutdown
         ch.close()
@@ -72,7 +74,8 @@ def test_server_matches_direct_engine(gpu, tmp_path):
         eng.update_prop_cols([7], [2], [1.2])
         eng.set_ou([0], [0.7], [0.25], [8.0])
         eng.set_samples([1, 2, 3, 3000, 3007])
-        d2 = eng.run(200, syn_mode=E.SYN_PUSH_EXACT, sample_spike=True, sample_v=True)
+        d2 = eng.run(200, syn_mode=E.SYN_PUSH_EXACT, sample_spike=True, sample_v=True, imean=True,
+                     receptor_imean=True, sample_isyn=True)
         sizes = eng.pop_sizes.astype(np.float32)
     f1 = np.stack([np.frombuffer(r.freq[0], np.int32) for r in r1])
     v1 = np.stack([np.frombuffer(r.vmean[0], np.float32) for r in r1])
@@ -84,3 +87,10 @@ def test_server_matches_direct_engine(gpu, tmp_path):
     s2 = np.stack([np.frombuffer(r.sample_spike[0], np.uint8) for r in r2])
     sv = np.stack([np.frombuffer(r.sample_vmemb[0], np.float32) for r in r2])
     assert np.array_equal(s2, d2.sample_spike) and np.array_equal(sv, d2.sample_v)
+    im = np.stack([np.frombuffer(r.imean[0], np.float32) for r in r2])
+    assert np.array_equal(im, d2.imeans)
+    for c, name in enumerate(("ampa_imean", "nmda_imean", "gabaa_imean", "gabab_imean")):
+        got = np.stack([np.frombuffer(getattr(r, name)[0], np.float32) for r in r2])
+        assert np.array_equal(got, d2.receptor_imeans[:, c])
+    si = np.stack([np.frombuffer(r.sample_isynaptic[0], np.float32) for r in r2])
+    assert np.array_equal(si, d2.sample_isyn) and np.abs(si).max() > 0
