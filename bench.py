@@ -41,6 +41,9 @@ CSR_COL_BYTES = 4
 ACC_BYTES = 8             # one logical accumulator update (a float pair) per event
 ROW_BYTES = 12            # rowptr pair + spike-list entry per spiking row
 PUSH_KINDS = ["reg", "tma", "local"]
+# DRAM bytes per delivered synaptic event of the population-local push with FP32 weights,
+# measured with ncu over a whole 500-step window (profiles/push_traffic_250k_window.md)
+LOCAL_PUSH_DRAM_BYTES_PER_EVENT_F32 = 13.4
 PUSH_KERNELS = ["push_kernel", "push_tma_kernel", "push_kernel (cross-population) + push_local_kernel (windows)"]
 
 
@@ -158,15 +161,13 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def traffic_per_launch(events_per_launch):
-    """DRAM bytes per push launch from the committed ncu summary, scaled by events."""
-    path = os.path.join(ROOT, "profiles", "push_kernel_ncu.json")
-    try:
-        with open(path) as f:
-            d = json.load(f)
-        return float(d["dram_bytes_per_launch"]) * events_per_launch / float(d["events_per_launch"])
-    except Exception:
-        return None
+def traffic_per_launch(events_per_launch, push_kind, f32):
+    """DRAM bytes of one push launch: the ncu-measured bytes per event (local push, FP32
+    weights; profiles/push_traffic_250k_window.md) times the launch's events; None for
+    variants without such a measurement."""
+    if push_kind == 2 and f32:
+        return LOCAL_PUSH_DRAM_BYTES_PER_EVENT_F32 * events_per_launch
+    return None
 
 
 def aggregate_replicas(counts, times_ms, dist=None, device=None):
@@ -282,7 +283,7 @@ def run_ours(args):
     if rank == 0:
         peak, peak_kind = peaks()
         achieved = push_bytes / (push_ms * 1e-3) / 1e9
-        traffic = traffic_per_launch(ev_launch)
+        traffic = traffic_per_launch(ev_launch, info.push_kind, wt == E.W_F32)
         step_bytes = push_bytes + lif_bytes
         cpu = None
         if world == 1 and not args.no_cpu:
