@@ -25,8 +25,9 @@ Batch::~Batch() {
     for (void* p : {static_cast<void*>(d_views), static_cast<void*>(d_prefix), static_cast<void*>(list),
                     static_cast<void*>(list_count), static_cast<void*>(list_ticket), static_cast<void*>(local_scratch)})
         if (p) cudaFree(p);
-    for (cudaEvent_t e : {ev0, ev1, tev[0], tev[1]})
+    for (cudaEvent_t e : {ev0, ev1, tev[0], tev[1], ev_fork, ev_join})
         if (e) cudaEventDestroy(e);
+    if (aux) cudaStreamDestroy(aux);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -36,6 +37,9 @@ int Batch::create(Engine* const* engines, uint32_t n) {
     DTB_CU(cudaEventCreate(&ev1));
     DTB_CU(cudaEventCreate(&tev[0]));
     DTB_CU(cudaEventCreate(&tev[1]));
+    DTB_CU(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
+    DTB_CU(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    DTB_CU(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     return set_members(engines, n);
 }
 
@@ -109,6 +113,9 @@ int Batch::set_members(Engine* const* engines, uint32_t n) {
     lb.windows_total = windows;
     lb.local_scratch = local_scratch;
     lb.sm_count = static_cast<uint32_t>(sm_count);
+    lb.aux = aux;
+    lb.ev_fork = ev_fork;
+    lb.ev_join = ev_join;
     if (graph) {
         cudaGraphExecDestroy(graph);
         graph = nullptr;

@@ -18,6 +18,8 @@ public:
     std::vector<Engine*> m;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev[2] = {nullptr, nullptr};
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int sm_count = 148;
     uint32_t wtype = W_F32;
     NetView* d_views = nullptr;

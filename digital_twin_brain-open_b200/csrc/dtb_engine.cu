@@ -55,6 +55,9 @@ Engine::~Engine() {
     if (tune_ev[1]) cudaEventDestroy(tune_ev[1]);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (aux) cudaStreamDestroy(aux);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -86,6 +89,9 @@ int Engine::init_common(const dtb_options& opt, uint32_t n_neurons) {
     DTB_CU(cudaGetDevice(&device));
     DTB_CU(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
     DTB_CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    DTB_CU(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
+    DTB_CU(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    DTB_CU(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     DTB_CU(cudaEventCreate(&ev0));
     DTB_CU(cudaEventCreate(&ev1));
     dt = opt.dt;
@@ -236,6 +242,9 @@ LaunchBatch Engine::single_batch() const {
     b.windows_total = n_windows;
     b.local_scratch = local_scratch;
     b.sm_count = static_cast<uint32_t>(sm_count);
+    b.aux = aux;
+    b.ev_fork = ev_fork;
+    b.ev_join = ev_join;
     return b;
 }
 
@@ -243,7 +252,7 @@ LaunchBatch Engine::single_batch() const {
 // param 1000 + lanes per row selects sub-warp rows.
 bool push_cfg_from_abi(int kind, int param, PushCfg& cfg) {
     cfg = PushCfg{kind, param, 32};
-    if ((kind == PUSH_REG || kind == PUSH_LOCAL) && param >= 1000) {
+    if ((kind == PUSH_REG || kind == PUSH_LOCAL) && param >= 1000 && param < 2000) {
         cfg.param = 8;
         cfg.lpr = param - 1000;
     }

@@ -75,6 +75,8 @@ public:
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t aux = nullptr;                            // second stream of the concurrent local push
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     float dt = 0.1f;
     uint32_t wtype = W_F32;
     uint64_t seed = 0;

@@ -628,6 +628,8 @@ push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase
 // rounding of float atomics onto J of order 10).
 // ---------------------------------------------------------------------------
 constexpr int kLocalThreads = 1024;
+constexpr int kLocalThreadsShared = 768;   // window kernel beside a cross-population CTA on the same SM
+constexpr int kLocalThreadsShared2 = 512;  // ... beside two
 constexpr int kLocalUnroll = 8;
 constexpr uint32_t kLocalUnitRows = 512;
 constexpr size_t kLocalSmem = 4ull * kLocalWin * sizeof(int) + kLocalUnitRows * (2 * sizeof(uint32_t) + sizeof(unsigned long long));
@@ -745,7 +747,7 @@ __device__ __forceinline__ void local_flush(const LocalWindow& W, int* acc) {
     __syncthreads();
     float4* J = W.nv->J + W.lo;
     const uint32_t width = W.hi - W.lo;
-    for (uint32_t i = threadIdx.x; i < width; i += kLocalThreads) {
+    for (uint32_t i = threadIdx.x; i < width; i += blockDim.x) {
         const int4 v = make_int4(acc[i], acc[kLocalWin + i], acc[2 * kLocalWin + i], acc[3 * kLocalWin + i]);
         if (v.x | v.y | v.z | v.w) {
             red_add_f32x4(J + i, make_float4(__fmul_rn(__int2float_rn(v.x), W.unscale), __fmul_rn(__int2float_rn(v.y), W.unscale),
@@ -759,7 +761,9 @@ __device__ __forceinline__ void local_flush(const LocalWindow& W, int* acc) {
     __syncthreads();
 }
 
-template <int WT>
+// launch bound of the full CTA for every NT: 64 registers, so the 768-thread form leaves a
+// 256-thread push CTA room on the SM
+template <int WT, int NT>
 __global__ void __launch_bounds__(kLocalThreads, 1)
 push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ win_prefix, uint32_t n_nets,
                   uint32_t windows, uint32_t* scratch) {
@@ -775,7 +779,7 @@ push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__
     uint32_t* counter = scratch + 2 * windows + 1;
     const uint32_t total_units = upre[windows];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    for (uint32_t i = threadIdx.x; i < 4 * kLocalWin; i += kLocalThreads) acc[i] = 0;
+    for (uint32_t i = threadIdx.x; i < 4 * kLocalWin; i += NT) acc[i] = 0;
     LocalWindow W{};
     uint32_t cur = 0xFFFFFFFFu;
     for (;;) {
@@ -800,7 +804,7 @@ push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__
         // rows with population rank in [r_lo, r_hi): block prefix over the bitmap
         const uint32_t* bits = (W.nv->clock->n & 1ull) ? W.nv->bits1 : W.nv->bits0;
         const uint32_t w_lo = W.p_lo >> 5, w_hi = (W.p_hi + 31) >> 5;
-        const uint32_t per = (w_hi - w_lo + kLocalThreads - 1) / kLocalThreads;
+        const uint32_t per = (w_hi - w_lo + NT - 1) / NT;
         const uint32_t my_lo = min(w_lo + threadIdx.x * per, w_hi), my_hi = min(my_lo + per, w_hi);
         uint32_t c = 0;
         for (uint32_t wi = my_lo; wi < my_hi; ++wi) c += __popc(pop_word(bits, wi, W.p_lo, W.p_hi));
@@ -820,7 +824,7 @@ push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__
         const uint32_t nrows = r_hi - r_lo;
         // span of every row of the unit: [out_ptr[j] + woff[k], out_ptr[j] + woff[k + 1])
         const NetView& nv = *W.nv;
-        for (uint32_t r = threadIdx.x; r < nrows; r += kLocalThreads) {
+        for (uint32_t r = threadIdx.x; r < nrows; r += NT) {
             const uint32_t j = s_rows[r];
             const uint32_t* wo = nv.woff + W.rb_k + static_cast<unsigned long long>(j - W.p_lo) * W.ka1;
             const uint32_t s0 = __ldg(wo), s1 = __ldg(wo + 1);
@@ -830,7 +834,7 @@ push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__
         __syncthreads();
         const uint32_t* col = nv.out_col;
         const void* wts = nv.out_w;
-        for (uint32_t r = warp; r < nrows; r += kLocalThreads / 32) {
+        for (uint32_t r = warp; r < nrows; r += NT / 32) {
             const unsigned long long e0 = s_start[r], e1 = e0 + s_len[r];
             for (unsigned long long e = e0 + lane; e < e1; e += 32ull * kLocalUnroll) {
                 uint32_t cc[kLocalUnroll];
@@ -1417,6 +1421,29 @@ cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop
 
 template <int ACC, int WT>
 static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint32_t ctas, cudaStream_t s) {
+    if (cfg.kind == PUSH_LOCAL && ACC == 0 && (cfg.param == kLocalConcurrent || cfg.param == kLocalConcurrent2) &&
+        b.aux && b.windows_total) {
+        // cross-population spans on the auxiliary stream, one (two) 256-thread CTA(s) per SM, next
+        // to the window kernel's 768 (512)-thread CTA: L2 reductions and shared-memory sums overlap
+        const bool two = cfg.param == kLocalConcurrent2;
+        cudaError_t e = cudaEventRecord(b.ev_fork, s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b.aux, b.ev_fork, 0);
+        if (e != cudaSuccess) return e;
+        push_kernel<ACC, WT, 8, 32, 1><<<b.sm_count * (two ? 2u : 1u), kPushThreads, 0, b.aux>>>(b.nets, b.vbase, b.n_nets, b.spikes);
+        e = cudaEventRecord(b.ev_join, b.aux);
+        if (e != cudaSuccess) return e;
+        local_count_kernel<<<b.windows_total, 256, 0, s>>>(b.nets, b.win_prefix, b.n_nets, b.local_scratch);
+        local_scan_kernel<<<1, 1024, 0, s>>>(b.local_scratch, b.windows_total);
+        if (two)
+            push_local_kernel<WT, kLocalThreadsShared2><<<b.sm_count, kLocalThreadsShared2, kLocalSmem, s>>>(
+                b.nets, b.win_prefix, b.n_nets, b.windows_total, b.local_scratch);
+        else
+            push_local_kernel<WT, kLocalThreadsShared><<<b.sm_count, kLocalThreadsShared, kLocalSmem, s>>>(
+                b.nets, b.win_prefix, b.n_nets, b.windows_total, b.local_scratch);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b.ev_join, 0);
+        return e;
+    }
     if (cfg.kind == PUSH_LOCAL && ACC == 0) {
         const dim3 grid(ctas), block(kPushThreads);
         if (cfg.lpr == 16)
@@ -1426,8 +1453,8 @@ static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint
         if (b.windows_total) {
             local_count_kernel<<<b.windows_total, 256, 0, s>>>(b.nets, b.win_prefix, b.n_nets, b.local_scratch);
             local_scan_kernel<<<1, 1024, 0, s>>>(b.local_scratch, b.windows_total);
-            push_local_kernel<WT><<<b.sm_count, kLocalThreads, kLocalSmem, s>>>(b.nets, b.win_prefix, b.n_nets,
-                                                                                 b.windows_total, b.local_scratch);
+            push_local_kernel<WT, kLocalThreads><<<b.sm_count, kLocalThreads, kLocalSmem, s>>>(
+                b.nets, b.win_prefix, b.n_nets, b.windows_total, b.local_scratch);
         }
     } else if (cfg.kind == PUSH_REG || cfg.kind == PUSH_LOCAL) {
         const dim3 grid(ctas), block(kPushThreads);
@@ -1460,8 +1487,14 @@ static cudaError_t push_prepare_wt(const PushCfg& cfg, int sm_count, uint32_t* c
     int per_sm = 0;
     cudaError_t e = cudaSuccess;
     if (cfg.kind == PUSH_LOCAL && ACC == 0) {
-        e = cudaFuncSetAttribute(push_local_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(push_local_kernel<WT, kLocalThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(kLocalSmem));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(push_local_kernel<WT, kLocalThreadsShared>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kLocalSmem));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(push_local_kernel<WT, kLocalThreadsShared2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kLocalSmem));
         if (e == cudaSuccess)
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.lpr == 16 ? push_kernel<ACC, WT, 8, 16, 1> : push_kernel<ACC, WT, 8, 32, 1>,
                                                               kPushThreads, 0);
@@ -1506,7 +1539,8 @@ static cudaError_t push_launch_acc(const LaunchBatch& b, int wt, const PushCfg& 
 const PushCfg kPushCands[kPushCandidates] = {{PUSH_REG, 4, 32}, {PUSH_REG, 8, 32}, {PUSH_REG, 16, 32},
                                              {PUSH_REG, 8, 16}, {PUSH_REG, 8, 8},
                                              {PUSH_TMA, 256, 32}, {PUSH_TMA, 512, 32},
-                                             {PUSH_LOCAL, 8, 32}, {PUSH_LOCAL, 8, 16}};
+                                             {PUSH_LOCAL, 8, 32}, {PUSH_LOCAL, 8, 16},
+                                             {PUSH_LOCAL, kLocalConcurrent, 32}, {PUSH_LOCAL, kLocalConcurrent2, 32}};
 
 cudaError_t push_prepare(int exact, int wt, const PushCfg& cfg, int sm_count, uint32_t* ctas) {
     if (exact) {

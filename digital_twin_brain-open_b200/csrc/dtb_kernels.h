@@ -23,6 +23,8 @@ struct LaunchBatch {
     uint32_t windows_total;
     uint32_t* local_scratch;      // device [2 * windows_total + 2]: rows per window, unit prefix, unit counter
     uint32_t sm_count;
+    cudaStream_t aux;             // second stream of the concurrent local push (fork/join by events)
+    cudaEvent_t ev_fork, ev_join;
     SpikeList spikes;
 };
 
@@ -39,7 +41,9 @@ struct PushCfg {
 };
 
 // Every variant the autotuner times.
-constexpr int kPushCandidates = 9;
+constexpr int kPushCandidates = 11;
+constexpr int kLocalConcurrent = 2008;   // PUSH_LOCAL param: cross-population part on a second stream
+constexpr int kLocalConcurrent2 = 2016;  // ... with two push CTAs per SM beside a 512-thread window CTA
 extern const PushCfg kPushCands[kPushCandidates];
 // Sets kernel attributes and returns the persistent grid (max resident CTAs).
 cudaError_t push_prepare(int exact, int weight_type, const PushCfg& cfg, int sm_count, uint32_t* ctas);
@@ -47,7 +51,7 @@ cudaError_t launch_push(const LaunchBatch& b, int exact, int weight_type, const 
                         cudaStream_t s);
 // Kernels launch_push issues beyond the first (the local variant's count, scan and window passes).
 inline uint32_t push_extra_launches(const LaunchBatch& b, int exact, const PushCfg& cfg) {
-    return (cfg.kind == PUSH_LOCAL && !exact && b.windows_total) ? 3u : 0u;
+    return (cfg.kind == PUSH_LOCAL && !exact && b.windows_total) ? 3u : 0u;   // concurrent form: same count
 }
 cudaError_t launch_pull(const LaunchBatch& b, int gather, int weight_type, uint32_t flags, int prop_mode, cudaStream_t s);
 cudaError_t launch_fold_finish(const LaunchBatch& b, cudaStream_t s);

@@ -85,7 +85,7 @@ def test_batch_local_push_step(gpu, graph):
         j_ref = [e.read_state(E.STATE_J) for e in engines]
         for e, blob in zip(engines, blobs):
             e.load_state(blob)
-        b.set_push_variant(E.PUSH_LOCAL, 8)
+        b.set_push_variant(E.PUSH_LOCAL, 2008 if graph else 8)
         got = b.run(1, record_spikes=True, syn_mode=E.SYN_PUSH)
         assert b.info()["push_kind"] == E.PUSH_LOCAL
     for i, e in enumerate(engines):
