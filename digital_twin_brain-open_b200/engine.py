@@ -124,6 +124,8 @@ SIGNATURES = {
     "dtb_batch_set_push_variant": (_I32, [_P, _I32, _I32]),
     "dtb_batch_info": (_I32, [_P, _P, _P, _P, _P]),
     "dtb_compact_spikes_noalloc": (_I32, [_P, _U32, _P, _P, _P]),
+    "dtb_bold_default_params": (None, [_P]),
+    "dtb_bold_run": (_I32, [_P, _U32, _U32, _P, _P, _P, _P]),
     "dtb_server_default_options": (None, [_P]),
     "dtb_server_create": (_I32, [_P, C.POINTER(C.c_void_p)]),
     "dtb_server_destroy": (_I32, [_P]),
@@ -224,6 +226,33 @@ class ServerInfo(C.Structure):
 
 
 SERVE_BATCHED, SERVE_SEQUENTIAL = 0, 1
+
+
+class BoldParams(C.Structure):
+    _fields_ = [(f, C.c_double) for f in ("epsilon", "tao_s", "tao_f", "tao_0", "alpha", "E_0", "V_0", "delta_t")]
+
+
+def bold_params(**kw):
+    """dtb_bold_params with DA_voxel.py's defaults, overridden by keyword."""
+    p = BoldParams()
+    LIB.dtb_bold_default_params(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, float(v))
+    return p
+
+
+def bold_run(u, state, params=None, out=True, stream=0):
+    """BOLD.run over a window: u, state are CUDA float32 torch tensors ([steps, n], [4, n]:
+    s, q, v, f_in, advanced in place); returns the [steps, n] signal (or None)."""
+    import torch
+    assert u.is_cuda and state.is_cuda and u.dtype == torch.float32 and state.dtype == torch.float32
+    steps, n = u.shape
+    u = u.contiguous()
+    o = torch.empty_like(u) if out else None
+    p = params or bold_params()
+    _check(LIB.dtb_bold_run(C.byref(p), n, steps, C.c_void_p(u.data_ptr()), C.c_void_p(state.data_ptr()),
+                            None if o is None else C.c_void_p(o.data_ptr()), C.c_void_p(stream)))
+    return o
 
 
 @dataclasses.dataclass

@@ -335,6 +335,22 @@ int32_t dtb_server_add_npz(void* server, const char* path, const dtb_options* op
 int32_t dtb_server_play(void* server, uint32_t n, dtb_request* reqs, uint32_t policy);
 int32_t dtb_server_info(void* server, dtb_server_stats* info);
 
+/* --- BOLD signal (data assimilation) ----------------------------------------
+ * models/bold_model_pytorch.py:61-96, driven per simulated step by
+ * data_assimilation/DA_voxel.py:314-331.  Parameters are doubles, as the
+ * reference's Python floats are. */
+typedef struct dtb_bold_params {
+    double epsilon, tao_s, tao_f, tao_0, alpha, E_0, V_0;
+    double delta_t;          /* s per step (BOLD.__init__ default 1e-3) */
+} dtb_bold_params;
+void dtb_bold_default_params(dtb_bold_params* p);   /* DA_voxel.py:470-476 */
+/* Advance n voxels by `steps` steps of BOLD.run: u [steps * n] voxel activity,
+ * state [4 * n] = s, q, v, f_in (in/out; BOLD.run starts from 0, 0, 1, 1),
+ * out [steps * n] the BOLD signal of every step or NULL.  Device pointers,
+ * enqueued on `stream` (NULL: the default stream). */
+int32_t dtb_bold_run(const dtb_bold_params* p, uint32_t n, uint32_t steps, const float* u, float* state,
+                     float* out, void* stream);
+
 /* --- state access (tests, checkpoint, serving eviction) ------------------ */
 #define DTB_STATE_V      0  /* float [n]                                       */
 #define DTB_STATE_J      1  /* float [n*4] (AMPA, NMDA, GABAa, GABAb per neuron) */
