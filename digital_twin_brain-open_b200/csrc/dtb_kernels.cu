@@ -516,6 +516,24 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
     }
 }
 
+// Prefetch into L2 the 128-byte lines of a CSR span (targets and weight pairs),
+// one line per lane: no registers stay live and nothing waits for the data.
+template <int WT>
+__device__ __forceinline__ void prefetch_span_l2(const uint32_t* col, const void* wts, unsigned long long e0,
+                                                 uint32_t len, uint32_t lane) {
+    if (len == 0) return;
+    constexpr uint32_t kWB = WT == W_F32 ? 8 : (WT == W_U8 ? 2 : 4);
+    const uintptr_t c0 = reinterpret_cast<uintptr_t>(col + e0) & ~uintptr_t(127);
+    const uintptr_t c1 = reinterpret_cast<uintptr_t>(col + e0 + len);
+    const uintptr_t w0 = (reinterpret_cast<uintptr_t>(wts) + e0 * kWB) & ~uintptr_t(127);
+    const uintptr_t w1 = reinterpret_cast<uintptr_t>(wts) + (e0 + len) * kWB;
+    const uint32_t nc = static_cast<uint32_t>((c1 - c0 + 127) >> 7), nw = static_cast<uint32_t>((w1 - w0 + 127) >> 7);
+    for (uint32_t k = lane; k < nc + nw; k += 32) {
+        const uintptr_t a = k < nc ? c0 + (static_cast<uintptr_t>(k) << 7) : w0 + (static_cast<uintptr_t>(k - nc) << 7);
+        asm volatile("prefetch.global.L2 [%0];" :: "l"(a));
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Push propagation: one warp per spiking row of the out-degree CSR
 // ---------------------------------------------------------------------------
@@ -836,6 +854,10 @@ push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__
         const void* wts = nv.out_w;
         for (uint32_t r = warp; r < nrows; r += NT / 32) {
             const unsigned long long e0 = s_start[r], e1 = e0 + s_len[r];
+            // the warp's next row: pull its span into L2 while this row is summed (measured:
+            // one row ahead beats two; prefetching in the scattered push made it slower)
+            if (r + NT / 32 < nrows)
+                prefetch_span_l2<WT>(col, wts, s_start[r + NT / 32], s_len[r + NT / 32], lane);
             for (unsigned long long e = e0 + lane; e < e1; e += 32ull * kLocalUnroll) {
                 uint32_t cc[kLocalUnroll];
                 float2 w[kLocalUnroll];
