@@ -275,7 +275,6 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
            int prop_mode) {
     extern __shared__ __align__(128) float lsm[];
     __shared__ __align__(8) uint64_t s_bar[2];
-    __shared__ NetView s_nv;
     __shared__ int s_cnt[kStatSlots];
     __shared__ long long s_vs[kStatSlots];
 
@@ -302,11 +301,10 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
         const uint32_t net = n_nets > 1 ? find_net(tile_prefix, n_nets, gt) : 0u;
         const uint32_t stg = it & 1u;
         if (net != cur_net) {
-            // hand in the previous network's tiles, then switch views
-            if (tid == 0 && done_here) lif_ticket(s_nv, done_here, t_last_tile, n_last_tile);
+            // hand in the previous network's tiles (views are read through the
+            // read-only cache, so switching needs no barrier)
+            if (tid == 0 && done_here) lif_ticket(nets[cur_net], done_here, t_last_tile, n_last_tile);
             done_here = 0;
-            __syncthreads();
-            load_netview(s_nv, nets + net);
             cur_net = net;
         }
         // barrier A: the other stage's readers (previous tile) are done and its
@@ -316,7 +314,7 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
             lif_prefetch(nets, tile_prefix, n_nets, gt + gridDim.x, lsm + (stg ^ 1u) * kLifStageFloats, &s_bar[stg ^ 1u]);
         }
         __syncthreads();
-        const NetView& nv = s_nv;
+        const NetView& nv = nets[net];
         const uint32_t tile = gt - __ldg(tile_prefix + net);
         const uint32_t tile_first = tile * kLifTile;
         const uint32_t i0 = tile_first + tid * 4;
@@ -512,7 +510,7 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
     // the CTA's last stores complete before its tiles count towards the clock
     if (tid == 0) {
         bulk_wait_all();
-        if (done_here) lif_ticket(s_nv, done_here, t_last_tile, n_last_tile);
+        if (done_here) lif_ticket(nets[cur_net], done_here, t_last_tile, n_last_tile);
     }
 }
 
