@@ -68,6 +68,10 @@ def parse():
     p.add_argument("--slice", type=int, default=100, help="steps per continuous-batching slice (serve form)")
     p.add_argument("--hbm-cap-gb", type=float, default=150.0, help="HBM cap of the resident networks (serve form)")
     p.add_argument("--members", type=int, default=None, help="ensemble members (64) or served networks (128)")
+    p.add_argument("--net", default="regional", choices=["regional", "uniform"],
+                   help="regional: the structured regional network; uniform: the plain one-population block")
+    p.add_argument("--syn", default="push", choices=["push", "exact", "pull"],
+                   help="synaptic mode: float push, exact (fixed-point) push, or deterministic pull")
     p.add_argument("--window", type=int, default=800, help="steps per assimilation window (ensemble form)")
     return p.parse_args()
 
@@ -204,9 +208,18 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     wt = E.W_BF16 if args.weights == "bf16" else E.W_F32
-    spec = nw.structured_spec(args.neurons, args.pops, args.degree, SPEC_SEED)
+    syn = {"push": E.SYN_PUSH, "exact": E.SYN_PUSH_EXACT, "pull": E.SYN_PULL}[args.syn]
     t0 = time.perf_counter()
-    eng = E.Engine.structured(spec, weight_type=wt, seed=1000 + rank)
+    if args.net == "uniform":
+        # the plain block: one population, fixed in-degree, uniform sources (host-built CSR)
+        net = nw.make_uniform_block(args.neurons, args.degree, seed=0)
+        if wt == E.W_BF16:
+            net["weight"] = net["weight"].astype(np.float32)
+        eng = E.Engine.from_arrays(net, weight_type=wt, seed=1000 + rank, push=syn != E.SYN_PULL, pull=syn == E.SYN_PULL)
+        del net
+    else:
+        spec = nw.structured_spec(args.neurons, args.pops, args.degree, SPEC_SEED)
+        eng = E.Engine.structured(spec, weight_type=wt, seed=1000 + rank, push=syn != E.SYN_PULL, pull=syn == E.SYN_PULL)
     build_s = time.perf_counter() - t0
     if args.push != "auto":
         kind, param = args.push.split(":")
@@ -222,7 +235,7 @@ def run_ours(args):
             dist.barrier()
 
     for _ in range(args.warmup):
-        eng.run(WINDOW, freq=True, out=(fr, None))
+        eng.run(WINDOW, freq=True, out=(fr, None), syn_mode=syn)
 
     uuid = str(getattr(torch.cuda.get_device_properties(dev), "uuid", ""))
     sampler = ClockSampler(uuid)
@@ -235,7 +248,7 @@ def run_ours(args):
     with torch.cuda.stream(stream):
         start.record(stream)
         for _ in range(args.steps):
-            r = eng.run(WINDOW, freq=True, out=(fr, None))
+            r = eng.run(WINDOW, freq=True, out=(fr, None), syn_mode=syn)
             events += r.events
             spikes += int(fr.sum())
             launches += r.launches
@@ -248,13 +261,20 @@ def run_ours(args):
     info = eng.info()
     tuning = [{"kernel": PUSH_KINDS[k], "param": p, "ms": m} for k, p, m in eng.tuning_report()]
     # per-kernel timing window (after the timed region)
-    rk = eng.run(WINDOW, freq=True, out=(fr, None), time_kernels=True)
+    rk = eng.run(WINDOW, freq=True, out=(fr, None), time_kernels=True, syn_mode=syn)
     lif_ms, push_ms = rk.kernel_ms[0] / WINDOW, rk.kernel_ms[1] / WINDOW
     ev_launch = rk.events / WINDOW
     spk_launch = fr.sum() / WINDOW
     wbytes = 4 if wt == E.W_BF16 else 8
     push_bytes = spk_launch * ROW_BYTES + ev_launch * (CSR_COL_BYTES + wbytes + ACC_BYTES)
     lif_bytes = info.n_neurons * BYTES_STATE + info.n_neurons / 8
+    roof_kernel = PUSH_KERNELS[info.push_kind]
+    if syn == E.SYN_PULL:
+        # one fused kernel gathers every in-edge (4 + B_w bytes each), tests the bitmap and steps the neurons
+        lif_ms, push_ms = 0.0, rk.kernel_ms[2] / WINDOW
+        push_bytes = info.n_edges * (CSR_COL_BYTES + wbytes) + info.n_neurons / 8 + lif_bytes
+        lif_bytes = 0.0
+        roof_kernel = "lif_pull_kernel (in-degree gather fused with the LIF step)"
 
     # e2e through the C-ABI with host buffers (H2D of OU parameters, D2H of every step's outputs)
     rng = np.random.default_rng(rank)
@@ -269,7 +289,7 @@ def run_ours(args):
             mean = rng.uniform(0.55, 0.65, P).astype(np.float32)
             sigma = rng.uniform(0.18, 0.22, P).astype(np.float32)
             eng.set_ou(pop_ids, mean, sigma, np.full(P, 10.0, np.float32))
-            r = eng.run(WINDOW, freq=True, vmean=True, out=(fr, vm))
+            r = eng.run(WINDOW, freq=True, vmean=True, out=(fr, vm), syn_mode=syn)
             e2e_events += r.events
         e_end.record(stream)
     e_end.synchronize()
@@ -283,7 +303,7 @@ def run_ours(args):
     if rank == 0:
         peak, peak_kind = peaks()
         achieved = push_bytes / (push_ms * 1e-3) / 1e9
-        traffic = traffic_per_launch(ev_launch, info.push_kind, wt == E.W_F32)
+        traffic = traffic_per_launch(ev_launch, info.push_kind, wt == E.W_F32) if syn == E.SYN_PUSH else None
         step_bytes = push_bytes + lif_bytes
         cpu = None
         if world == 1 and not args.no_cpu:
@@ -297,8 +317,9 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32" if wt == E.W_F32 else "bf16-weights/f32-state",
             "data": "synthetic (seeded regional network generated on the device)",
             "sim_ms_per_wall_s": args.steps * WINDOW * 0.1 / (ms / 1e3),
-            "config": {"workload": f"{info.n_neurons}-neuron regional LIF network, {P} populations, "
-                                   f"in-degree {args.degree}, {args.weights} weights, OU background, push propagation",
+            "config": {"workload": f"{info.n_neurons}-neuron {args.net} LIF network, {P} populations, "
+                                   f"in-degree {args.degree}, {args.weights} weights, OU background, "
+                                   f"{ {'push': 'push', 'exact': 'exact fixed-point push', 'pull': 'deterministic pull'}[args.syn] } propagation",
                        "neurons": info.n_neurons, "synapses": int(info.n_edges), "populations": P,
                        "dt_ms": 0.1, "steps_per_bench_step": WINDOW,
                        "timed_sim_steps": args.steps * WINDOW, "warmup_sim_steps": args.warmup * WINDOW,
@@ -313,7 +334,7 @@ def run_ours(args):
                        "local_windows": int(info.local_windows),
                        "push_autotune": tuning,
                        "step_roofline_frac": step_bytes / ((lif_ms + push_ms) * 1e-3) / 1e9 / peak},
-            "roofline": {"bound": "hbm", "kernel": PUSH_KERNELS[info.push_kind], "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": roof_kernel, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "algorithmic_bytes_per_launch": push_bytes},
             "cpu_baseline": cpu,
