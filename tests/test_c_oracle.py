@@ -64,9 +64,9 @@ def test_c_oracle64_equals_numpy_float64_oracle():
 def test_float32_clock_explains_the_rate_gap():
     """FP64 with only its clock rounded to float32 fires like the float32 model: the
     refractory test on block_new's float32 time is what moves the rate, not V."""
-    spec = nw.structured_spec(100_000, 4, 1000, seed=1)
+    spec = nw.structured_spec(30_000, 2, 1000, seed=1)
     net = cc.structured_edges(spec)
-    steps, warm = 500, 200
+    steps, warm = 400, 150
     z = np.random.default_rng(7).standard_normal((steps, spec.n), dtype=np.float32)
     r64 = cc.COracle64(net).run(z)[0][warm:].mean()
     r64c = cc.COracle64(net).run(z, clock32=True)[0][warm:].mean()
