@@ -13,7 +13,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libdtb_b200.so")
-SOURCES = ["dtb_engine.cu", "dtb_kernels.cu", "dtb_generate.cu", "dtb_host.cu", "dtb_compact.cu", "dtb_compact_noalloc.cu", "dtb_batch.cu", "dtb_serve.cu", "dtb_bold.cu"]
+SOURCES = ["dtb_engine.cu", "dtb_kernels.cu", "dtb_generate.cu", "dtb_host.cu", "dtb_compact.cu", "dtb_compact_noalloc.cu", "dtb_batch.cu", "dtb_serve.cu", "dtb_bold.cu", "dtb_da.cu"]
 HEADERS = ["dtb_device.cuh", "dtb_kernels.h", "dtb_engine.h", "dtb_host.h", "dtb_compact.h", "dtb_batch.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

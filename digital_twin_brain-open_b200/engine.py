@@ -126,6 +126,7 @@ SIGNATURES = {
     "dtb_compact_spikes_noalloc": (_I32, [_P, _U32, _P, _P, _P]),
     "dtb_bold_default_params": (None, [_P]),
     "dtb_bold_run": (_I32, [_P, _U32, _U32, _P, _P, _P, _P]),
+    "dtb_da_filter": (_I32, [_U32, _U32, _U32, _P, _P, _P, C.c_double, C.c_double, _P, _P]),
     "dtb_server_default_options": (None, [_P]),
     "dtb_server_create": (_I32, [_P, C.POINTER(C.c_void_p)]),
     "dtb_server_destroy": (_I32, [_P]),
@@ -239,6 +240,19 @@ def bold_params(**kw):
     for k, v in kw.items():
         setattr(p, k, float(v))
     return p
+
+
+def da_filter(w_hat, bold_y, noise, bold_sigma, rate=0.5, stream=0):
+    """DA_voxel.filter on CUDA float32 torch tensors w_hat [E, V, S], bold_y [V], noise [E, V]."""
+    import torch
+    assert w_hat.is_cuda and w_hat.dtype == torch.float32
+    E, V, S = w_hat.shape
+    w_hat, bold_y, noise = w_hat.contiguous(), bold_y.contiguous(), noise.contiguous()
+    out = torch.empty_like(w_hat)
+    _check(LIB.dtb_da_filter(E, V, S, C.c_void_p(w_hat.data_ptr()), C.c_void_p(bold_y.data_ptr()),
+                             C.c_void_p(noise.data_ptr()), float(bold_sigma), float(rate), C.c_void_p(out.data_ptr()),
+                             C.c_void_p(stream)))
+    return out
 
 
 def bold_run(u, state, params=None, out=True, stream=0):

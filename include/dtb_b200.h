@@ -351,6 +351,15 @@ void dtb_bold_default_params(dtb_bold_params* p);   /* DA_voxel.py:470-476 */
 int32_t dtb_bold_run(const dtb_bold_params* p, uint32_t n, uint32_t steps, const float* u, float* state,
                      float* out, void* stream);
 
+/* Ensemble Kalman update DA_voxel.filter (data_assimilation/DA_voxel.py:289-307):
+ * w_hat [E * V * S] float32 (member-major, then voxel, then state; S = hp_num + 6,
+ * the BOLD signal last), bold_y [V] the observed BOLD, noise [E * V] the
+ * standard-normal draws the reference takes from torch.normal (scaled by
+ * sqrt(bold_sigma) inside), rate as in filter(); w_out [E * V * S].  Device
+ * pointers on `stream`; accumulation in double, one rounding to float32. */
+int32_t dtb_da_filter(uint32_t ensembles, uint32_t voxels, uint32_t states, const float* w_hat, const float* bold_y,
+                      const float* noise, double bold_sigma, double rate, float* w_out, void* stream);
+
 /* --- state access (tests, checkpoint, serving eviction) ------------------ */
 #define DTB_STATE_V      0  /* float [n]                                       */
 #define DTB_STATE_J      1  /* float [n*4] (AMPA, NMDA, GABAa, GABAb per neuron) */

@@ -63,3 +63,25 @@ def bold_inputs(n, steps, seed):
     rng = np.random.default_rng(seed)
     walk = np.cumsum(rng.standard_normal((steps, n)), axis=0) / 20.0
     return np.maximum(0.1 + 0.05 * walk, 1e-5).astype(np.float32)
+
+
+def da_filter(w_hat, bold_y, noise, hp_num, bold_sigma, rate=0.5):
+    """Ensemble Kalman update of DA_voxel.filter (data_assimilation/DA_voxel.py:289-307),
+    float32 in, reductions and products accumulated in float64, result rounded once.
+
+    w_hat [E, V, S] (S = hp_num + 6, the BOLD signal last), bold_y [V] the observation,
+    noise [E, V] the standard-normal draws the reference takes from torch.normal (scaled
+    by sqrt(bold_sigma) here as there).  Returns w [E, V, S] float32.
+    """
+    w_hat = np.asarray(w_hat, np.float64)
+    E, V, S = w_hat.shape
+    assert S == hp_num + 6
+    w_mean = w_hat.mean(axis=0, keepdims=True)
+    w_diff = w_hat - w_mean
+    w_cxx = (w_diff[:, :, -1] ** 2).sum(axis=0) / (E - 1) + bold_sigma
+    temp = w_diff[:, :, -1] / w_cxx[None, :] / (E - 1)
+    innov = np.asarray(bold_y, np.float64)[None, :] + np.sqrt(bold_sigma) * np.asarray(noise, np.float64) - w_hat[:, :, -1]
+    w = w_hat + rate * innov[:, :, None] * (temp[:, :, None] * w_diff).sum(axis=0, keepdims=True)
+    g = (innov @ temp.T) / V
+    w = w + (1 - rate) * (g @ w_diff.reshape(E, V * S)).reshape(E, V, S)
+    return w.astype(np.float32)
