@@ -287,6 +287,12 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
     uint32_t done_here = 0;            // tiles of cur_net this CTA finished (thread 0's ticket)
     float t_last_tile = 0.f;
     unsigned long long n_last_tile = 0;
+    // finished (network, tiles) pairs, handed in when the CTA ends; a full table is handed in early
+    constexpr int kTicketSlots = 48;
+    __shared__ uint32_t s_tk_net[kTicketSlots], s_tk_cnt[kTicketSlots];
+    __shared__ float s_tk_t[kTicketSlots];
+    __shared__ unsigned long long s_tk_n[kTicketSlots];
+    uint32_t n_tk = 0;                 // thread 0's count of table entries
     if (tid < kStatSlots) { s_cnt[tid] = 0; s_vs[tid] = 0; }
     if (tid == 0) {
         mbar_init(&s_bar[0], 1);
@@ -303,7 +309,17 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
         if (net != cur_net) {
             // hand in the previous network's tiles (views are read through the
             // read-only cache, so switching needs no barrier)
-            if (tid == 0 && done_here) lif_ticket(nets[cur_net], done_here, t_last_tile, n_last_tile);
+            if (tid == 0 && done_here) {
+                if (n_tk == kTicketSlots) {
+                    for (uint32_t q = 0; q < n_tk; ++q) lif_ticket(nets[s_tk_net[q]], s_tk_cnt[q], s_tk_t[q], s_tk_n[q]);
+                    n_tk = 0;
+                }
+                s_tk_net[n_tk] = cur_net;
+                s_tk_cnt[n_tk] = done_here;
+                s_tk_t[n_tk] = t_last_tile;
+                s_tk_n[n_tk] = n_last_tile;
+                ++n_tk;
+            }
             done_here = 0;
             cur_net = net;
         }
@@ -510,6 +526,7 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
     // the CTA's last stores complete before its tiles count towards the clock
     if (tid == 0) {
         bulk_wait_all();
+        for (uint32_t q = 0; q < n_tk; ++q) lif_ticket(nets[s_tk_net[q]], s_tk_cnt[q], s_tk_t[q], s_tk_n[q]);
         if (done_here) lif_ticket(nets[cur_net], done_here, t_last_tile, n_last_tile);
     }
 }
