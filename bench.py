@@ -80,6 +80,8 @@ def parse():
 # CPU: the C port of the reference model on a bounded sample
 # ---------------------------------------------------------------------------
 def cpu_sample_rate(max_seconds=None):
+    import __graft_entry__
+    __graft_entry__.load_package()        # registers the package (network specs only; no CUDA library)
     from dtb_b200 import network as nw
     from oracle import c_oracle as cc
     from oracle import lif_oracle as lo
