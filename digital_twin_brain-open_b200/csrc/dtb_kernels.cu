@@ -533,7 +533,7 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
 
 // Prefetch into L2 the 128-byte lines of a CSR span (targets and weight pairs),
 // one line per lane: no registers stay live and nothing waits for the data.
-template <int WT>
+template <int WT, int LANES = 32>
 __device__ __forceinline__ void prefetch_span_l2(const uint32_t* col, const void* wts, unsigned long long e0,
                                                  uint32_t len, uint32_t lane) {
     if (len == 0) return;
@@ -543,7 +543,7 @@ __device__ __forceinline__ void prefetch_span_l2(const uint32_t* col, const void
     const uintptr_t w0 = (reinterpret_cast<uintptr_t>(wts) + e0 * kWB) & ~uintptr_t(127);
     const uintptr_t w1 = reinterpret_cast<uintptr_t>(wts) + (e0 + len) * kWB;
     const uint32_t nc = static_cast<uint32_t>((c1 - c0 + 127) >> 7), nw = static_cast<uint32_t>((w1 - w0 + 127) >> 7);
-    for (uint32_t k = lane; k < nc + nw; k += 32) {
+    for (uint32_t k = lane; k < nc + nw; k += LANES) {
         const uintptr_t a = k < nc ? c0 + (static_cast<uintptr_t>(k) << 7) : w0 + (static_cast<uintptr_t>(k - nc) << 7);
         asm volatile("prefetch.global.L2 [%0];" :: "l"(a));
     }
@@ -796,7 +796,7 @@ __device__ __forceinline__ void local_flush(const LocalWindow& W, int* acc) {
 
 // launch bound of the full CTA for every NT: 64 registers, so the 768-thread form leaves a
 // 256-thread push CTA room on the SM
-template <int WT, int NT>
+template <int WT, int NT, int RL = 32>
 __global__ void __launch_bounds__(kLocalThreads, 1)
 push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ win_prefix, uint32_t n_nets,
                   uint32_t windows, uint32_t* scratch) {
@@ -867,18 +867,22 @@ push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__
         __syncthreads();
         const uint32_t* col = nv.out_col;
         const void* wts = nv.out_w;
-        for (uint32_t r = warp; r < nrows; r += NT / 32) {
+        // RL lanes per row: 32 (a warp per row) or 16 (two rows per warp, for short spans)
+        constexpr uint32_t kRows = 32 / RL;
+        const uint32_t sl = lane % RL;
+        const uint32_t rstride = (NT / 32) * kRows;
+        for (uint32_t r = warp * kRows + lane / RL; r < nrows; r += rstride) {
             const unsigned long long e0 = s_start[r], e1 = e0 + s_len[r];
-            // the warp's next row: pull its span into L2 while this row is summed (measured:
-            // one row ahead beats two; prefetching in the scattered push made it slower)
-            if (r + NT / 32 < nrows)
-                prefetch_span_l2<WT>(col, wts, s_start[r + NT / 32], s_len[r + NT / 32], lane);
-            for (unsigned long long e = e0 + lane; e < e1; e += 32ull * kLocalUnroll) {
+            // the next row of these lanes: pull its span into L2 while this row is summed
+            // (measured: one row ahead beats two; prefetching in the scattered push made it slower)
+            if (r + rstride < nrows)
+                prefetch_span_l2<WT, RL>(col, wts, s_start[r + rstride], s_len[r + rstride], sl);
+            for (unsigned long long e = e0 + sl; e < e1; e += static_cast<unsigned long long>(RL) * kLocalUnroll) {
                 uint32_t cc[kLocalUnroll];
                 float2 w[kLocalUnroll];
 #pragma unroll
                 for (int q = 0; q < kLocalUnroll; ++q) {
-                    const unsigned long long idx = e + 32ull * q;
+                    const unsigned long long idx = e + static_cast<unsigned long long>(RL) * q;
                     if (idx < e1) {
                         cc[q] = __ldcs(col + idx);
                         w[q] = load_weight<WT>(wts, idx);
@@ -886,7 +890,7 @@ push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__
                 }
 #pragma unroll
                 for (int q = 0; q < kLocalUnroll; ++q) {
-                    if (e + 32ull * q < e1) {
+                    if (e + static_cast<unsigned long long>(RL) * q < e1) {
                         const int* d = acc + (cc[q] >> 31) * (2u * kLocalWin) + ((cc[q] & kIndexMask) - W.lo);
                         red_add_shared_u32(d, static_cast<uint32_t>(__float2int_rn(__fmul_rn(w[q].x, W.scale))));
                         red_add_shared_u32(d + kLocalWin, static_cast<uint32_t>(__float2int_rn(__fmul_rn(w[q].y, W.scale))));
@@ -1458,7 +1462,8 @@ cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop
 
 template <int ACC, int WT>
 static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint32_t ctas, cudaStream_t s) {
-    if (cfg.kind == PUSH_LOCAL && ACC == 0 && (cfg.param == kLocalConcurrent || cfg.param == kLocalConcurrent2) &&
+    if (cfg.kind == PUSH_LOCAL && ACC == 0 &&
+        (cfg.param == kLocalConcurrent || cfg.param == kLocalConcurrent2 || cfg.param == kLocalConcurrentHalf) &&
         b.aux && b.windows_total) {
         // cross-population spans on the auxiliary stream, one (two) 256-thread CTA(s) per SM, next
         // to the window kernel's 768 (512)-thread CTA: L2 reductions and shared-memory sums overlap
@@ -1473,6 +1478,9 @@ static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint
         local_scan_kernel<<<1, 1024, 0, s>>>(b.local_scratch, b.windows_total);
         if (two)
             push_local_kernel<WT, kLocalThreadsShared2><<<b.sm_count, kLocalThreadsShared2, kLocalSmem, s>>>(
+                b.nets, b.win_prefix, b.n_nets, b.windows_total, b.local_scratch);
+        else if (cfg.param == kLocalConcurrentHalf)
+            push_local_kernel<WT, kLocalThreadsShared, 16><<<b.sm_count, kLocalThreadsShared, kLocalSmem, s>>>(
                 b.nets, b.win_prefix, b.n_nets, b.windows_total, b.local_scratch);
         else
             push_local_kernel<WT, kLocalThreadsShared><<<b.sm_count, kLocalThreadsShared, kLocalSmem, s>>>(
@@ -1533,6 +1541,9 @@ static cudaError_t push_prepare_wt(const PushCfg& cfg, int sm_count, uint32_t* c
             e = cudaFuncSetAttribute(push_local_kernel<WT, kLocalThreadsShared2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(kLocalSmem));
         if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(push_local_kernel<WT, kLocalThreadsShared, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kLocalSmem));
+        if (e == cudaSuccess)
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.lpr == 16 ? push_kernel<ACC, WT, 8, 16, 1> : push_kernel<ACC, WT, 8, 32, 1>,
                                                               kPushThreads, 0);
     } else if (cfg.kind == PUSH_REG || cfg.kind == PUSH_LOCAL) {
@@ -1577,7 +1588,8 @@ const PushCfg kPushCands[kPushCandidates] = {{PUSH_REG, 4, 32}, {PUSH_REG, 8, 32
                                              {PUSH_REG, 8, 16}, {PUSH_REG, 8, 8},
                                              {PUSH_TMA, 256, 32}, {PUSH_TMA, 512, 32},
                                              {PUSH_LOCAL, 8, 32}, {PUSH_LOCAL, 8, 16},
-                                             {PUSH_LOCAL, kLocalConcurrent, 32}, {PUSH_LOCAL, kLocalConcurrent2, 32}};
+                                             {PUSH_LOCAL, kLocalConcurrent, 32}, {PUSH_LOCAL, kLocalConcurrent2, 32},
+                                             {PUSH_LOCAL, kLocalConcurrentHalf, 32}};
 
 cudaError_t push_prepare(int exact, int wt, const PushCfg& cfg, int sm_count, uint32_t* ctas) {
     if (exact) {

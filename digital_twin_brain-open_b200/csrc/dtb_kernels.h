@@ -41,9 +41,10 @@ struct PushCfg {
 };
 
 // Every variant the autotuner times.
-constexpr int kPushCandidates = 11;
+constexpr int kPushCandidates = 12;
 constexpr int kLocalConcurrent = 2008;   // PUSH_LOCAL param: cross-population part on a second stream
 constexpr int kLocalConcurrent2 = 2016;  // ... with two push CTAs per SM beside a 512-thread window CTA
+constexpr int kLocalConcurrentHalf = 3008;  // ... as 2008 with half-warp rows in the window kernel (short spans)
 extern const PushCfg kPushCands[kPushCandidates];
 // Sets kernel attributes and returns the persistent grid (max resident CTAs).
 cudaError_t push_prepare(int exact, int weight_type, const PushCfg& cfg, int sm_count, uint32_t* ctas);

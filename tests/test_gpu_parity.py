@@ -363,7 +363,7 @@ def test_autotuner_picks_a_variant(gpu):
         assert r.freqs[-200:].sum() > 0.005 * 200 * spec.n
         rep = eng.tuning_report()
         assert eng.info().local_windows > 0
-        assert len(rep) == 11 and all(ms > 0 for _, _, ms in rep)
+        assert len(rep) == 12 and all(ms > 0 for _, _, ms in rep)
         inf = eng.info()
         assert min(ms for _, _, ms in rep) == pytest.approx(inf.push_tuned_ms)
 
@@ -459,7 +459,7 @@ def test_local_push_step_matches_exact_push(gpu, wt):
         r0 = eng.run(1, record_spikes=True, syn_mode=E.SYN_PUSH_EXACT)
         v_ref, j_ref = eng.read_state(E.STATE_V), eng.read_state(E.STATE_J)
         assert r0.spikes.sum() > 0.0005 * spec.n
-        for variant in ((E.PUSH_LOCAL, 8), (E.PUSH_LOCAL, 1016), (E.PUSH_LOCAL, 2008), (E.PUSH_LOCAL, 2016), (E.PUSH_REG, 8)):
+        for variant in ((E.PUSH_LOCAL, 8), (E.PUSH_LOCAL, 1016), (E.PUSH_LOCAL, 2008), (E.PUSH_LOCAL, 2016), (E.PUSH_LOCAL, 3008), (E.PUSH_REG, 8)):
             eng.load_state(blob)
             eng.set_push_variant(*variant)
             r = eng.run(1, record_spikes=True, syn_mode=E.SYN_PUSH)
