@@ -186,6 +186,14 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
     const int wt = static_cast<int>(wtype);
     uint64_t tune_at = ~0ull;
     if (rq.syn_mode != DTB_SYN_PULL) {
+        if (autotune) {
+            uint64_t total = 0;
+            for (Engine* e : m) total += e->n_pad;
+            size_class = 64u - static_cast<uint32_t>(__builtin_clzll(total | 1ull));
+            const auto it = tuned_by_size[exact].find(size_class);
+            push_tuned[exact] = it != tuned_by_size[exact].end();
+            if (push_tuned[exact]) push_cfg = it->second;
+        }
         DTB_CU(push_prepare(exact, wt, push_cfg, sm_count, &push_ctas));
         if (autotune && !push_tuned[exact]) {
             const uint64_t settle = 300;
@@ -254,6 +262,7 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
                     if (tune.tuned) {
                         push_cfg = tune.best;
                         push_tuned[exact] = true;
+                        tuned_by_size[exact][size_class] = push_cfg;
                         DTB_CU(push_prepare(exact, wt, push_cfg, sm_count, &push_ctas));
                     } else {
                         tune_at += 50;
@@ -354,6 +363,8 @@ int32_t dtb_batch_set_push_variant(void* batch, int32_t kind, int32_t param) {
     if (kind < 0) {
         b->autotune = true;
         b->push_tuned[0] = b->push_tuned[1] = false;
+        b->tuned_by_size[0].clear();
+        b->tuned_by_size[1].clear();
         return DTB_OK;
     }
     dtb::PushCfg cfg;

@@ -1,6 +1,7 @@
 // The batched form: several engines advanced by one launch of each per-step kernel.
 #pragma once
 
+#include <map>
 #include <vector>
 
 #include "dtb_engine.h"
@@ -36,6 +37,10 @@ public:
     uint32_t push_ctas = 0;
     bool push_tuned[2] = {false, false};
     bool autotune = true;
+    // tuned variant per size class (bit length of the batch's padded neuron count), so a
+    // serving batch whose membership changes keeps a variant fit for its current size
+    std::map<uint32_t, PushCfg> tuned_by_size[2];
+    uint32_t size_class = 0;
     TuneResult tune;
     bool use_graph = true;
     cudaGraphExec_t graph = nullptr;

@@ -95,6 +95,7 @@ int Server::build(ServedNet& sn) {
         delete e;
         return st;
     }
+    e->autotune = o.autotune != 0;     // plain-path runs tune (or not) like the batch
     sn.eng = e;
     sn.bytes = e->dev_bytes;
     resident_bytes += sn.bytes;
