@@ -23,7 +23,8 @@ Batch::~Batch() {
     if (stream) cudaStreamSynchronize(stream);
     if (graph) cudaGraphExecDestroy(graph);
     for (void* p : {static_cast<void*>(d_views), static_cast<void*>(d_prefix), static_cast<void*>(list),
-                    static_cast<void*>(list_count), static_cast<void*>(list_ticket), static_cast<void*>(local_scratch)})
+                    static_cast<void*>(list_count), static_cast<void*>(list_ticket), static_cast<void*>(local_scratch),
+                    static_cast<void*>(tile_net)})
         if (p) cudaFree(p);
     for (cudaEvent_t e : {ev0, ev1, tev[0], tev[1], ev_fork, ev_join})
         if (e) cudaEventDestroy(e);
@@ -86,6 +87,16 @@ int Batch::set_members(Engine* const* engines, uint32_t n) {
         cap_neurons = total;
     }
     const uint32_t windows = pre[3 * (n + 1) + n];
+    std::vector<uint32_t> tnet(pre[n]);
+    for (uint32_t i = 0; i < n; ++i)
+        for (uint32_t t = pre[i]; t < pre[i + 1]; ++t) tnet[t] = i;
+    if (pre[n] > cap_tiles) {
+        if (tile_net) cudaFree(tile_net);
+        tile_net = nullptr;
+        DTB_CU(cudaMalloc(reinterpret_cast<void**>(&tile_net), sizeof(uint32_t) * std::max<uint32_t>(pre[n], 1u)));
+        cap_tiles = pre[n];
+    }
+    if (pre[n]) DTB_CU(cudaMemcpyAsync(tile_net, tnet.data(), sizeof(uint32_t) * pre[n], cudaMemcpyHostToDevice, stream));
     if (windows > cap_windows) {
         if (local_scratch) cudaFree(local_scratch);
         local_scratch = nullptr;
@@ -109,6 +120,7 @@ int Batch::set_members(Engine* const* engines, uint32_t n) {
     lb.push_ctas = static_cast<uint32_t>(sm_count) * 8u;
     lb.lif_ctas = static_cast<uint32_t>(sm_count) * m[0]->lif_ctas_per_sm;
     lb.spikes = SpikeList{list, list_count, list_ticket, static_cast<uint32_t>(total)};
+    lb.tile_net = tile_net;
     lb.win_prefix = d_prefix + 3 * (n + 1);
     lb.windows_total = windows;
     lb.local_scratch = local_scratch;

@@ -31,6 +31,8 @@ public:
     uint32_t cap_members = 0;         // capacity of d_views / d_prefix
     uint64_t cap_neurons = 0;         // capacity of the spike list
     uint32_t* local_scratch = nullptr;
+    uint32_t* tile_net = nullptr;     // network of every LIF tile
+    uint32_t cap_tiles = 0;
     uint32_t cap_windows = 0;         // capacity of local_scratch (windows)
     LaunchBatch lb{};
     PushCfg push_cfg{PUSH_REG, 8, 32};

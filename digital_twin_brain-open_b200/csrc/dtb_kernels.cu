@@ -244,9 +244,17 @@ __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.w
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 // thread 0: issue the copies of tile `gt` into stage `stg`
+// Network of a batch tile: one load from the tile table when the batch has one.
+__device__ __forceinline__ uint32_t tile_to_net(const uint32_t* __restrict__ tile_net, const uint32_t* __restrict__ tile_prefix,
+                                                uint32_t n_nets, uint32_t gt) {
+    if (n_nets <= 1) return 0u;
+    return tile_net ? __ldg(tile_net + gt) : find_net(tile_prefix, n_nets, gt);
+}
+
 __device__ __forceinline__ void lif_prefetch(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_prefix,
-                                             uint32_t n_nets, uint32_t gt, float* stage, uint64_t* bar) {
-    const uint32_t net = n_nets > 1 ? find_net(tile_prefix, n_nets, gt) : 0u;
+                                             const uint32_t* __restrict__ tile_net, uint32_t n_nets, uint32_t gt,
+                                             float* stage, uint64_t* bar) {
+    const uint32_t net = tile_to_net(tile_net, tile_prefix, n_nets, gt);
     const NetView* nv = nets + net;
     const size_t first = static_cast<size_t>(gt - __ldg(tile_prefix + net)) * kLifTile;
     mbar_expect_tx(bar, static_cast<uint32_t>(kLifStageFloats * sizeof(float)));
@@ -272,7 +280,7 @@ template <int JM>
 __global__ void __launch_bounds__(kLifThreads, 3)
 lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_prefix,
            const uint32_t* __restrict__ vbase, uint32_t n_nets, uint32_t total_tiles, SpikeList sl, uint32_t flags,
-           int prop_mode) {
+           int prop_mode, const uint32_t* __restrict__ tile_net) {
     extern __shared__ __align__(128) float lsm[];
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ int s_cnt[kStatSlots];
@@ -298,13 +306,13 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (blockIdx.x < total_tiles) lif_prefetch(nets, tile_prefix, n_nets, blockIdx.x, lsm, &s_bar[0]);
+        if (blockIdx.x < total_tiles) lif_prefetch(nets, tile_prefix, tile_net, n_nets, blockIdx.x, lsm, &s_bar[0]);
     }
     __syncthreads();
 
     uint32_t it = 0;
     for (uint32_t gt = blockIdx.x; gt < total_tiles; gt += gridDim.x, ++it) {
-        const uint32_t net = n_nets > 1 ? find_net(tile_prefix, n_nets, gt) : 0u;
+        const uint32_t net = tile_to_net(tile_net, tile_prefix, n_nets, gt);
         const uint32_t stg = it & 1u;
         if (net != cur_net) {
             // hand in the previous network's tiles (views are read through the
@@ -327,7 +335,7 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
         // store has been issued; refill it with the tile after this one
         if (tid == 0 && gt + gridDim.x < total_tiles) {
             bulk_wait_read();
-            lif_prefetch(nets, tile_prefix, n_nets, gt + gridDim.x, lsm + (stg ^ 1u) * kLifStageFloats, &s_bar[stg ^ 1u]);
+            lif_prefetch(nets, tile_prefix, tile_net, n_nets, gt + gridDim.x, lsm + (stg ^ 1u) * kLifStageFloats, &s_bar[stg ^ 1u]);
         }
         __syncthreads();
         const NetView& nv = nets[net];
@@ -1453,9 +1461,9 @@ cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop
     const dim3 grid(std::min(b.lif_tiles_total, b.lif_ctas)), block(kLifThreads);
     const uint32_t T = b.lif_tiles_total;
     switch (jmode) {
-        case J_DIRECT: lif_kernel<J_DIRECT><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode); break;
-        case J_FOLD: lif_kernel<J_FOLD><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode); break;
-        default: lif_kernel<J_ASIS><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode); break;
+        case J_DIRECT: lif_kernel<J_DIRECT><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net); break;
+        case J_FOLD: lif_kernel<J_FOLD><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net); break;
+        default: lif_kernel<J_ASIS><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net); break;
     }
     return cudaGetLastError();
 }

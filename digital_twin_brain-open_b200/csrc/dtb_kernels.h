@@ -12,6 +12,7 @@ namespace dtb {
 struct LaunchBatch {
     const NetView* nets;          // device array [n_nets]
     const uint32_t* lif_prefix;   // device [n_nets + 1] cumulative LIF tiles (1024 neurons)
+    const uint32_t* tile_net;     // device [lif tiles] network of every LIF tile (batches), or null
     const uint32_t* pull_prefix;  // device [n_nets + 1] cumulative pull tiles (256 neurons)
     const uint32_t* vbase;        // device [n_nets + 1] cumulative padded neuron counts
     uint32_t n_nets;
