@@ -494,9 +494,9 @@ def run_serve(args):
         ou = (rng.uniform(0.55, 0.65, P).astype(np.float32), rng.uniform(0.18, 0.22, P).astype(np.float32),
               np.full(P, 10.0, np.float32))
         reqs.append(dict(net=net, iters=args.window, arrival_s=t, ou=ou))
-    # warm-up past step 300 on every network, so each engine (plain path) and the batch (batched path)
-    # has autotuned its push before the timed trace
-    warm = [dict(net=i, iters=400, arrival_s=0.0, ou=None) for i in range(len(specs))]
+    # warm-up past step 300 plus the tuner's samples (every 47 steps) on every network, so each
+    # engine (plain path) and the batch (batched path) has autotuned its push before the timed trace
+    warm = [dict(net=i, iters=600, arrival_s=0.0, ou=None) for i in range(len(specs))]
 
     def serve(wt, policy):
         t0 = time.perf_counter()

@@ -270,14 +270,19 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
                 if (tune_at == done + s) {
                     std::vector<NetView> v(m.size());
                     for (size_t i = 0; i < m.size(); ++i) v[i] = m[i]->view;
+                    if (tune_class != (size_class << 1 | static_cast<uint32_t>(exact))) {
+                        tune.reset();       // samples of another membership size or mode do not carry over
+                        tune_class = size_class << 1 | static_cast<uint32_t>(exact);
+                    }
                     DTB_TRY(tune_push_views(lb, v, exact, wt, sm_count, stream, tev, tune));
                     if (tune.tuned) {
                         push_cfg = tune.best;
                         push_tuned[exact] = true;
                         tuned_by_size[exact][size_class] = push_cfg;
+                        tune.reset();
                         DTB_CU(push_prepare(exact, wt, push_cfg, sm_count, &push_ctas));
                     } else {
-                        tune_at += 50;
+                        tune_at = tune.next_step(tune_at);
                     }
                 }
                 DTB_CU(launch_push(lb, exact, wt, push_cfg, push_ctas, stream));
@@ -375,6 +380,7 @@ int32_t dtb_batch_set_push_variant(void* batch, int32_t kind, int32_t param) {
     if (kind < 0) {
         b->autotune = true;
         b->push_tuned[0] = b->push_tuned[1] = false;
+        b->tune.reset();
         b->tuned_by_size[0].clear();
         b->tuned_by_size[1].clear();
         return DTB_OK;

@@ -43,7 +43,8 @@ public:
     // serving batch whose membership changes keeps a variant fit for its current size
     std::map<uint32_t, PushCfg> tuned_by_size[2];
     uint32_t size_class = 0;
-    TuneResult tune;
+    TuneResult tune;                      // samples of the size class being tuned
+    uint32_t tune_class = ~0u;            // that class (size class << 1 | exact)
     bool use_graph = true;
     cudaGraphExec_t graph = nullptr;
     uint64_t graph_key[6] = {0, 0, 0, 0, 0, 0};

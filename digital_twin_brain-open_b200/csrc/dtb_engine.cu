@@ -880,7 +880,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
                     DTB_TRY(timed_launch(0, [&] { return launch_lif(b, J_DIRECT, kflags, pm, stream); }));
                     if (tune_at == done + s) {
                         DTB_TRY(tune_push(b, 0));
-                        if (!push_tuned[0]) tune_at += 50;   // still quiet: retry later in this run
+                        if (!push_tuned[0]) tune_at = tune_acc[0].next_step(tune_at);
                     }
                     DTB_TRY(timed_launch(1, [&] { return launch_push(b, 0, static_cast<int>(wtype), push_cfg, push_ctas, stream); }));
                     launches += push_extra_launches(b, 0, push_cfg);
@@ -890,7 +890,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
                     DTB_TRY(timed_launch(0, [&] { return launch_lif(b, first ? J_ASIS : J_FOLD, kflags, pm, stream); }));
                     if (tune_at == done + s) {
                         DTB_TRY(tune_push(b, 1));
-                        if (!push_tuned[1]) tune_at += 50;
+                        if (!push_tuned[1]) tune_at = tune_acc[1].next_step(tune_at);
                     }
                     DTB_TRY(timed_launch(1, [&] { return launch_push(b, 1, static_cast<int>(wtype), push_cfg, push_ctas, stream); }));
                     if (isyn_any) DTB_TRY(timed_launch(3, [&] { return launch_stat_isyn(b, 1, sm_count, stream); }));
@@ -949,14 +949,17 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
 // fastest.  `views` are the host copies of the launch's networks.
 int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int exact, int wtype, int sm_count,
                     cudaStream_t stream, cudaEvent_t ev[2], TuneResult& res) {
-    res.tuned = false;
-    res.report.clear();
     uint32_t count = 0;
     DTB_CU(cudaMemcpyAsync(&count, b.spikes.count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     DTB_CU(cudaStreamSynchronize(stream));
     uint64_t total_n = 0;
     for (const NetView& v : views) total_n += v.n_pad;
-    if (count < std::max<uint64_t>(64u, total_n / 500u)) return DTB_OK;   // too quiet to be representative
+    res.sampled = false;
+    ++res.observed;
+    res.peak = std::max(res.peak, count);
+    if (res.observed <= kTuneObserve || count < res.peak / 2 || count < std::max<uint64_t>(64u, total_n / 500u))
+        return DTB_OK;
+    res.sampled = true;
     const size_t per = exact ? sizeof(long long) * 4 : sizeof(float4);
     void* scratch = nullptr;
     NetView* tview = nullptr;
@@ -972,7 +975,7 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
         if (exact) v.dJ = reinterpret_cast<long long*>(base); else v.J = reinterpret_cast<float4*>(base);
         off += v.n_pad;
     }
-    float best_ms = 1e30f;
+    std::vector<TuneEntry> step;
     auto body = [&]() -> int {
         DTB_CU(cudaMemcpyAsync(tview, tv.data(), sizeof(NetView) * tv.size(), cudaMemcpyHostToDevice, stream));
         DTB_CU(cudaMemsetAsync(scratch, 0, per * total_n, stream));
@@ -993,8 +996,7 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
                 DTB_CU(cudaEventElapsedTime(&ms, ev[0], ev[1]));
                 ms_min = std::min(ms_min, ms);
             }
-            res.report.push_back({c, ms_min});
-            if (ms_min < best_ms) { best_ms = ms_min; res.best = c; }
+            step.push_back({c, ms_min});
         }
         set_u32_kernel<<<1, 1, 0, stream>>>(b.spikes.count, count);
         DTB_CU(cudaGetLastError());
@@ -1005,8 +1007,20 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
     cudaFree(scratch);
     cudaFree(tview);
     if (st != DTB_OK) return st;
+    // running mean per variant over the samples
+    if (res.report.size() != step.size()) {
+        res.report = step;
+        res.samples = 1;
+    } else {
+        ++res.samples;
+        for (size_t k = 0; k < step.size(); ++k)
+            res.report[k].ms += (step[k].ms - res.report[k].ms) / static_cast<float>(res.samples);
+    }
+    if (res.samples < kTuneSamples) return DTB_OK;
     res.tuned = true;
-    res.best_ms = best_ms;
+    res.best_ms = 1e30f;
+    for (const TuneEntry& t : res.report)
+        if (t.ms < res.best_ms) { res.best_ms = t.ms; res.best = t.cfg; }
     return DTB_OK;
 }
 
@@ -1015,7 +1029,7 @@ int Engine::tune_push(const LaunchBatch& b, int exact) {
         DTB_CU(cudaEventCreate(&tune_ev[0]));
         DTB_CU(cudaEventCreate(&tune_ev[1]));
     }
-    TuneResult res;
+    TuneResult& res = tune_acc[exact];
     DTB_TRY(tune_push_views(b, {view}, exact, static_cast<int>(wtype), sm_count, stream, tune_ev, res));
     if (!res.tuned) return DTB_OK;
     push_cfg = res.best;
@@ -1472,6 +1486,8 @@ int32_t dtb_set_push_variant(void* engine, int32_t kind, int32_t param) {
     if (kind < 0) {
         e->autotune = true;
         e->push_tuned[0] = e->push_tuned[1] = false;
+        e->tune_acc[0].reset();
+        e->tune_acc[1].reset();
         return DTB_OK;
     }
     dtb::PushCfg cfg;

@@ -22,15 +22,33 @@ int cuda_fail(cudaError_t e, const char* what);
 #define DTB_TRY(x) do { int s__ = (x); if (s__ != DTB_OK) return s__; } while (0)
 
 struct TuneEntry { PushCfg cfg; float ms; };
+// Push-variant tuning state.  The tuner reads the spike count of every step for
+// kTuneObserve steps to learn the network's peak activity, then times every variant
+// on kTuneSamples live spike lists of at least half that peak, kTuneStride or more
+// steps apart; `best` is the variant with the smallest mean.  Bursting networks spend
+// most of their push time in their bursts, which a fixed sampling step can miss.
+constexpr uint32_t kTuneObserve = 50;
+constexpr uint32_t kTuneSamples = 4;
+constexpr uint64_t kTuneStride = 47;
 struct TuneResult {
     bool tuned = false;
+    bool sampled = false;            // the last call timed the variants
     PushCfg best{PUSH_REG, 8, 32};
-    float best_ms = 0.0f;
-    std::vector<TuneEntry> report;
+    float best_ms = 0.0f;            // mean per sampled step of the best variant
+    uint32_t samples = 0;
+    uint32_t observed = 0;           // steps whose spike count was read
+    uint32_t peak = 0;               // largest spike count seen
+    std::vector<TuneEntry> report;   // per variant: mean time per sampled step
+    void reset() { tuned = sampled = false; samples = observed = peak = 0; report.clear(); }
+    // run-relative step of the next call after one at step `s`
+    uint64_t next_step(uint64_t s) const { return s + (sampled ? kTuneStride : 1); }
 };
 bool push_cfg_from_abi(int kind, int param, PushCfg& cfg);
 __global__ void set_u64_kernel(unsigned long long* p, unsigned long long v);
 __global__ void set_u32_kernel(uint32_t* p, uint32_t v);
+// Reads the live spike count and, when the step qualifies as a sample (TuneResult),
+// times every push variant on it and adds the times to `res`.  A list of fewer than
+// 0.2 % of the neurons never qualifies.
 int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int exact, int wtype, int sm_count,
                     cudaStream_t stream, cudaEvent_t ev[2], TuneResult& res);
 
@@ -162,6 +180,7 @@ public:
     uint32_t push_ctas = 0;
     bool autotune = true;
     bool push_tuned[2] = {false, false};
+    TuneResult tune_acc[2];               // samples gathered so far (float push, exact push)
     float tuned_ms = 0.0f;
     std::vector<TuneEntry> tune_report;
     int tune_push(const LaunchBatch& b, int exact);

@@ -54,16 +54,6 @@ __device__ inline void load_netview(NetView& dst, const NetView* __restrict__ sr
     for (int w = threadIdx.x; w < static_cast<int>(sizeof(NetView) / 4); w += blockDim.x) d[w] = s[w];
 }
 
-// 4-bit nibble of lane l covers neurons 4l..4l+3 of the warp's 128; gather the
-// 32-bit word of neurons 32w..32w+31 (lanes 8w..8w+7) into every lane of the group.
-__device__ inline uint32_t nibbles_to_word(uint32_t nib, int lane) {
-    uint32_t x = nib << (4 * (lane & 7));
-    x |= __shfl_xor_sync(0xffffffffu, x, 1);
-    x |= __shfl_xor_sync(0xffffffffu, x, 2);
-    x |= __shfl_xor_sync(0xffffffffu, x, 4);
-    return x;
-}
-
 __device__ inline long long warp_sum_ll(long long v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -76,18 +66,29 @@ __device__ inline unsigned long long warp_sum_ull(unsigned long long v) {
     return v;
 }
 
-// Normal draws (OU) and uniforms (noise train) for 4 consecutive neurons.
-__device__ inline void draw_noise(const NetView& nv, uint32_t i0, unsigned long long n, unsigned long long inj_base,
-                                  bool injected, bool need_u, float z[4], float u[4], uint32_t& err) {
+// Neuron slots of a LIF tile: thread `slot` of the tile's CTA steps neurons
+// tile_first + slot + kLifThreads * k (k = 0..3), so each step of k touches 32
+// consecutive neurons per warp.  One Philox4x32-10 block per (slot, step) gives
+// the four draws of the slot's neurons: counter (tile_first / 4 + slot, step,
+// stream); draw k belongs to neuron tile_first + slot + kLifThreads * k.
+constexpr uint32_t kSlotsPerTile = kLifThreads;
+static_assert(kLifTile == 4 * kLifThreads, "a LIF thread steps four neurons");
+
+// Normal draws (OU) and uniforms (noise train) for the four neurons of a slot.
+__device__ inline void draw_noise(const NetView& nv, uint32_t tile_first, uint32_t slot, unsigned long long n,
+                                  unsigned long long inj_base, bool injected, bool need_u, float z[4], float u[4],
+                                  uint32_t& err) {
     if (injected) {
         const unsigned long long row = n - inj_base - 1;
         if (row < nv.inj_rows && nv.inj_z != nullptr) {
-            const float4 zz = __ldcs(reinterpret_cast<const float4*>(nv.inj_z + row * nv.n_pad + i0));
-            z[0] = zz.x; z[1] = zz.y; z[2] = zz.z; z[3] = zz.w;
+            const float* zr = nv.inj_z + row * nv.n_pad + tile_first + slot;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) z[k] = __ldcs(zr + kSlotsPerTile * k);
             if (need_u) {
                 if (nv.inj_u != nullptr) {
-                    const float4 uu = __ldcs(reinterpret_cast<const float4*>(nv.inj_u + row * nv.n_pad + i0));
-                    u[0] = uu.x; u[1] = uu.y; u[2] = uu.z; u[3] = uu.w;
+                    const float* ur = nv.inj_u + row * nv.n_pad + tile_first + slot;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) u[k] = __ldcs(ur + kSlotsPerTile * k);
                 } else {
                     u[0] = u[1] = u[2] = u[3] = 1.0f;
                     err |= kErrNoiseExhausted;
@@ -100,11 +101,12 @@ __device__ inline void draw_noise(const NetView& nv, uint32_t i0, unsigned long 
         }
     } else {
         const uint32_t k0 = static_cast<uint32_t>(nv.seed), k1 = static_cast<uint32_t>(nv.seed >> 32);
-        const U4 r = philox4x32_10(U4{i0 >> 2, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamOU}, k0, k1);
+        const uint32_t ctr = (tile_first >> 2) + slot;
+        const U4 r = philox4x32_10(U4{ctr, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamOU}, k0, k1);
         box_muller(r.x, r.y, z[0], z[1]);
         box_muller(r.z, r.w, z[2], z[3]);
         if (need_u) {
-            const U4 q = philox4x32_10(U4{i0 >> 2, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamNoise}, k0, k1);
+            const U4 q = philox4x32_10(U4{ctr, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamNoise}, k0, k1);
             u[0] = u01(q.x); u[1] = u01(q.y); u[2] = u01(q.z); u[3] = u01(q.w);
         }
     }
@@ -112,7 +114,7 @@ __device__ inline void draw_noise(const NetView& nv, uint32_t i0, unsigned long 
 
 __device__ inline void draw_noise1(const NetView& nv, uint32_t i, unsigned long long n, unsigned long long inj_base,
                                    bool injected, bool need_u, float& z, float& u, uint32_t& err) {
-    // one neuron: same streams as draw_noise (the neuron's slot of its quad)
+    // one neuron: same streams as draw_noise (draw k of its slot)
     if (injected) {
         const unsigned long long row = n - inj_base - 1;
         if (row < nv.inj_rows && nv.inj_z != nullptr) {
@@ -126,15 +128,17 @@ __device__ inline void draw_noise1(const NetView& nv, uint32_t i, unsigned long 
         }
     } else {
         const uint32_t k0 = static_cast<uint32_t>(nv.seed), k1 = static_cast<uint32_t>(nv.seed >> 32);
-        const U4 r = philox4x32_10(U4{i >> 2, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamOU}, k0, k1);
+        const uint32_t w = i % kLifTile, k = w / kSlotsPerTile;
+        const uint32_t ctr = ((i - w) >> 2) + w % kSlotsPerTile;
+        const U4 r = philox4x32_10(U4{ctr, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamOU}, k0, k1);
         float z4[4];
         box_muller(r.x, r.y, z4[0], z4[1]);
         box_muller(r.z, r.w, z4[2], z4[3]);
-        z = z4[i & 3];
+        z = z4[k];
         if (need_u) {
-            const U4 q = philox4x32_10(U4{i >> 2, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamNoise}, k0, k1);
+            const U4 q = philox4x32_10(U4{ctr, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamNoise}, k0, k1);
             const uint32_t qq[4] = {q.x, q.y, q.z, q.w};
-            u = u01(qq[i & 3]);
+            u = u01(qq[k]);
         }
     }
 }
@@ -166,6 +170,22 @@ __device__ inline void stat_add(const NetView& nv, const StatAcc& sa, long long 
         const size_t o = static_cast<size_t>(row) * nv.n_pops + p;
         if (c) atomicAdd(nv.hist_cnt + o, c);
         atomicAdd(reinterpret_cast<unsigned long long*>(nv.hist_vsum + o), static_cast<unsigned long long>(v));
+    }
+}
+
+// Warp-collective: lanes holding (pop, count, V sum) with `has` add their sums per
+// distinct pop, one shared-slot (or global) update per pop.
+__device__ inline void warp_stat_segments(const NetView& nv, const StatAcc& sa, long long row, uint32_t pop, bool has,
+                                          int cnt, long long vs, uint32_t lane) {
+    uint32_t rem = __ballot_sync(0xffffffffu, has);
+    while (rem) {
+        const uint32_t leader = static_cast<uint32_t>(__ffs(rem) - 1);
+        const uint32_t pk = __shfl_sync(0xffffffffu, pop, leader);
+        const bool in = ((rem >> lane) & 1u) && pop == pk;
+        const int c = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(in ? cnt : 0));
+        const long long v = warp_sum_ll(in ? vs : 0ll);
+        if (lane == leader) stat_add(nv, sa, row, pk, c, v);
+        rem &= ~__ballot_sync(0xffffffffu, in);
     }
 }
 
@@ -341,7 +361,7 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
         const NetView& nv = nets[net];
         const uint32_t tile = gt - __ldg(tile_prefix + net);
         const uint32_t tile_first = tile * kLifTile;
-        const uint32_t i0 = tile_first + tid * 4;
+        const uint32_t i0 = tile_first + tid;             // this thread: neurons i0 + kSlotsPerTile * k
         const float t_prev = nv.clock->t;
         const unsigned long long n_prev = nv.clock->n;
         const unsigned long long run_base = nv.clock->run_base;
@@ -357,116 +377,134 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
         if ((stats || record) && (row < 0 || row >= static_cast<long long>(nv.hist_cap))) {
             stats = false; record = false; err |= kErrHistOverflow;
         }
+        const bool sample = (flags & kFlagSample) && nv.n_samples && row >= 0 && row < static_cast<long long>(nv.hist_cap);
         StatAcc sa{s_cnt, s_vs, p_tile};
         float z[4], u[4] = {1.f, 1.f, 1.f, 1.f};
-        draw_noise(nv, i0, n, inj_base, injected, need_u, z, u, err);
-        longlong2* dq = reinterpret_cast<longlong2*>(nv.dJ + static_cast<size_t>(i0) * 4);   // J_FOLD: this quad's sums
+        draw_noise(nv, tile_first, tid, n, inj_base, injected, need_u, z, u, err);
         if (!mbar_wait_bounded(&s_bar[stg], (it >> 1) & 1u)) {
             late = 1;
             mbar_wait_bounded(&s_bar[stg], (it >> 1) & 1u);
         }
         if (late) err |= kErrTimeout;
+        // stage accesses: each step of k reads and writes 32 consecutive neurons
+        // per warp, so every shared-memory access is free of bank conflicts
         float* st = lsm + stg * kLifStageFloats;
-        float* sV = st + tid * 4;
-        float* sI = st + kLifTile + tid * 4;
-        float* sT = st + 2 * kLifTile + tid * 4;
-        float4* sJ = reinterpret_cast<float4*>(st + 3 * kLifTile) + tid * 4;
+        float* sV = st + tid;
+        float* sI = st + kLifTile + tid;
+        float* sT = st + 2 * kLifTile + tid;
+        float4* sJ = reinterpret_cast<float4*>(st + 3 * kLifTile) + tid;
 
         uint32_t nib_prop = 0, nib_act = 0;
-        unsigned long long ev = 0;
+        uint32_t ev = 0;                   // out-degrees of this thread's (at most four) spiking neurons
         uint32_t p = p_tile;
         const uint32_t i_first = min(i0, nv.n - 1);
         while (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i_first) ++p;
         const uint32_t p_first = p;
         bool uniform = true;
-        int cnt_acc = 0;
-        long long vs_acc = 0;
-        float v_out[4], i_out[4];
+        int cnt_acc = 0, cnt_nxt = 0;          // neurons of p_first, and of p_first + 1
+        long long vs_acc = 0, vs_nxt = 0;
         PopParams pp;
         load_pop_params(nv, p, i_first, pp);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            const uint32_t i = i0 + k;
-            if (i >= nv.n) { uniform = false; v_out[k] = 0.f; i_out[k] = 0.f; continue; }
+            const uint32_t i = i0 + kSlotsPerTile * k;
+            if (i >= nv.n) { uniform = false; continue; }
             if (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) {
                 while (p + 1 < nv.n_pops && __ldg(nv.pop_off + p + 1) <= i) ++p;
                 uniform = false;
                 if (!nv.per_neuron) load_pop_params(nv, p, i, pp);
             }
             if (nv.per_neuron && k > 0) load_pop_params(nv, p, i, pp);
-            const float4 Jk = sJ[k];
+            const int ks = kSlotsPerTile * k;
+            const float4 Jk = sJ[ks];
             NeuronIn in;
-            in.V = sV[k];
-            in.iou = sI[k];
-            in.tlast = sT[k];
+            in.V = sV[ks];
+            in.iou = sI[ks];
+            in.tlast = sT[ks];
             if constexpr (JM == J_FOLD) {
-                const longlong2 d01 = dq[2 * k], d23 = dq[2 * k + 1];
+                longlong2* dq = reinterpret_cast<longlong2*>(nv.dJ + static_cast<size_t>(i) * 4);
+                const longlong2 d01 = dq[0], d23 = dq[1];
                 in.J[0] = decay_add(Jk.x, pp.decay[0], fix_to_float(d01.x));
                 in.J[1] = decay_add(Jk.y, pp.decay[1], fix_to_float(d01.y));
                 in.J[2] = decay_add(Jk.z, pp.decay[2], fix_to_float(d23.x));
                 in.J[3] = decay_add(Jk.w, pp.decay[3], fix_to_float(d23.y));
-                dq[2 * k] = make_longlong2(0, 0);
-                dq[2 * k + 1] = make_longlong2(0, 0);
+                dq[0] = make_longlong2(0, 0);
+                dq[1] = make_longlong2(0, 0);
             } else {
                 in.J[0] = Jk.x; in.J[1] = Jk.y; in.J[2] = Jk.z; in.J[3] = Jk.w;
             }
             const NeuronOut o = lif_update(pp, in, t, z[k], use_ou);
-            sV[k] = o.V;
-            sI[k] = o.iou;
-            sT[k] = o.tlast;
-            v_out[k] = o.V;
-            i_out[k] = o.iou;
+            sV[ks] = o.V;
+            sI[ks] = o.iou;
+            sT[ks] = o.tlast;
             if constexpr (JM == J_DIRECT) {
-                sJ[k] = make_float4(__fmul_rn(in.J[0], pp.decay[0]), __fmul_rn(in.J[1], pp.decay[1]),
-                                    __fmul_rn(in.J[2], pp.decay[2]), __fmul_rn(in.J[3], pp.decay[3]));
+                sJ[ks] = make_float4(__fmul_rn(in.J[0], pp.decay[0]), __fmul_rn(in.J[1], pp.decay[1]),
+                                     __fmul_rn(in.J[2], pp.decay[2]), __fmul_rn(in.J[3], pp.decay[3]));
             } else if constexpr (JM == J_FOLD) {
-                sJ[k] = make_float4(in.J[0], in.J[1], in.J[2], in.J[3]);
+                sJ[ks] = make_float4(in.J[0], in.J[1], in.J[2], in.J[3]);
             }
             const bool sp = propagated(prop_mode, o.active, u[k], pp.noise_rate);
             nib_prop |= static_cast<uint32_t>(sp) << k;
             nib_act |= static_cast<uint32_t>(o.active) << k;
             if (sp) ev += __ldg(nv.out_deg + i);
+            // sampled neurons (stat_samples_kernel, src/stage/stat_result.cpp:393-431)
+            if (sample) {
+                const uint32_t sbw = __ldg(nv.sample_bits + (i >> 5)), sh = i & 31u;
+                if ((sbw >> sh) & 1u) {
+                    const size_t so = static_cast<size_t>(row) * nv.n_samples + __ldg(nv.sample_pre + (i >> 5)) +
+                                      __popc(sbw & ((1u << sh) - 1u));
+                    nv.hist_sspk[so] = static_cast<uint8_t>(o.active);
+                    nv.hist_sv[so] = o.V;
+                    nv.hist_siou[so] = o.iou;
+                }
+            }
             if (stats) {
                 if (excluded(nv, i)) { uniform = false; continue; }
                 if (p == p_first) {
                     cnt_acc += o.active;
                     vs_acc += v_fix(o.V);
-                } else {
+                } else if (p == p_first + 1) {
+                    cnt_nxt += o.active;
+                    vs_nxt += v_fix(o.V);
+                } else {                      // a population narrower than a thread's span
                     stat_add(nv, sa, row, p, o.active, v_fix(o.V));
                 }
             }
         }
 
-        // ---- spike bitmaps (propagated: parity buffer; threshold: history row)
+        // ---- spike bitmaps and list: step k of a warp covers one 32-neuron word
+        //      (propagated: parity buffer and one slot range per warp in the list;
+        //      threshold: history row)
         {
-            const uint32_t wprop = nibbles_to_word(nib_prop, lane);
-            const uint32_t wact = nibbles_to_word(nib_act, lane);
-            if ((lane & 7) == 0) {
-                const uint32_t word = (i0 >> 5);
-                uint32_t* bits = parity ? nv.bits1 : nv.bits0;
-                bits[word] = wprop;
-                if (record) nv.rec_bits[static_cast<size_t>(row) * nv.n_words + word] = wact;
+            uint32_t* bits = parity ? nv.bits1 : nv.bits0;
+            const uint32_t word0 = (tile_first >> 5) + (tid >> 5);
+            uint32_t wprop[4], wtotal = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                wprop[k] = __ballot_sync(0xffffffffu, (nib_prop >> k) & 1u);
+                wtotal += __popc(wprop[k]);
+                const uint32_t wact = __ballot_sync(0xffffffffu, (nib_act >> k) & 1u);
+                if (lane == 0) {
+                    const uint32_t word = word0 + (kSlotsPerTile / 32) * k;
+                    bits[word] = wprop[k];
+                    if (record) nv.rec_bits[static_cast<size_t>(row) * nv.n_words + word] = wact;
+                }
             }
-        }
-        // ---- sampled neurons (stat_samples_kernel, src/stage/stat_result.cpp:393-431)
-        if ((flags & kFlagSample) && nv.n_samples && row >= 0 && row < static_cast<long long>(nv.hist_cap)) {
-            const uint32_t word = i0 >> 5, sh = i0 & 31u;
-            const uint32_t sb = (__ldg(nv.sample_bits + word) >> sh) & 0xFu;
-            if (sb) {
-                uint32_t slot = __ldg(nv.sample_pre + word) + __popc(__ldg(nv.sample_bits + word) & ((1u << sh) - 1u));
+            if ((flags & kFlagList) && wtotal) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(sl.count, wtotal);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                const uint32_t below = (1u << lane) - 1u;
+                const uint32_t vb = __ldg(vbase + net) + i0;
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    if ((sb >> k) & 1u) {
-                        const size_t o = static_cast<size_t>(row) * nv.n_samples + slot;
-                        nv.hist_sspk[o] = static_cast<uint8_t>((nib_act >> k) & 1u);
-                        nv.hist_sv[o] = v_out[k];
-                        nv.hist_siou[o] = i_out[k];
-                        ++slot;
-                    }
+                    if ((nib_prop >> k) & 1u) sl.list[base + __popc(wprop[k] & below)] = vb + kSlotsPerTile * k;
+                    base += __popc(wprop[k]);
                 }
             }
         }
-        // ---- population statistics: warp-uniform fast path, else per-thread slots
+        // ---- population statistics: one sum per warp when the warp's neurons share a
+        //      population, else one per (warp, population) by a segmented reduction
         if (stats) {
             const uint32_t pl = __shfl_sync(0xffffffffu, p_first, 0);
             const bool wuni = __all_sync(0xffffffffu, uniform && p_first == pl);
@@ -474,29 +512,9 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
                 const int c = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(cnt_acc));
                 const long long v = warp_sum_ll(vs_acc);
                 if (lane == 0) stat_add(nv, sa, row, pl, c, v);
-            } else if (i0 < nv.n) {
-                stat_add(nv, sa, row, p_first, cnt_acc, vs_acc);
-            }
-        }
-        // ---- spike list (push modes): one slot range per warp, ascending within it
-        const uint32_t my_cnt = __popc(nib_prop);
-        uint32_t incl = my_cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= static_cast<uint32_t>(o)) incl += y;
-        }
-        const uint32_t wtotal = __shfl_sync(0xffffffffu, incl, 31);
-        if ((flags & kFlagList) && wtotal) {
-            uint32_t base = 0;
-            if (lane == 31) base = atomicAdd(sl.count, wtotal);
-            base = __shfl_sync(0xffffffffu, base, 31);
-            if (my_cnt) {
-                uint32_t pos = base + incl - my_cnt;
-                const uint32_t vb = __ldg(vbase + net);
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if ((nib_prop >> k) & 1u) sl.list[pos++] = vb + i0 + k;
+            } else {
+                warp_stat_segments(nv, sa, row, p_first, i0 < nv.n, cnt_acc, vs_acc, lane);
+                warp_stat_segments(nv, sa, row, p_first + 1, cnt_nxt != 0 || vs_nxt != 0, cnt_nxt, vs_nxt, lane);
             }
         }
         const unsigned long long wev = warp_sum_ull(ev);
