@@ -272,6 +272,8 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
                     for (size_t i = 0; i < m.size(); ++i) v[i] = m[i]->view;
                     if (tune_class != (size_class << 1 | static_cast<uint32_t>(exact))) {
                         tune.reset();       // samples of another membership size or mode do not carry over
+                        tune.observe = 0;   // a batch serves requests: tune on the first busy steps
+                        tune.want = 2;
                         tune_class = size_class << 1 | static_cast<uint32_t>(exact);
                     }
                     DTB_TRY(tune_push_views(lb, v, exact, wt, sm_count, stream, tev, tune));

@@ -957,8 +957,17 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
     res.sampled = false;
     ++res.observed;
     res.peak = std::max(res.peak, count);
-    if (res.observed <= kTuneObserve || count < res.peak / 2 || count < std::max<uint64_t>(64u, total_n / 500u))
+    if (res.observed <= res.observe || count < res.peak / 2 || count < std::max<uint64_t>(64u, total_n / 500u)) {
+        if (res.observed >= res.observe + kTuneGiveUp) {
+            // settle: the best of the samples so far, or the default variant
+            res.tuned = true;
+            res.best_ms = 1e30f;
+            for (const TuneEntry& t : res.report)
+                if (t.ms < res.best_ms) { res.best_ms = t.ms; res.best = t.cfg; }
+            if (res.report.empty()) res.best_ms = 0.0f;
+        }
         return DTB_OK;
+    }
     res.sampled = true;
     const size_t per = exact ? sizeof(long long) * 4 : sizeof(float4);
     void* scratch = nullptr;
@@ -1016,7 +1025,7 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
         for (size_t k = 0; k < step.size(); ++k)
             res.report[k].ms += (step[k].ms - res.report[k].ms) / static_cast<float>(res.samples);
     }
-    if (res.samples < kTuneSamples) return DTB_OK;
+    if (res.samples < res.want) return DTB_OK;
     res.tuned = true;
     res.best_ms = 1e30f;
     for (const TuneEntry& t : res.report)

@@ -23,14 +23,20 @@ int cuda_fail(cudaError_t e, const char* what);
 
 struct TuneEntry { PushCfg cfg; float ms; };
 // Push-variant tuning state.  The tuner reads the spike count of every step for
-// kTuneObserve steps to learn the network's peak activity, then times every variant
-// on kTuneSamples live spike lists of at least half that peak, kTuneStride or more
-// steps apart; `best` is the variant with the smallest mean.  Bursting networks spend
-// most of their push time in their bursts, which a fixed sampling step can miss.
-constexpr uint32_t kTuneObserve = 50;
-constexpr uint32_t kTuneSamples = 4;
+// `observe` steps to learn the network's peak activity, then times every variant on
+// `want` live spike lists of at least half that peak, kTuneStride or more steps apart;
+// `best` is the variant with the smallest mean.  Bursting networks spend most of
+// their push time in their bursts, which a fixed sampling step can miss.  A step that
+// does not qualify is retried at the next step for kTuneEager reads, then every
+// kTuneStride steps; after kTuneGiveUp reads the tuner settles for the samples it has
+// (or the default variant) so a quiet network stops paying for the reads.
+constexpr uint32_t kTuneObserve = 50;     // plain engine; a batch uses 0 (latency-sensitive)
+constexpr uint32_t kTuneSamples = 4;      // plain engine; a batch uses 2
 constexpr uint64_t kTuneStride = 47;
+constexpr uint32_t kTuneEager = 200;
+constexpr uint32_t kTuneGiveUp = 400;
 struct TuneResult {
+    uint32_t observe = kTuneObserve, want = kTuneSamples;
     bool tuned = false;
     bool sampled = false;            // the last call timed the variants
     PushCfg best{PUSH_REG, 8, 32};
@@ -41,7 +47,9 @@ struct TuneResult {
     std::vector<TuneEntry> report;   // per variant: mean time per sampled step
     void reset() { tuned = sampled = false; samples = observed = peak = 0; report.clear(); }
     // run-relative step of the next call after one at step `s`
-    uint64_t next_step(uint64_t s) const { return s + (sampled ? kTuneStride : 1); }
+    uint64_t next_step(uint64_t s) const {
+        return s + ((sampled || observed >= observe + kTuneEager) ? kTuneStride : 1);
+    }
 };
 bool push_cfg_from_abi(int kind, int param, PushCfg& cfg);
 __global__ void set_u64_kernel(unsigned long long* p, unsigned long long v);
