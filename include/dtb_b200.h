@@ -210,10 +210,14 @@ int32_t dtb_info(void* engine, dtb_engine_info* info);
  * per lane, or 1000 + lanes per row 16/8 for sub-warp rows), 1 (TMA bulk-copy
  * staged rows, param 256/512 synapses per stage) or 2 (population-local: each
  * row's own-population synapses are summed per window of its population in
- * shared memory, the rest as kind 0; param 8 or 1016; float push mode only,
- * the exact mode runs kind 0 instead);
- * kind < 0 re-enables the autotuner, which times every variant on a live spike
- * list of the first active run and keeps the fastest. */
+ * shared memory, the rest as kind 0; param 8 or 1016, or 2008 / 2016 / 3008 for
+ * the forms that run the rest on a second stream beside the window kernel; float
+ * push mode only, the exact mode runs kind 0 instead);
+ * kind < 0 re-enables the autotuner.  From step 300 it reads the spike count of
+ * every step for 50 steps, then times every variant on the live spike lists of
+ * four steps with at least half the peak count seen (and 0.2 % of the neurons),
+ * 47 or more steps apart, and keeps the variant with the smallest mean; it gives
+ * up (keeping the best so far, or kind 0 param 8) after 400 reads of quiet steps. */
 int32_t dtb_set_push_variant(void* engine, int32_t kind, int32_t param);
 /* The autotuner's last measurement: on entry *n is the capacity of the arrays,
  * on return the number of variants timed (kind, param, push time in ms). */
@@ -293,7 +297,8 @@ typedef struct dtb_server_options {
     uint32_t max_batch;      /* most requests in flight together                                  */
     uint32_t syn_mode;       /* DTB_SYN_* of every run                                            */
     uint32_t flags;          /* DTB_RUN_USE_OU etc.; DTB_RUN_FREQ is always on                    */
-    uint32_t autotune;       /* 1: the batch autotunes its push variant once                      */
+    uint32_t autotune;       /* 1: each engine and the batch autotune their push variant (the batch
+                                once per size class of its membership, on two busy steps)       */
     uint32_t reserved[3];
 } dtb_server_options;
 
