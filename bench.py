@@ -272,10 +272,10 @@ def run_ours(args):
     lif_bytes = info.n_neurons * BYTES_STATE + info.n_neurons / 8
     roof_kernel = PUSH_KERNELS[info.push_kind]
     if syn == E.SYN_PULL:
-        # one fused kernel reads every in-edge's source (4 bytes), tests it in the bitmap, reads the
-        # weight pair of the active ones (B_w bytes per event) and steps the neurons
+        # algorithmic bytes of the pull: every in-edge (4 + B_w bytes), the bitmap and the neuron
+        # state (the kernel itself reads a weight pair only for an edge whose source spiked)
         lif_ms, push_ms = 0.0, rk.kernel_ms[2] / WINDOW
-        push_bytes = info.n_edges * CSR_COL_BYTES + ev_launch * wbytes + info.n_neurons / 8 + lif_bytes
+        push_bytes = info.n_edges * (CSR_COL_BYTES + wbytes) + info.n_neurons / 8 + lif_bytes
         lif_bytes = 0.0
         roof_kernel = "lif_pull_kernel (in-degree gather fused with the LIF step)"
 
