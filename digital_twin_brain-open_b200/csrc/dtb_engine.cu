@@ -944,6 +944,26 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     return DTB_OK;
 }
 
+// The variant to keep: the fastest mean, except that variants within kTuneTie of it
+// count as tied (a few sampled steps do not resolve smaller differences) and the tie
+// goes to the concurrent population-local push, then to list order.  On the regional
+// 5M network local:8 and local:2008 come within 1-3 % of each other on the sampled
+// bursts, while over whole runs local:2008 is 6.6 % faster (push 0.548 vs 0.585 ms).
+constexpr float kTuneTie = 0.02f;
+static void pick_best(TuneResult& res) {
+    if (res.report.empty()) { res.best_ms = 0.0f; return; }
+    float fastest = 1e30f;
+    for (const TuneEntry& t : res.report) fastest = std::min(fastest, t.ms);
+    const TuneEntry* pick = nullptr;
+    for (const TuneEntry& t : res.report) {
+        if (t.ms > fastest * (1.0f + kTuneTie)) continue;
+        const bool preferred = t.cfg.kind == PUSH_LOCAL && t.cfg.param == kLocalConcurrent;
+        if (!pick || (preferred && !(pick->cfg.kind == PUSH_LOCAL && pick->cfg.param == kLocalConcurrent))) pick = &t;
+    }
+    res.best = pick->cfg;
+    res.best_ms = pick->ms;
+}
+
 // Time every push variant on the spike list the LIF kernel just wrote, into
 // scratch accumulators so the simulation state is untouched, and return the
 // fastest.  `views` are the host copies of the launch's networks.
@@ -961,10 +981,7 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
         if (res.observed >= res.observe + kTuneGiveUp) {
             // settle: the best of the samples so far, or the default variant
             res.tuned = true;
-            res.best_ms = 1e30f;
-            for (const TuneEntry& t : res.report)
-                if (t.ms < res.best_ms) { res.best_ms = t.ms; res.best = t.cfg; }
-            if (res.report.empty()) res.best_ms = 0.0f;
+            pick_best(res);
         }
         return DTB_OK;
     }
@@ -1027,9 +1044,7 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
     }
     if (res.samples < res.want) return DTB_OK;
     res.tuned = true;
-    res.best_ms = 1e30f;
-    for (const TuneEntry& t : res.report)
-        if (t.ms < res.best_ms) { res.best_ms = t.ms; res.best = t.cfg; }
+    pick_best(res);
     return DTB_OK;
 }
 

@@ -578,9 +578,9 @@ __device__ __forceinline__ void prefetch_span_l2(const uint32_t* col, const void
 // ---------------------------------------------------------------------------
 // Push propagation: one warp per spiking row of the out-degree CSR
 // ---------------------------------------------------------------------------
-template <int ACC, int WT, int kPushUnroll, int LPR, int LOCAL = 0>
-__global__ void __launch_bounds__(kPushThreads)
-push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase, uint32_t n_nets, SpikeList sl) {
+template <int ACC, int WT, int kPushUnroll, int LPR, int LOCAL>
+__device__ __forceinline__ void push_rows(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase, uint32_t n_nets,
+                                          SpikeList sl) {
     // LPR lanes per row: 32 (a warp per row) or 16 / 8 (2 / 4 rows per warp, for short rows).
     // LOCAL: the own-population span of a row (own_seg) is left to push_local_kernel.
     constexpr uint32_t kGroups = 32 / LPR;
@@ -657,6 +657,24 @@ push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase
             __threadfence();
         }
     }
+}
+
+template <int ACC, int WT, int kPushUnroll, int LPR, int LOCAL = 0>
+__global__ void __launch_bounds__(kPushThreads)
+push_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase, uint32_t n_nets, SpikeList sl) {
+    push_rows<ACC, WT, kPushUnroll, LPR, LOCAL>(nets, vbase, n_nets, sl);
+}
+
+// The cross-population part held to 64 registers (4 CTAs of 256 threads) for local:2016: two
+// CTAs of it and the 512-thread window kernel (64 registers) fill exactly the SM's 65,536
+// registers, so the two kernels really share every SM; at the 80 registers the compiler picks
+// otherwise, a window CTA cannot start on an SM until the cross-population CTAs there have
+// finished.  local:2008 keeps that 80-register form: held to 64 it also shared its SMs but ran
+// 2 % slower on burst steps and no faster over whole runs of the regional network.
+template <int ACC, int WT>
+__global__ void __launch_bounds__(kPushThreads, 4)
+push_kernel_cross64(const NetView* __restrict__ nets, const uint32_t* __restrict__ vbase, uint32_t n_nets, SpikeList sl) {
+    push_rows<ACC, WT, 8, 32, 1>(nets, vbase, n_nets, sl);
 }
 
 // ---------------------------------------------------------------------------
@@ -1497,7 +1515,10 @@ static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint
         cudaError_t e = cudaEventRecord(b.ev_fork, s);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(b.aux, b.ev_fork, 0);
         if (e != cudaSuccess) return e;
-        push_kernel<ACC, WT, 8, 32, 1><<<b.sm_count * (two ? 2u : 1u), kPushThreads, 0, b.aux>>>(b.nets, b.vbase, b.n_nets, b.spikes);
+        if (two)
+            push_kernel_cross64<ACC, WT><<<b.sm_count * 2u, kPushThreads, 0, b.aux>>>(b.nets, b.vbase, b.n_nets, b.spikes);
+        else
+            push_kernel<ACC, WT, 8, 32, 1><<<b.sm_count, kPushThreads, 0, b.aux>>>(b.nets, b.vbase, b.n_nets, b.spikes);
         e = cudaEventRecord(b.ev_join, b.aux);
         if (e != cudaSuccess) return e;
         local_count_kernel<<<b.windows_total, 256, 0, s>>>(b.nets, b.win_prefix, b.n_nets, b.local_scratch);
@@ -1569,6 +1590,12 @@ static cudaError_t push_prepare_wt(const PushCfg& cfg, int sm_count, uint32_t* c
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(push_local_kernel<WT, kLocalThreadsShared, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(kLocalSmem));
+        // the cross-population CTAs land on an SM first: ask for the largest shared-memory
+        // carve-out so a window CTA (229 KB) can join them there
+        for (auto fn : {push_kernel<ACC, WT, 8, 32, 1>, push_kernel<ACC, WT, 8, 16, 1>, push_kernel_cross64<ACC, WT>})
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         static_cast<int>(cudaSharedmemCarveoutMaxShared));
         if (e == cudaSuccess)
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cfg.lpr == 16 ? push_kernel<ACC, WT, 8, 16, 1> : push_kernel<ACC, WT, 8, 32, 1>,
                                                               kPushThreads, 0);

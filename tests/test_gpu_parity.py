@@ -365,7 +365,9 @@ def test_autotuner_picks_a_variant(gpu):
         assert eng.info().local_windows > 0
         assert len(rep) == 12 and all(ms > 0 for _, _, ms in rep)
         inf = eng.info()
-        assert min(ms for _, _, ms in rep) == pytest.approx(inf.push_tuned_ms)
+        fastest = min(ms for _, _, ms in rep)
+        assert fastest <= inf.push_tuned_ms <= fastest * 1.02 + 1e-6     # ties within 2 % go to local:2008
+        assert any(ms == pytest.approx(inf.push_tuned_ms) for _, _, ms in rep)
 
 
 @pytest.mark.parametrize("n", [1, 31, 32, 33, 4095, 4096, 4097, 100_000, 5_000_000])
