@@ -70,8 +70,8 @@ def test_batch_graph_window_and_solo_interleave(gpu):
         e.close()
 
 
-@pytest.mark.parametrize("graph", [False, True])
-def test_batch_local_push_step(gpu, graph):
+@pytest.mark.parametrize("graph,param", [(False, 8), (True, 2008), (True, 2016)])
+def test_batch_local_push_step(gpu, graph, param):
     """Batched population-local push: from saved mid-run member states, one float
     step gives every member the exact push's spikes and V, and J within float rounding."""
     specs = _members()
@@ -85,7 +85,7 @@ def test_batch_local_push_step(gpu, graph):
         j_ref = [e.read_state(E.STATE_J) for e in engines]
         for e, blob in zip(engines, blobs):
             e.load_state(blob)
-        b.set_push_variant(E.PUSH_LOCAL, 2008 if graph else 8)
+        b.set_push_variant(E.PUSH_LOCAL, param)
         got = b.run(1, record_spikes=True, syn_mode=E.SYN_PUSH)
         assert b.info()["push_kind"] == E.PUSH_LOCAL
     for i, e in enumerate(engines):
