@@ -124,6 +124,9 @@ cudaError_t compact_launch(const uint32_t* bits, uint32_t n, uint32_t* idx, uint
 extern "C" int32_t dtb_compact_spikes(const uint32_t* d_bits, uint32_t n_neurons, uint32_t* d_indices,
                                       uint32_t* d_count, void* stream) {
     if (!d_count || (n_neurons && (!d_bits || !d_indices))) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
+    if (n_neurons > dtb::kCompactMaxNeurons)
+        return dtb::fail(DTB_INVALID_PARAMETER, "dtb_compact_spikes: n_neurons " + std::to_string(n_neurons) +
+                                                    " exceeds the limit of " + std::to_string(dtb::kCompactMaxNeurons));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const uint32_t tiles = dtb::compact_tiles(n_neurons);
     uint32_t* scratch = nullptr;

@@ -8,9 +8,12 @@ namespace dtb {
 
 constexpr int kCompactWordsPerTile = 128;                  // 4096 neurons per tile
 constexpr uint32_t kCompactTileNeurons = kCompactWordsPerTile * 32;
+// Largest bitmap the operator takes: the last tile boundary below 2^32, so the tile
+// count, the word count (n + 31) / 32 and every neuron index stay in 32 bits.
+constexpr uint32_t kCompactMaxNeurons = 0xFFFFFFFFu / kCompactTileNeurons * kCompactTileNeurons;
 
 inline uint32_t compact_tiles(uint32_t n) {
-    return (n + kCompactTileNeurons - 1) / kCompactTileNeurons;
+    return static_cast<uint32_t>((static_cast<uint64_t>(n) + kCompactTileNeurons - 1) / kCompactTileNeurons);
 }
 
 // Count, scan and write; `tile_scratch` holds compact_tiles(n) words.

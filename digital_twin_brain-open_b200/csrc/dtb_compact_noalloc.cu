@@ -2,8 +2,6 @@
 //
 // Some callers of this library cannot allocate device memory at the point where
 // they need a compaction:
-// * a host that records its per-step work into a CUDA graph -- allocation calls
-//   are not allowed while a stream is being captured;
 // * a long-running serving or data-assimilation loop whose device-memory budget is
 //   fixed when it starts, so that its admission decisions stay valid;
 // * a runtime that embeds the engine and owns all device memory through its own
@@ -23,7 +21,10 @@
 //   calls whose kernels overlap on the GPU (unordered streams, or host threads that
 //   do not order their calls) race on it and produce wrong lists: order them;
 // * the first call on each device looks up the array's device address, with that
-//   device current, and caches it; make that first call before any stream capture.
+//   device current, and keeps it for the life of the process; make that first call
+//   before any stream capture.  The kept address assumes the device's primary
+//   context is never reset: after a cudaDeviceReset the old address is stale, so
+//   the library must not be called again in that process.
 #include <mutex>
 
 #include "dtb_compact.h"

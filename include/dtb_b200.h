@@ -396,19 +396,26 @@ int32_t dtb_build_out_csr_host(uint32_t n_neurons, uint64_t n_edges, const uint3
  * `d_indices` (room for n entries) and its length `*d_count`, all in device
  * memory, ordered on `stream` (a cudaStream_t, NULL = default stream).
  * Deterministic.  Scratch: one word per 4096 neurons, allocated and released
- * on `stream` by each call. */
+ * on `stream` by each call.  n_neurons <= 4,294,963,200 (the last 4096-neuron
+ * tile boundary below 2^32); larger values return DTB_INVALID_PARAMETER before
+ * anything runs. */
 int32_t dtb_compact_spikes(const uint32_t* d_bits, uint32_t n_neurons, uint32_t* d_indices, uint32_t* d_count,
                            void* stream);
 
 /* The same compaction for callers that cannot allocate device memory at the point
- * of the call -- a host recording a CUDA graph (no allocation during stream
- * capture), a loop with a device-memory budget fixed at start-up, a runtime that
- * owns all device memory.  No counterpart in the reference.  It allocates
+ * of the call: a serving or data-assimilation loop whose device-memory budget is
+ * fixed when it starts (so that its admission decisions stay valid), or a runtime
+ * that embeds the engine, owns all device memory through its own pool and forbids
+ * libraries to allocate.  No counterpart in the reference.  It allocates
  * nothing: its scratch is a fixed 64 KiB array inside the library, so
- * n_neurons <= 2^26 (larger inputs return DTB_INVALID_PARAMETER).  All calls
- * share that array: calls whose kernels overlap on the GPU race and must be
- * ordered.  The first call on each device looks the array up (with that device
- * current); make it before any stream capture. */
+ * n_neurons <= 2^26 (larger inputs return DTB_INVALID_PARAMETER before anything
+ * runs).  All calls share that array, which keeps the last call's counts (each is
+ * written before it is read, so nothing needs clearing): calls whose kernels
+ * overlap on the GPU race and must be ordered.  The first call on each device
+ * looks the array's address up (with that device current) and keeps it for the
+ * life of the process; make that first call before any stream capture.  The kept
+ * address assumes the device's primary context is never reset: after a
+ * cudaDeviceReset the library must not be called again in that process. */
 int32_t dtb_compact_spikes_noalloc(const uint32_t* d_bits, uint32_t n_neurons, uint32_t* d_indices,
                                    uint32_t* d_count, void* stream);
 

@@ -63,6 +63,18 @@ def test_invalid_arguments_are_statuses_not_crashes():
     assert E.LIB.dtb_create_from_npz(b"", C.byref(o), C.byref(h)) == E.INVALID_PARAMETER
 
 
+@pytest.mark.skipif(has_gpu(), reason="argument check only; no device calls")
+def test_compaction_rejects_counts_beyond_32_bits():
+    """Bitmaps whose tile or word counts would wrap 32 bits are rejected before any
+    CUDA call (the pointers are never touched, so placeholders suffice here)."""
+    import ctypes as C
+    fake = C.c_void_p(256)
+    for n in (0xFFFFFFFF, 0xFFFFF001):
+        assert E.LIB.dtb_compact_spikes(fake, n, fake, fake, None) == E.INVALID_PARAMETER
+        assert "limit" in E.LIB.dtb_last_error().decode()
+    assert E.LIB.dtb_compact_spikes_noalloc(fake, (1 << 26) + 1, fake, fake, None) == E.INVALID_PARAMETER
+
+
 @pytest.mark.parametrize("seed", [0, 1, 2])
 def test_host_csr_matches_oracle(seed):
     """The engine's host CSR builder equals the restated reference builder, bit for bit."""

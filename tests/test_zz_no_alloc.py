@@ -1,9 +1,8 @@
 """The spike compaction that allocates nothing, against the one that allocates.
 
 Callers that cannot allocate device memory where they need a compaction -- a
-host recording its step into a CUDA graph (no allocation while a stream is
-captured), a serving or data-assimilation loop whose device-memory budget is fixed
-at start-up, or a runtime that owns all device memory through its own pool -- call
+serving or data-assimilation loop whose device-memory budget is fixed at start-up,
+or a runtime that owns all device memory through its own pool -- call
 ``dtb_compact_spikes_noalloc``, whose scratch is a fixed array inside the library.
 This file checks, through the C-ABI, that two calls in a row give exactly the same
 index lists and counts as ``dtb_compact_spikes`` on the same inputs (integer
@@ -59,10 +58,14 @@ def test_noalloc_matches_allocating_compaction(gpu):
 
 def test_noalloc_rejects_inputs_beyond_its_limit(gpu):
     import torch
-    bits = torch.zeros(16, dtype=torch.int32, device="cuda")
-    idx = torch.zeros(16, dtype=torch.int32, device="cuda")
-    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
-    st = E.LIB.dtb_compact_spikes_noalloc(C.c_void_p(bits.data_ptr()), MAX_NEURONS + 1, C.c_void_p(idx.data_ptr()),
+    n = MAX_NEURONS + 1
+    # buffers sized for n, so that even a broken limit check could not write out of bounds
+    bits = torch.zeros((n + 31) // 32, dtype=torch.int32, device="cuda")
+    idx = torch.zeros(n, dtype=torch.int32, device="cuda")
+    cnt = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+    st = E.LIB.dtb_compact_spikes_noalloc(C.c_void_p(bits.data_ptr()), n, C.c_void_p(idx.data_ptr()),
                                           C.c_void_p(cnt.data_ptr()), None)
     assert st == E.INVALID_PARAMETER
     assert "limit" in E.LIB.dtb_last_error().decode()
+    torch.cuda.synchronize()
+    assert int(cnt.item()) == -1          # rejected before anything ran
