@@ -53,6 +53,9 @@ def lib():
         _lib.oracle_run_f64.restype = C.c_int64
         _lib.oracle_run_f64.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_int32, C.c_int32]
+        _lib.oracle_run_events.restype = C.c_int64
+        _lib.oracle_run_events.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_float, C.c_void_p, C.c_void_p,
+                                           C.c_int, C.c_void_p]
     return _lib
 
 
@@ -191,3 +194,64 @@ class COracle64:
                                   None if sp is None else sp.ctypes.data, counts.ctypes.data,
                                   None if vt is None else vt.ctypes.data, n_v, int(clock32))
         return (None if sp is None else sp.astype(bool)), counts, int(ev), vt
+
+
+class _Events(C.Structure):
+    _fields_ = [("out_ptr", C.c_void_p), ("out_post", C.c_void_p), ("out_kind", C.c_void_p), ("ow0", C.c_void_p),
+                ("ow1", C.c_void_p), ("pop_of", C.c_void_p), ("n_pops", C.c_int32), ("step0", C.c_int64),
+                ("warm", C.c_int64), ("pop_spikes", C.c_void_p), ("last_spike", C.c_void_p), ("isi", C.c_void_p),
+                ("acc", C.c_void_p), ("list", C.c_void_p)]
+
+
+class COracleEvents(COracle):
+    """``COracle`` with the event-driven step (``oracle_run_events``): the same
+    float32 results, O(events) per step, plus running population spike counts and
+    pooled inter-spike-interval moments from step ``warm`` on -- the long
+    statistical runs of the firing-rate / ISI-CV checks."""
+
+    def __init__(self, net, pop_of, warm=0, **kw):
+        super().__init__(net, **kw)
+        n = self.n
+        pre = np.asarray(net["input_neuron_idx"], np.uint32)
+        post = np.asarray(net["output_neuron_idx"], np.uint32)
+        if post.size and np.all(post[1:] >= post[:-1]):
+            order = np.argsort(pre, kind="stable")          # post-major input: rows ascend by target
+        else:
+            order = np.lexsort((post, pre))
+        self.out_ptr = np.concatenate([[0], np.cumsum(np.bincount(pre, minlength=n))]).astype(np.int64)
+        self.out_post = np.ascontiguousarray(post[order])
+        self.out_kind = np.ascontiguousarray((np.asarray(net["input_channel_offset"]) != 0)[order].astype(np.uint8))
+        w = np.asarray(net["weight"], np.float32)
+        self.ow0 = np.ascontiguousarray(w[order, 0])
+        self.ow1 = np.ascontiguousarray(w[order, 1])
+        self.pop_of = np.ascontiguousarray(pop_of, np.int32)
+        self.n_pops = int(self.pop_of.max()) + 1 if n else 0
+        self.pop_spikes = np.zeros(self.n_pops, np.int64)
+        self.last_spike = np.full(n, -1, np.int64)
+        self.isi = np.zeros(3, np.float64)
+        self._acc = np.zeros(4 * n, np.float64)
+        self._list = np.zeros(max(n, 1), np.uint32)
+        self._ev = _Events(self.out_ptr.ctypes.data, self.out_post.ctypes.data, self.out_kind.ctypes.data,
+                           self.ow0.ctypes.data, self.ow1.ctypes.data, self.pop_of.ctypes.data, self.n_pops, 0,
+                           int(warm), self.pop_spikes.ctypes.data, self.last_spike.ctypes.data,
+                           self.isi.ctypes.data, self._acc.ctypes.data, self._list.ctypes.data)
+
+    def run(self, z, u=None, record=False):
+        """Run z.shape[0] steps; returns (None, counts [steps], events).  Statistics
+        accumulate in pop_spikes / isi across calls."""
+        if record:
+            raise ValueError("the event-driven oracle keeps running statistics, not rasters")
+        z = np.ascontiguousarray(z, np.float32)
+        steps = z.shape[0]
+        u = None if u is None else np.ascontiguousarray(u, np.float32)
+        counts = np.zeros(steps, np.int64)
+        ev = lib().oracle_run_events(C.byref(self._s), C.byref(self._ev), steps, self.dt, z.ctypes.data,
+                                     None if u is None else u.ctypes.data, self.prop_mode, counts.ctypes.data)
+        return None, counts, int(ev)
+
+    def isi_cv(self):
+        c, s1, s2 = self.isi
+        if c < 2:
+            return float("nan")
+        mean = s1 / c
+        return float(np.sqrt(max(s2 / c - mean * mean, 0.0)) / mean)

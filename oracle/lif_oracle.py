@@ -88,6 +88,26 @@ def torch_noise_stream(seed, n, steps, with_uniform):
     return z, u
 
 
+def torch_noise_chunks(seed, n, steps, chunk, with_uniform=False):
+    """The stream of ``torch_noise_stream`` in chunks of at most ``chunk`` steps
+    (same call order, so the concatenated chunks equal its arrays), for runs too
+    long to hold every draw at once.  Yields (z, u or None)."""
+    import torch
+    g = torch.Generator()
+    g.manual_seed(seed)
+    done = 0
+    while done < steps:
+        k = min(chunk, steps - done)
+        z = np.empty((k, n), np.float32)
+        u = np.empty((k, n), np.float32) if with_uniform else None
+        for s in range(k):
+            z[s] = torch.randn(n, generator=g).numpy()
+            if with_uniform:
+                u[s] = torch.rand(n, generator=g).numpy()
+        done += k
+        yield z, u
+
+
 class LifOracle:
     """One LIF block, stepping exactly like block_new (see module docstring).
 

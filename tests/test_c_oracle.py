@@ -73,3 +73,51 @@ def test_float32_clock_explains_the_rate_gap():
     r32 = cc.COracle(net).run(z)[0][warm:].mean()
     assert abs(r64 - r32) > 0.05 * r32            # a visible gap on this network...
     assert abs(r64c - r32) < 0.002 * r32          # ...closed by the float32 clock alone
+
+
+@pytest.mark.parametrize("prop_mode", [lo.PROP_THRESHOLD, lo.PROP_OR])
+def test_event_driven_oracle_equals_full_sweep(prop_mode):
+    """oracle_run_events (O(events) per step, threads over target ranges) gives the
+    same float32 state as oracle_run (every in-edge each step): the double sums of
+    weights that are multiples of 2^-24 are exact in any order."""
+    spec = nw.structured_spec(12_000, 5, 300, seed=6)
+    net = cc.structured_edges(spec)
+    net["property"][:, 0] = 0.01
+    steps = 300
+    z, u = lo.torch_noise_stream(2, spec.n, steps, prop_mode != lo.PROP_THRESHOLD)
+    a = cc.COracle(net, prop_mode=prop_mode)
+    sp, counts, ev = a.run(z, u)
+    pop = np.repeat(np.arange(spec.n_pops), spec.pop_sizes)
+    b = cc.COracleEvents(net, pop, warm=0, prop_mode=prop_mode)
+    _, counts_b, ev_b = b.run(z[:120], None if u is None else u[:120])
+    _, counts_c, ev_c = b.run(z[120:], None if u is None else u[120:])
+    assert counts.sum() > 0
+    assert np.array_equal(np.concatenate([counts_b, counts_c]), counts) and ev_b + ev_c == ev
+    for k in ("V", "J", "i_bg", "t_last", "I_syn"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+    # running statistics equal the ones taken from the raster
+    from tests.spike_stats import IsiMoments
+    assert np.array_equal(b.pop_spikes, np.bincount(pop, weights=sp.sum(0), minlength=spec.n_pops).astype(np.int64))
+    m = IsiMoments(spec.n, 0)
+    m.add(sp[:77], 0)
+    m.add(sp[77:], 77)
+    assert m.count == int(b.isi[0]) and m.count > 0
+    assert abs(m.cv() - b.isi_cv()) < 1e-12
+
+
+def test_isi_moments_warm_up_and_chunks():
+    rng = np.random.default_rng(3)
+    r = rng.random((400, 50)) < 0.05
+    warm = 100
+    ref = []
+    for j in range(50):
+        t = np.nonzero(r[:, j])[0]
+        t = t[t >= warm]
+        ref.extend(np.diff(t))
+    ref = np.asarray(ref, np.float64)
+    from tests.spike_stats import IsiMoments
+    m = IsiMoments(50, warm)
+    for a in range(0, 400, 37):
+        m.add(r[a:a + 37], a)
+    assert m.count == ref.size
+    assert abs(m.cv() - ref.std() / ref.mean()) < 1e-12
