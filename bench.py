@@ -12,8 +12,17 @@ Contract (one JSON line on rank 0):
   host buffers: each window uploads new per-population OU parameters and reads
   back every step's spike counts and mean potentials;
 * roofline = the push kernel (the dominant kernel) against the measured HBM copy
-  bandwidth; cpu_baseline = the C port of the reference CPU model on a sample.
+  bandwidth; cpu_baseline = the C port of the reference CPU model on the bounded
+  CPU sample (20 x 75 simulated steps of a 50,000-neuron network of the same
+  construction);
+* batched / served (single GPU, default configuration) = the metric's second half on
+  reduced configurations: a 16-member BF16 ensemble batched vs the same members run
+  one by one on the plain FP32 path, and a 60-request Poisson stream at 40/s over 32
+  resident networks served with continuous batching (BF16) vs one request at a time
+  (plain FP32), p50/p99 latency at the same offered rate; each with its own clocks.
 N > 1 GPUs run independent replicas (no data-path collective: "scaling": "weak").
+--impl reference: the reference arm, the C port of the reference CPU model on the
+host cores, W warm-up and K timed bench steps of the CPU sample.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -35,7 +44,11 @@ METRIC = "synaptic events/s and sim-ms per wall-s; batched/served vs plain p50/p
 UNIT = "synaptic events/s"
 WINDOW = 500
 N_NEURONS, N_POPS, IN_DEGREE, SPEC_SEED = 5_000_000, 200, 1000, 1
-CPU_SAMPLE = dict(n=50_000, pops=20, in_degree=1000, seed=7, burn_in=400, timed=60)
+# the bounded CPU sample: the regional construction at 50,000 neurons (the 5M network needs
+# 200-280 GB of host memory as block_new's sparse tensors); one bench step = 75 simulated steps
+CPU_SAMPLE = dict(n=50_000, pops=20, in_degree=1000, seed=7, burn_in=400, per_step=75)
+CPU_WORKLOAD = ("50,000-neuron regional LIF network, 20 populations, in-degree 1000, f32 weights, OU background "
+                "(the 5M-neuron network's construction at a size the host runs)")
 BYTES_STATE = 56          # V, J x4, i_ou, t_last read + written per neuron per step
 CSR_COL_BYTES = 4
 ACC_BYTES = 8             # one logical accumulator update (a float pair) per event
@@ -55,6 +68,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--weights", default="f32", choices=["f32", "bf16"])
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--no-forms", action="store_true",
+                   help="skip the reduced batched and served comparisons of the default line")
     p.add_argument("--neurons", type=int, default=N_NEURONS, help="network size (profiling runs use a small one)")
     p.add_argument("--pops", type=int, default=N_POPS)
     p.add_argument("--degree", type=int, default=IN_DEGREE)
@@ -70,39 +85,53 @@ def parse():
     p.add_argument("--members", type=int, default=None, help="ensemble members (64) or served networks (128)")
     p.add_argument("--net", default="regional", choices=["regional", "uniform"],
                    help="regional: the structured regional network; uniform: the plain one-population block")
-    p.add_argument("--syn", default="push", choices=["push", "exact", "pull"],
-                   help="synaptic mode: float push, exact (fixed-point) push, or deterministic pull")
+    p.add_argument("--syn", default="push", choices=["push", "exact", "pull", "fixed"],
+                   help="synaptic mode: float push, exact (64-bit fixed-point) push, deterministic pull, or the "
+                        "deterministic 32-bit fixed-point push")
     p.add_argument("--window", type=int, default=800, help="steps per assimilation window (ensemble form)")
+    p.add_argument("--graph", default="on", choices=["on", "off"], help="replay repeated windows from CUDA graphs")
+    p.add_argument("--batched-syn", default="fixed", choices=["fixed", "push"],
+                   help="synaptic mode of the batched / served side of the ensemble and serve forms: the "
+                        "deterministic fixed-point push (a member equals its solo run) or the float push")
     return p.parse_args()
 
 
 # ---------------------------------------------------------------------------
 # CPU: the C port of the reference model on a bounded sample
 # ---------------------------------------------------------------------------
-def cpu_sample_rate(max_seconds=None):
+def cpu_port_run(timed, warm):
+    """The C port of models/block_new.py on the CPU sample (CPU_WORKLOAD): an untimed burn-in
+    past the network's quiet start, `warm` untimed bench steps, then `timed` bench steps of
+    CPU_SAMPLE["per_step"] simulated steps each, on every host thread."""
     import __graft_entry__
     __graft_entry__.load_package()        # registers the package (network specs only; no CUDA library)
     from dtb_b200 import network as nw
     from oracle import c_oracle as cc
-    from oracle import lif_oracle as lo
     s = CPU_SAMPLE
     spec = nw.structured_spec(s["n"], s["pops"], s["in_degree"], s["seed"])
-    net = cc.structured_edges(spec)
-    orc = cc.COracle(net)
+    orc = cc.COracle(cc.structured_edges(spec))
     rng = np.random.default_rng(0)
-    z = rng.standard_normal((s["burn_in"], spec.n), dtype=np.float32)
-    orc.run(z, record=False)                             # untimed burn-in past the start-up transient
-    z = rng.standard_normal((s["timed"], spec.n), dtype=np.float32)
-    t0 = time.perf_counter()
-    _, counts, events = orc.run(z, record=False)
-    dt = time.perf_counter() - t0
+    orc.run(rng.standard_normal((s["burn_in"], spec.n), dtype=np.float32), record=False)
+    for _ in range(warm):
+        orc.run(rng.standard_normal((s["per_step"], spec.n), dtype=np.float32), record=False)
+    events = spikes = 0
+    wall = 0.0
+    for _ in range(timed):
+        z = rng.standard_normal((s["per_step"], spec.n), dtype=np.float32)
+        t0 = time.perf_counter()
+        _, counts, ev = orc.run(z, record=False)
+        wall += time.perf_counter() - t0
+        events += ev
+        spikes += int(counts.sum())
     threads = cc.lib().oracle_threads()
-    sample = (f"C port of models/block_new.py (W.s over all synapses each step, float32) on a "
-              f"{spec.n}-neuron, {spec.n_pops}-population, in-degree-{spec.in_degree} network of the same "
-              f"construction: {s['timed']} steps timed after {s['burn_in']} untimed, "
-              f"{int(counts.sum())} spikes, {events} events in {dt:.2f} s")
-    return dict(value=events / dt, unit=UNIT, cores=threads, kind="port", sample=sample,
-                sim_ms_per_wall_s=s["timed"] * 0.1 / dt, ms_per_step=1e3 * dt / s["timed"])
+    sim_steps = timed * s["per_step"]
+    sample = (f"C port of models/block_new.py (W.s over all synapses each step, float32), {threads} threads, on "
+              f"the {CPU_WORKLOAD}: {sim_steps} simulated steps timed ({timed} x {s['per_step']}) after "
+              f"{s['burn_in'] + warm * s['per_step']} untimed; {spikes} spikes, {events} events in {wall:.2f} s. "
+              f"models/block_new.py itself (torch.sparse_coo weights) steps this network 1,400x slower than the "
+              f"port on the same threads (profiles/cpu_port_vs_block_new_50k.md)")
+    return dict(value=events / wall, unit=UNIT, cores=threads, kind="port", sample=sample, wall_s=wall,
+                sim_ms_per_wall_s=sim_steps * 0.1 / wall, ms_per_step=1e3 * wall / max(timed, 1), steps=timed)
 
 
 # ---------------------------------------------------------------------------
@@ -210,7 +239,7 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     wt = E.W_BF16 if args.weights == "bf16" else E.W_F32
-    syn = {"push": E.SYN_PUSH, "exact": E.SYN_PUSH_EXACT, "pull": E.SYN_PULL}[args.syn]
+    syn = {"push": E.SYN_PUSH, "exact": E.SYN_PUSH_EXACT, "pull": E.SYN_PULL, "fixed": E.SYN_PUSH_FIXED}[args.syn]
     t0 = time.perf_counter()
     if args.net == "uniform":
         # the plain block: one population, fixed in-degree, uniform sources (host-built CSR)
@@ -226,6 +255,7 @@ def run_ours(args):
     if args.push != "auto":
         kind, param = args.push.split(":")
         eng.set_push_variant(PUSH_KINDS.index(kind), int(param))
+    eng.set_graph(args.graph == "on")
     info = eng.info()
     stream = torch.cuda.ExternalStream(eng.stream(), device=dev)
     P = eng.n_pops
@@ -310,7 +340,7 @@ def run_ours(args):
         step_bytes = push_bytes + lif_bytes
         cpu = None
         if world == 1 and not args.no_cpu:
-            cpu = cpu_sample_rate()
+            cpu = cpu_port_run(20, 0)
             cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         h2d = P * 96 + P * 3 * 4
         d2h = WINDOW * P * (4 + 8)
@@ -322,7 +352,7 @@ def run_ours(args):
             "sim_ms_per_wall_s": args.steps * WINDOW * 0.1 / (ms / 1e3),
             "config": {"workload": f"{info.n_neurons}-neuron {args.net} LIF network, {P} populations, "
                                    f"in-degree {args.degree}, {args.weights} weights, OU background, "
-                                   f"{ {'push': 'push', 'exact': 'exact fixed-point push', 'pull': 'deterministic pull'}[args.syn] } propagation",
+                                   f"{ {'push': 'push', 'exact': 'exact fixed-point push', 'pull': 'deterministic pull', 'fixed': 'fixed-point push'}[args.syn] } propagation",
                        "neurons": info.n_neurons, "synapses": int(info.n_edges), "populations": P,
                        "dt_ms": 0.1, "steps_per_bench_step": WINDOW,
                        "timed_sim_steps": args.steps * WINDOW, "warmup_sim_steps": args.warmup * WINDOW,
@@ -353,6 +383,11 @@ def run_ours(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    if out is not None and world == 1 and not args.no_forms and args.net == "regional" and \
+            args.neurons == N_NEURONS:
+        # the metric's second half, batched/served vs plain at equal rate, on reduced configurations
+        out["batched"] = measure_ensemble(16, 4, 800, 1, args.batched_syn)
+        out["served"] = measure_serve(32, 60, 40.0, 800, 100, 150.0, args.batched_syn)
     return out
 
 
@@ -369,16 +404,20 @@ def isi_cv(spikes):
     return float(x.std() / x.mean())
 
 
-def run_ensemble(args):
-    """Batched BF16 data-assimilation ensemble vs the same members run one by one (FP32)."""
+def _clock_sampler(torch):
+    return ClockSampler(str(getattr(torch.cuda.get_device_properties(torch.cuda.current_device()), "uuid", "")))
+
+
+def measure_ensemble(n_members, windows, W, warmup, batched_syn, seed=3):
+    """Batched BF16 data-assimilation ensemble vs the same members run one by one through
+    the plain FP32 path, same windows and property updates.  Returns the comparison."""
     import torch
     import __graft_entry__
     __graft_entry__.load_package()
     from dtb_b200 import engine as E
     from dtb_b200 import network as nw
 
-    specs = nw.ensemble_specs(n_members=args.members or 64, seed=3)
-    windows, W = args.steps, args.window
+    specs = nw.ensemble_specs(n_members=n_members, seed=seed)
     rng_hp = np.random.default_rng(11)
     # per-window DA hyper-parameter factors (mul_property_by_subblk of g_AMPA per population)
     factors = [[rng_hp.uniform(0.97, 1.03, s.n_pops).astype(np.float32) for s in specs] for _ in range(windows)]
@@ -401,24 +440,28 @@ def run_ensemble(args):
         return rates, np.array(cvs)
 
     # ---- batched BF16 (one graph-replayed launch sequence per window for all members)
+    bsyn = E.SYN_PUSH_FIXED if batched_syn == "fixed" else E.SYN_PUSH
     engs, build_b = build(E.W_BF16)
     batch = E.Batch(engs)
-    for _ in range(args.warmup):
-        batch.run(W)
+    for _ in range(warmup):
+        batch.run(W, syn_mode=bsyn)
     acc = [[np.zeros((0, s.n_pops), np.int32), np.zeros((0, 200), np.uint8)] for s in specs]
     ev_b = 0
     dev_b = 0.0
+    sampler = _clock_sampler(torch)
+    sampler.start()
     t0 = time.perf_counter()
     for w in range(windows):
         for e, s, f in zip(engs, specs, factors[w]):
             e.update_prop_cols([g_ampa] * s.n_pops, np.arange(s.n_pops), f)
-        res = batch.run(W, sample_spike=True)
+        res = batch.run(W, sample_spike=True, syn_mode=bsyn)
         dev_b += res[0].device_ms
         for i, r in enumerate(res):
             ev_b += r.events
             acc[i][0] = np.concatenate([acc[i][0], r.freqs])
             acc[i][1] = np.concatenate([acc[i][1], r.sample_spike])
     wall_b = time.perf_counter() - t0
+    clocks = sampler.stop()
     rates_b, cv_b = summarise(acc)
     binfo = batch.info()
     batch.close()
@@ -428,7 +471,7 @@ def run_ensemble(args):
     # ---- sequential plain FP32 (each member through its own dtb_run)
     engs, build_s = build(E.W_F32)
     for e in engs:
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             e.run(W)
     acc = [[np.zeros((0, s.n_pops), np.int32), np.zeros((0, 200), np.uint8)] for s in specs]
     ev_s = 0
@@ -447,18 +490,15 @@ def run_ensemble(args):
     for e in engs:
         e.close()
     rate_rel = np.concatenate([np.abs(a - b) / np.maximum(b, 1e-9) for a, b in zip(rates_b, rates_s)])
-    mean_rate_b = float(np.mean(np.concatenate(rates_b)))
     member_steps = len(specs) * windows * W
     return {
-        "metric": METRIC, "form": "ensemble", "value": ev_b / wall_b, "unit": UNIT + " (ensemble, wall)",
-        "n_gpus": 1, "steps": windows, "warmup": args.warmup, "ms_per_step": 1e3 * wall_b / windows,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16-weights/f32-state",
-        "data": "synthetic (64 seeded DA members generated on the device)",
-        "config": {"workload": f"{len(specs)} ensemble members, N in [20k, 400k], in-degree in {{100,200,500}}, "
-                               f"10-50 populations, {W}-step windows, g_AMPA multiplied per population between windows",
-                   "neurons": int(sum(s.n for s in specs)), "synapses": int(sum(s.n_edges for s in specs)),
-                   "batched_graph_launches": binfo["graph_launches"],
-                   "batched_push_variant": binfo["push_kind"] * 10000 + binfo["push_param"]},
+        "workload": f"{len(specs)} ensemble members (N in [20k, 400k], in-degree in {{100, 200, 500}}, 10-50 "
+                    f"populations), {windows} windows of {W} steps, g_AMPA multiplied per population between "
+                    f"windows, {warmup} warm-up window(s)",
+        "neurons": int(sum(s.n for s in specs)), "synapses": int(sum(s.n_edges for s in specs)),
+        "batched_synaptic_mode": batched_syn, "sequential_synaptic_mode": "push",
+        "batched_graph_launches": binfo["graph_launches"],
+        "batched_push_variant": binfo["push_kind"] * 10000 + binfo["push_param"],
         "batched_bf16": {"events_per_s_wall": ev_b / wall_b, "events_per_s_device": ev_b / (dev_b / 1e3),
                          "member_steps_per_s": member_steps / wall_b, "wall_s": wall_b, "device_s": dev_b / 1e3,
                          "build_s": build_b},
@@ -466,80 +506,115 @@ def run_ensemble(args):
                            "member_steps_per_s": member_steps / wall_s, "wall_s": wall_s, "device_s": dev_s / 1e3,
                            "build_s": build_s},
         "speedup_wall": (ev_b / wall_b) / (ev_s / wall_s),
+        "speedup_device": (ev_b / dev_b) / (ev_s / dev_s),
         "accuracy_bf16_batched_vs_f32_sequential": {
-            "mean_rate_hz": mean_rate_b,
+            "mean_rate_hz": float(np.mean(np.concatenate(rates_b))),
             "population_rate_rel_diff_median": float(np.median(rate_rel)),
             "population_rate_rel_diff_p95": float(np.percentile(rate_rel, 95)),
             "isi_cv_batched_mean": float(np.nanmean(cv_b)), "isi_cv_sequential_mean": float(np.nanmean(cv_s)),
             "isi_cv_rel_diff_median": float(np.nanmedian(np.abs(cv_b - cv_s) / cv_s)),
         },
+        "clocks": clocks,
     }
 
 
-def run_serve(args):
-    """Served form: Poisson request stream over 128 resident networks, continuous batching
-    (BF16) vs the plain single-network path one request at a time (FP32)."""
+def run_ensemble(args):
+    m = measure_ensemble(args.members or 64, args.steps, args.window, args.warmup, args.batched_syn)
+    wall_b = m["batched_bf16"]["wall_s"]
+    return {
+        "metric": METRIC, "form": "ensemble", "value": m["batched_bf16"]["events_per_s_wall"],
+        "unit": UNIT + " (ensemble, wall)", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * wall_b / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16-weights/f32-state", "data": "synthetic (seeded DA members generated on the device)",
+        "config": {k: m[k] for k in ("workload", "neurons", "synapses", "batched_graph_launches",
+                                     "batched_synaptic_mode", "sequential_synaptic_mode", "batched_push_variant")},
+        **{k: m[k] for k in ("batched_bf16", "sequential_f32", "speedup_wall", "speedup_device",
+                             "accuracy_bf16_batched_vs_f32_sequential", "clocks")},
+    }
+
+
+def measure_serve(n_nets, n_requests, rate, window, slice_steps, cap_gb, batched_syn, seed=4):
+    """Served form: a Poisson stream of simulate-window requests over resident networks,
+    continuous batching (BF16) vs the plain single-network path one request at a time (FP32),
+    at the same offered rate."""
     import torch
     import __graft_entry__
     __graft_entry__.load_package()
     from dtb_b200 import engine as E
     from dtb_b200 import network as nw
 
-    specs = nw.ensemble_specs(n_members=args.members or 128, seed=4)
+    specs = nw.ensemble_specs(n_members=n_nets, seed=seed)
     rng = np.random.default_rng(12)
     t, reqs = 0.0, []
-    for _ in range(args.requests):
-        t += float(rng.exponential(1.0 / args.rate))
+    for _ in range(n_requests):
+        t += float(rng.exponential(1.0 / rate))
         net = int(rng.integers(len(specs)))
         P = specs[net].n_pops
         ou = (rng.uniform(0.55, 0.65, P).astype(np.float32), rng.uniform(0.18, 0.22, P).astype(np.float32),
               np.full(P, 10.0, np.float32))
-        reqs.append(dict(net=net, iters=args.window, arrival_s=t, ou=ou))
+        reqs.append(dict(net=net, iters=window, arrival_s=t, ou=ou))
     # warm-up past step 300 plus the tuner's samples (every 47 steps) on every network, so each
     # engine (plain path) and the batch (batched path) has autotuned its push before the timed trace
     warm = [dict(net=i, iters=600, arrival_s=0.0, ou=None) for i in range(len(specs))]
 
-    def serve(wt, policy):
+    def serve(wt, policy, syn):
         t0 = time.perf_counter()
-        srv = E.Server(hbm_cap_bytes=args.hbm_cap_gb * 1e9, slice_steps=args.slice, max_batch=64,
-                       syn_mode=E.SYN_PUSH, autotune=True)
+        srv = E.Server(hbm_cap_bytes=cap_gb * 1e9, slice_steps=slice_steps, max_batch=64, syn_mode=syn,
+                       autotune=True)
         for i, sp in enumerate(specs):
             srv.add_structured(sp, weight_type=wt, seed=200 + i)
         build_s = time.perf_counter() - t0
         srv.play(warm, policy)
         torch.cuda.synchronize()
+        sampler = _clock_sampler(torch)
+        sampler.start()
         got = srv.play(reqs, policy)
+        clocks = sampler.stop()
         info = srv.info()
         srv.close()
         lat = np.array([g["latency_s"] for g in got]) * 1e3
         svc = np.array([g["finish_s"] - g["start_s"] for g in got]) * 1e3
         span = max(g["finish_s"] for g in got) - reqs[0]["arrival_s"]
         ev = sum(g["events"] for g in got)
-        rates = np.concatenate([g["freqs"].sum(0) / (args.window * specs[r["net"]].pop_sizes) * 1e4
+        rates = np.concatenate([g["freqs"].sum(0) / (window * specs[r["net"]].pop_sizes) * 1e4
                                 for g, r in zip(got, reqs)])
         return {"latency_ms": {"p50": float(np.percentile(lat, 50)), "p90": float(np.percentile(lat, 90)),
                                "p99": float(np.percentile(lat, 99)), "mean": float(lat.mean()), "max": float(lat.max())},
                 "in_service_ms_mean": float(svc.mean()), "events_per_s": ev / span, "span_s": span,
                 "requests_per_s": len(got) / span, "build_s": build_s,
                 "mean_requests_per_slice": info["batch_members_sum"] / max(1, info["slices"]),
-                "evictions": info["evictions"], "resident_gb": info["resident_bytes"] / 1e9}, rates
+                "evictions": info["evictions"], "resident_gb": info["resident_bytes"] / 1e9,
+                "clocks": clocks}, rates
 
-    batched, rates_b = serve(E.W_BF16, E.SERVE_BATCHED)
-    plain, rates_s = serve(E.W_F32, E.SERVE_SEQUENTIAL)
+    batched, rates_b = serve(E.W_BF16, E.SERVE_BATCHED, E.SYN_PUSH_FIXED if batched_syn == "fixed" else E.SYN_PUSH)
+    plain, rates_s = serve(E.W_F32, E.SERVE_SEQUENTIAL, E.SYN_PUSH)
     rel = np.abs(rates_b - rates_s) / np.maximum(rates_s, 1e-9)
     return {
-        "metric": METRIC, "form": "serve", "value": batched["latency_ms"]["p99"], "unit": "ms p99 request latency",
-        "n_gpus": 1, "steps": args.requests, "warmup": 1, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "bf16-weights/f32-state (batched), f32 (plain)",
-        "data": "synthetic (128 seeded networks of the ensemble distribution generated on the device)",
-        "config": {"workload": f"Poisson arrivals {args.rate}/s, {args.requests} requests of {args.window} steps with "
-                               f"new per-population OU parameters, {len(specs)} resident networks, "
-                               f"HBM cap {args.hbm_cap_gb} GB, slices of {args.slice} steps",
-                   "neurons": int(sum(s.n for s in specs)), "synapses": int(sum(s.n_edges for s in specs))},
+        "workload": f"Poisson arrivals {rate}/s, {n_requests} requests of {window} steps with new per-population "
+                    f"OU parameters, {len(specs)} resident networks of the ensemble distribution, HBM cap "
+                    f"{cap_gb} GB, slices of {slice_steps} steps",
+        "neurons": int(sum(s.n for s in specs)), "synapses": int(sum(s.n_edges for s in specs)),
+        "batched_synaptic_mode": batched_syn, "sequential_synaptic_mode": "push",
         "batched_bf16": batched, "plain_sequential_f32": plain,
         "p50_ratio_plain_over_batched": plain["latency_ms"]["p50"] / batched["latency_ms"]["p50"],
         "p99_ratio_plain_over_batched": plain["latency_ms"]["p99"] / batched["latency_ms"]["p99"],
         "population_rate_rel_diff_median": float(np.median(rel)),
+    }
+
+
+def run_serve(args):
+    m = measure_serve(args.members or 128, args.requests, args.rate, args.window, args.slice, args.hbm_cap_gb,
+                      args.batched_syn)
+    return {
+        "metric": METRIC, "form": "serve", "value": m["batched_bf16"]["latency_ms"]["p99"],
+        "unit": "ms p99 request latency", "n_gpus": 1, "steps": args.requests, "warmup": 1,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16-weights/f32-state (batched), f32 (plain)",
+        "data": "synthetic (seeded networks of the ensemble distribution generated on the device)",
+        "config": {k: m[k] for k in ("workload", "neurons", "synapses", "batched_synaptic_mode",
+                                     "sequential_synaptic_mode")},
+        **{k: m[k] for k in ("batched_bf16", "plain_sequential_f32", "p50_ratio_plain_over_batched",
+                             "p99_ratio_plain_over_batched", "population_rate_rel_diff_median")},
     }
 
 
@@ -628,19 +703,22 @@ def run_precision(args):
 
 
 def run_reference(args):
+    """The reference arm: the C port of the reference CPU model (models/block_new.py) on the
+    box's host cores -- W warm-up and K timed bench steps of the CPU sample; rank 0 only."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
-    cpu = cpu_sample_rate()
+    cpu = cpu_port_run(args.steps, args.warmup)
     v = cpu["value"]
     return {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": cpu["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded regional network, generated on the host)",
         "sim_ms_per_wall_s": cpu["sim_ms_per_wall_s"],
-        "config": {"workload": "5M-neuron regional LIF network, 200 populations, in-degree 1000, f32 weights "
-                               "(timed on a bounded sample of the same construction)"},
+        "config": {"workload": CPU_WORKLOAD, "neurons": CPU_SAMPLE["n"], "populations": CPU_SAMPLE["pops"],
+                   "in_degree": CPU_SAMPLE["in_degree"], "sim_steps_per_bench_step": CPU_SAMPLE["per_step"],
+                   "timed_sim_steps": args.steps * CPU_SAMPLE["per_step"], "timed_s": cpu["wall_s"]},
         "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

@@ -9,9 +9,10 @@
 // entries carry a virtual neuron id (member base + neuron).  Uneven members cost
 // nothing extra: tiles and spiking rows are distributed over the whole GPU.
 //
-// A window of steps of the float push mode is captured once into a CUDA graph
-// (2 kernel nodes per step, 3 with the population-local push) and replayed per window; the push variant is chosen by
-// the same on-line autotuner as a single engine's, on the batch's own spike list.
+// A window of steps of a push mode is captured once into a CUDA graph (2 kernel
+// nodes per step, 5 with the population-local push) and replayed per window; the
+// push variant is chosen by the same on-line autotuner as a single engine's, on
+// the batch's own spike list.
 #include <algorithm>
 #include <cstring>
 
@@ -56,7 +57,7 @@ int Batch::set_members(Engine* const* engines, uint32_t n) {
         if (engines[i]->wtype != engines[0]->wtype) return fail(DTB_UNSUPPORTED, "batch members must share the weight type");
         if (engines[i]->device != engines[0]->device) return fail(DTB_UNSUPPORTED, "batch members must share the device");
     }
-    if (!m.empty() && engines[0]->wtype != wtype) push_tuned[0] = push_tuned[1] = false;
+    if (!m.empty() && engines[0]->wtype != wtype) push_tuned[0] = push_tuned[1] = push_tuned[2] = false;
     m.assign(engines, engines + n);
     wtype = m[0]->wtype;
     sm_count = m[0]->sm_count;
@@ -147,11 +148,12 @@ int Batch::refresh_views() {
 
 int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
     if (rq.iters == 0) return fail(DTB_INVALID_PARAMETER, "iter must be positive");
-    if (rq.prop_mode > DTB_PROP_OR || rq.syn_mode > DTB_SYN_PULL) return fail(DTB_INVALID_PARAMETER, "unknown mode");
+    if (rq.prop_mode > DTB_PROP_OR || rq.syn_mode > DTB_SYN_PUSH_FIXED) return fail(DTB_INVALID_PARAMETER, "unknown mode");
     const bool freq = (rq.flags & DTB_RUN_FREQ) != 0;
     const bool vmean = (rq.flags & DTB_RUN_VMEAN) != 0;
     const bool record = (rq.flags & DTB_RUN_RECORD_SPIKES) != 0;
-    const int exact = rq.syn_mode == DTB_SYN_PUSH_EXACT ? 1 : 0;
+    const int acc = acc_of(rq.syn_mode);
+    const bool pull = rq.syn_mode == DTB_SYN_PULL;
     const bool samples = (rq.flags & (DTB_RUN_SAMPLE_SPIKE | DTB_RUN_SAMPLE_V | DTB_RUN_SAMPLE_IOU)) != 0;
     const bool imean = (rq.flags & DTB_RUN_IMEAN) != 0, rimean = (rq.flags & DTB_RUN_RECEPTOR_IMEAN) != 0;
     const bool sisyn = (rq.flags & DTB_RUN_SAMPLE_ISYN) != 0;
@@ -161,8 +163,10 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
     bool injected = false;
     for (size_t i = 0; i < m.size(); ++i) {
         Engine& e = *m[i];
-        if (rq.syn_mode != DTB_SYN_PULL && !e.has_push) return fail(DTB_UNSUPPORTED, "a member has no out-degree CSR");
-        if (rq.syn_mode == DTB_SYN_PULL && !e.has_pull) return fail(DTB_UNSUPPORTED, "a member has no in-degree CSR");
+        if (!pull && !e.has_push) return fail(DTB_UNSUPPORTED, "a member has no out-degree CSR");
+        if (pull && !e.has_pull) return fail(DTB_UNSUPPORTED, "a member has no in-degree CSR");
+        if (acc == ACC_FIXED && e.fix_shift == 0)
+            return fail(DTB_UNSUPPORTED, "a member's weights do not allow the fixed-point push");
         if ((freq && !outs[i].freqs) || (vmean && !outs[i].vmeans) || (record && !outs[i].spike_bits) ||
             (imean && !outs[i].imeans) || (rimean && !outs[i].receptor_imeans) ||
             (sisyn && !e.sample_order.empty() && !outs[i].sample_isyn))
@@ -181,7 +185,8 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
         if (record) cap = std::min<uint32_t>(cap, std::max<uint32_t>(1u, static_cast<uint32_t>((512ull << 20) / (4ull * e->n_words))));
     }
     for (Engine* e : m) {
-        if (exact) DTB_TRY(e->ensure_dj());
+        if (acc == ACC_EXACT) DTB_TRY(e->ensure_dj());
+        if (acc == ACC_FIXED) DTB_TRY(e->ensure_djf());
         DTB_TRY(e->ensure_hist(cap, record, samples));
         if (isyn_any) DTB_TRY(e->ensure_isum(cap, sisyn));
     }
@@ -190,24 +195,24 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
     if (rq.flags & DTB_RUN_USE_OU) kflags |= kFlagUseOU;
     if (freq || vmean) kflags |= kFlagStats;
     if (record) kflags |= kFlagRecord;
-    if (rq.syn_mode != DTB_SYN_PULL) kflags |= kFlagList;
+    if (!pull) kflags |= kFlagList;
     if (injected) kflags |= kFlagInjected;
     if (samples) kflags |= kFlagSample;
     if (isyn_any) kflags |= kFlagIsyn;
     const int pm = static_cast<int>(rq.prop_mode);
     const int wt = static_cast<int>(wtype);
     uint64_t tune_at = ~0ull;
-    if (rq.syn_mode != DTB_SYN_PULL) {
+    if (!pull) {
         if (autotune) {
             uint64_t total = 0;
             for (Engine* e : m) total += e->n_pad;
             size_class = 64u - static_cast<uint32_t>(__builtin_clzll(total | 1ull));
-            const auto it = tuned_by_size[exact].find(size_class);
-            push_tuned[exact] = it != tuned_by_size[exact].end();
-            if (push_tuned[exact]) push_cfg = it->second;
+            const auto it = tuned_by_size[acc].find(size_class);
+            push_tuned[acc] = it != tuned_by_size[acc].end();
+            if (push_tuned[acc]) push_cfg = it->second;
         }
-        DTB_CU(push_prepare(exact, wt, push_cfg, sm_count, &push_ctas));
-        if (autotune && !push_tuned[exact]) {
+        DTB_CU(push_prepare(acc, wt, push_cfg, sm_count, &push_ctas));
+        if (autotune && !push_tuned[acc]) {
             const uint64_t settle = 300;
             const uint64_t st = m[0]->steps;
             tune_at = st >= settle ? 1 : (settle - st < rq.iters ? settle - st : ~0ull);
@@ -230,23 +235,26 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
             ++launches;
         }
         DTB_CU(cudaEventRecord(ev0, stream));
-        // Graph-replayed window: float push mode, no tuning pending inside it.
-        const bool graphable = use_graph && rq.syn_mode == DTB_SYN_PUSH &&
-                               !(tune_at >= done && tune_at < done + rows);
+        // Graph-replayed window: a push mode with no tuning pending inside it.  A chunk that
+        // starts a run folds nothing into J on its first step, and the last chunk of an
+        // exact or fixed run ends by folding the sums into J, so both are in the key.
+        const bool last_chunk = done + rows == rq.iters;
+        const bool graphable = use_graph && !pull && !(tune_at >= done && tune_at < done + rows);
         if (graphable) {
-            const uint64_t key[6] = {rows, kflags, static_cast<uint64_t>(pm),
+            const uint64_t key[9] = {rows, kflags, static_cast<uint64_t>(pm),
                                      static_cast<uint64_t>(push_cfg.kind) * 100000 + push_cfg.param * 100 + push_cfg.lpr,
-                                     push_ctas, 1};
+                                     push_ctas, rq.syn_mode, done == 0, last_chunk, 1};
             if (!graph || std::memcmp(key, graph_key, sizeof(key)) != 0) {
                 if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
                 cudaGraph_t g = nullptr;
                 DTB_CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
                 cudaError_t ce = cudaSuccess;
                 for (uint32_t s = 0; s < rows && ce == cudaSuccess; ++s) {
-                    ce = launch_lif(lb, J_DIRECT, kflags, pm, stream);
-                    if (ce == cudaSuccess) ce = launch_push(lb, 0, wt, push_cfg, push_ctas, stream);
-                    if (ce == cudaSuccess && isyn_any) ce = launch_stat_isyn(lb, 0, sm_count, stream);
+                    ce = launch_lif(lb, jmode_of(rq.syn_mode, done + s == 0), kflags, pm, stream);
+                    if (ce == cudaSuccess) ce = launch_push(lb, acc, wt, push_cfg, push_ctas, stream);
+                    if (ce == cudaSuccess && isyn_any) ce = launch_stat_isyn(lb, acc, sm_count, stream);
                 }
+                if (ce == cudaSuccess && last_chunk && acc != ACC_FLOAT) ce = launch_fold_finish(lb, acc, stream);
                 const cudaError_t ee = cudaStreamEndCapture(stream, &g);
                 if (ce != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(ce, "graph capture"); }
                 if (ee != cudaSuccess) return cuda_fail(ee, "cudaStreamEndCapture");
@@ -257,47 +265,48 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
             }
             DTB_CU(cudaGraphLaunch(graph, stream));
             ++graph_launches;
-            launches += (2 + push_extra_launches(lb, 0, push_cfg) + (isyn_any ? 1u : 0u)) * rows;
+            launches += (2 + push_extra_launches(lb, acc, push_cfg) + (isyn_any ? 1u : 0u)) * rows +
+                        (last_chunk && acc != ACC_FLOAT ? 1u : 0u);
         } else {
             for (uint32_t s = 0; s < rows; ++s) {
                 const bool first = (done + s) == 0;
-                if (rq.syn_mode == DTB_SYN_PULL) {
+                if (pull) {
                     DTB_CU(launch_pull(lb, first ? 0 : 1, wt, kflags, pm, stream));
                     ++launches;
                     continue;
                 }
-                DTB_CU(launch_lif(lb, exact ? (first ? J_ASIS : J_FOLD) : J_DIRECT, kflags, pm, stream));
+                DTB_CU(launch_lif(lb, jmode_of(rq.syn_mode, first), kflags, pm, stream));
                 if (tune_at == done + s) {
                     std::vector<NetView> v(m.size());
                     for (size_t i = 0; i < m.size(); ++i) v[i] = m[i]->view;
-                    if (tune_class != (size_class << 1 | static_cast<uint32_t>(exact))) {
+                    if (tune_class != (size_class << 2 | static_cast<uint32_t>(acc))) {
                         tune.reset();       // samples of another membership size or mode do not carry over
                         tune.observe = 0;   // a batch serves requests: tune on the first busy steps
                         tune.want = 2;
-                        tune_class = size_class << 1 | static_cast<uint32_t>(exact);
+                        tune_class = size_class << 2 | static_cast<uint32_t>(acc);
                     }
-                    DTB_TRY(tune_push_views(lb, v, exact, wt, sm_count, stream, tev, tune));
+                    DTB_TRY(tune_push_views(lb, v, acc, wt, sm_count, stream, tev, tune));
                     if (tune.tuned) {
                         push_cfg = tune.best;
-                        push_tuned[exact] = true;
-                        tuned_by_size[exact][size_class] = push_cfg;
+                        push_tuned[acc] = true;
+                        tuned_by_size[acc][size_class] = push_cfg;
                         tune.reset();
-                        DTB_CU(push_prepare(exact, wt, push_cfg, sm_count, &push_ctas));
+                        DTB_CU(push_prepare(acc, wt, push_cfg, sm_count, &push_ctas));
                     } else {
                         tune_at = tune.next_step(tune_at);
                     }
                 }
-                DTB_CU(launch_push(lb, exact, wt, push_cfg, push_ctas, stream));
-                launches += 2 + push_extra_launches(lb, exact, push_cfg);
+                DTB_CU(launch_push(lb, acc, wt, push_cfg, push_ctas, stream));
+                launches += 2 + push_extra_launches(lb, acc, push_cfg);
                 if (isyn_any) {
-                    DTB_CU(launch_stat_isyn(lb, exact, sm_count, stream));
+                    DTB_CU(launch_stat_isyn(lb, acc, sm_count, stream));
                     ++launches;
                 }
             }
-        }
-        if (done + rows == rq.iters) {
-            if (exact) { DTB_CU(launch_fold_finish(lb, stream)); ++launches; }
-            if (rq.syn_mode == DTB_SYN_PULL) { DTB_CU(launch_gather_finish(lb, wt, stream)); ++launches; }
+            if (last_chunk) {
+                if (acc != ACC_FLOAT && !pull) { DTB_CU(launch_fold_finish(lb, acc, stream)); ++launches; }
+                if (pull) { DTB_CU(launch_gather_finish(lb, wt, stream)); ++launches; }
+            }
         }
         DTB_CU(cudaEventRecord(ev1, stream));
         DTB_CU(cudaEventSynchronize(ev1));
@@ -381,10 +390,11 @@ int32_t dtb_batch_set_push_variant(void* batch, int32_t kind, int32_t param) {
     Batch* b = static_cast<Batch*>(batch);
     if (kind < 0) {
         b->autotune = true;
-        b->push_tuned[0] = b->push_tuned[1] = false;
+        for (int a = 0; a < 3; ++a) {
+            b->push_tuned[a] = false;
+            b->tuned_by_size[a].clear();
+        }
         b->tune.reset();
-        b->tuned_by_size[0].clear();
-        b->tuned_by_size[1].clear();
         return DTB_OK;
     }
     dtb::PushCfg cfg;

@@ -37,17 +37,17 @@ public:
     LaunchBatch lb{};
     PushCfg push_cfg{PUSH_REG, 8, 32};
     uint32_t push_ctas = 0;
-    bool push_tuned[2] = {false, false};
+    bool push_tuned[3] = {false, false, false};
     bool autotune = true;
     // tuned variant per size class (bit length of the batch's padded neuron count), so a
     // serving batch whose membership changes keeps a variant fit for its current size
-    std::map<uint32_t, PushCfg> tuned_by_size[2];
+    std::map<uint32_t, PushCfg> tuned_by_size[3];
     uint32_t size_class = 0;
     TuneResult tune;                      // samples of the size class being tuned
-    uint32_t tune_class = ~0u;            // that class (size class << 1 | exact)
+    uint32_t tune_class = ~0u;            // that class (size class << 2 | accumulator mode)
     bool use_graph = true;
     cudaGraphExec_t graph = nullptr;
-    uint64_t graph_key[6] = {0, 0, 0, 0, 0, 0};
+    uint64_t graph_key[9] = {};
     uint32_t graph_launches = 0;
 };
 

@@ -4,6 +4,7 @@
 //   V[n_pad], i_ou[n_pad], t_last[n_pad]         float32 SoA, read with 128-bit loads
 //   J[n_pad]                                      float4 (AMPA, NMDA, GABAa, GABAb)
 //   dJ[n_pad*4]                                   int64 fixed point (scale 2^32), exact mode only
+//   dJf[n_pad*2]                                  two u32 fixed-point sums (scale 2^s) per u64, fixed mode only
 //   bits[2][n_words]                              propagated spikes, double-buffered by step parity
 //   out_ptr[n+1] u64, out_col[S] u32, out_w[S]    out-degree CSR (push); col = post | kind << 31
 //   in_ptr[n+1]  u64, in_col[S]  u32, in_w[S]     in-degree CSR (pull);  col = pre  | kind << 31
@@ -45,7 +46,13 @@ constexpr uint32_t kErrNoiseExhausted = 2u;
 constexpr uint32_t kErrIndex = 4u;
 constexpr uint32_t kErrTimeout = 8u;      // a bounded wait gave up
 
-enum JMode : int { J_DIRECT = 0, J_FOLD = 1, J_ASIS = 2 };
+// J_DIRECT: J complete on entry, J*decay written back, the float push adds into J;
+// J_FOLD: J + exact 64-bit sums (dJ) folded on entry; J_ASIS: J complete, unchanged;
+// J_FIXF: J + packed 32-bit fixed-point sums (dJf) folded on entry.
+enum JMode : int { J_DIRECT = 0, J_FOLD = 1, J_ASIS = 2, J_FIXF = 3 };
+// Accumulator of a push launch: float reductions into J, exact 64-bit sums into dJ,
+// or packed 32-bit fixed-point sums into dJf.
+enum AccMode : int { ACC_FLOAT = 0, ACC_EXACT = 1, ACC_FIXED = 2 };
 enum WType : int { W_F32 = 0, W_BF16 = 1, W_F16 = 2, W_U8 = 3 };
 enum PropMode : int { PROP_THRESHOLD = 0, PROP_NOISE = 1, PROP_OR = 2 };
 
@@ -133,6 +140,14 @@ struct NetView {
     const uint4* pop_loc;          // [n_pops] {k_a, window width, rb(a) low word, rb(a) high word}
     const uint4* win_tab;          // [n_windows] {population, first neuron, end neuron, window index | s << 16}
     uint32_t n_windows;
+    // Fixed-point push (DTB_SYN_PUSH_FIXED): one step's input to neuron i as two
+    // pairs of unsigned 32-bit sums in units of 2^-fix_shift, receptor pair k in
+    // dJf[2 i + k] = (sum of w.y) << 32 | (sum of w.x).  fix_shift is chosen at
+    // creation so no field can carry (every weight >= 0, in-degree x max w x
+    // 2^fix_shift < 2^32); 0 when the network does not allow the mode.
+    unsigned long long* dJf;       // [n_pad * 2]
+    uint32_t fix_shift;
+    float fix_scale, fix_unscale;  // 2^fix_shift, 2^-fix_shift
 };
 
 // Batch-wide spike list written by the LIF kernel and consumed by the push kernel.
@@ -285,6 +300,17 @@ __device__ inline float fix_to_float(long long x) {
 
 __device__ inline long long float_to_fix(float w) {
     return __float2ll_rn(__fmul_rn(w, kFixScale));
+}
+
+// Fixed-mode pieces: a weight pair as one packed u64 addend, and a 32-bit field
+// back to float (u is rounded to float32 once; the power-of-two scale is exact).
+__device__ inline unsigned long long pack_fixed(float2 w, float scale) {
+    const unsigned long long lo = __float2uint_rn(__fmul_rn(w.x, scale));
+    const unsigned long long hi = __float2uint_rn(__fmul_rn(w.y, scale));
+    return (hi << 32) | lo;
+}
+__device__ inline float fixed_field(unsigned long long packed, int hi, float unscale) {
+    return __fmul_rn(__uint2float_rn(static_cast<uint32_t>(hi ? packed >> 32 : packed)), unscale);
 }
 
 // Population of neuron i: largest p with pop_off[p] <= i.

@@ -46,6 +46,7 @@ static uint32_t round_up(uint32_t x, uint32_t m) { return (x + m - 1) / m * m; }
 
 Engine::~Engine() {
     if (stream) cudaStreamSynchronize(stream);
+    if (graph) cudaGraphExecDestroy(graph);
     for (void* p : allocs) cudaFree(p);
     if (h_cnt) cudaFreeHost(h_cnt);
     if (h_vsum) cudaFreeHost(h_vsum);
@@ -220,6 +221,10 @@ int Engine::refresh_view() {
     v.pop_loc = pop_loc;
     v.win_tab = win_tab;
     v.n_windows = n_windows;
+    v.dJf = dJf;
+    v.fix_shift = fix_shift;
+    v.fix_scale = fix_shift ? static_cast<float>(std::ldexp(1.0, static_cast<int>(fix_shift))) : 0.0f;
+    v.fix_unscale = fix_shift ? static_cast<float>(std::ldexp(1.0, -static_cast<int>(fix_shift))) : 0.0f;
     view = v;
     DTB_CU(cudaMemcpyAsync(view_dev, &view, sizeof(NetView), cudaMemcpyHostToDevice, stream));
     DTB_CU(cudaStreamSynchronize(stream));
@@ -259,6 +264,27 @@ bool push_cfg_from_abi(int kind, int param, PushCfg& cfg) {
     for (const PushCfg& c : kPushCands)
         if (c.kind == cfg.kind && c.param == cfg.param && c.lpr == cfg.lpr) return true;
     return false;
+}
+
+int acc_of(uint32_t syn_mode) {
+    return syn_mode == DTB_SYN_PUSH_EXACT ? ACC_EXACT : syn_mode == DTB_SYN_PUSH_FIXED ? ACC_FIXED : ACC_FLOAT;
+}
+
+int jmode_of(uint32_t syn_mode, bool first) {
+    switch (syn_mode) {
+        case DTB_SYN_PUSH_EXACT: return first ? J_ASIS : J_FOLD;
+        case DTB_SYN_PUSH_FIXED: return first ? J_ASIS : J_FIXF;
+        default: return J_DIRECT;
+    }
+}
+
+uint32_t fixed_shift_for(uint64_t max_in_degree, double max_w, bool negative) {
+    if (negative || !(max_w >= 0.0) || !std::isfinite(max_w)) return 0;
+    // device weight types round the input (bf16/f16 by up to 2^-8 relative): bound with margin
+    const double w = std::max(max_w, 1e-30) * (1.0 + 1.0 / 128.0);
+    for (int sh = 32; sh >= 12; --sh)
+        if (static_cast<double>(max_in_degree) * (w * std::ldexp(1.0, sh) + 0.5) < 4294967295.0) return static_cast<uint32_t>(sh);
+    return 0;
 }
 
 // Population-local push tables.  A population gets k = ceil(size / kLocalWin)
@@ -499,6 +525,21 @@ int Engine::create_from_arrays(const dtb_network_arrays& a, const dtb_options& o
         DTB_TRY(dalloc(excl, n_words));
         DTB_CU(cudaMemcpyAsync(excl, ex.data(), sizeof(uint32_t) * n_words, cudaMemcpyHostToDevice, stream));
     }
+    {
+        // fixed-mode scale: largest in-degree and weight of the network
+        std::vector<uint32_t> indeg(n, 0);
+        double max_w = 0.0;
+        bool negative = false;
+        for (uint64_t e = 0; e < n_edges; ++e) {
+            ++indeg[a.output_neuron_idx[e]];
+            float w0, w1;
+            weight_to_f32(a.weight, a.weight_type, e, w0, w1);
+            negative |= (w0 < 0.0f) || (w1 < 0.0f) || !std::isfinite(w0) || !std::isfinite(w1);
+            max_w = std::max(max_w, static_cast<double>(std::max(w0, w1)));
+        }
+        const uint32_t deg = n ? *std::max_element(indeg.begin(), indeg.end()) : 0u;
+        fix_shift = fixed_shift_for(deg, max_w, negative);
+    }
     DTB_TRY(upload_csr_host(a.input_neuron_idx, a.output_neuron_idx, a.input_channel_offset, a.weight, a.weight_type,
                             opt.build_push != 0, opt.build_pull != 0));
     DTB_TRY(upload_params());
@@ -525,6 +566,7 @@ int Engine::create_structured(const dtb_structured_spec& s, const dtb_options& o
     if (total >= 0x7FFFFFFFull - kPad) return fail(DTB_UNSUPPORTED, "more than 2^31 neurons");
     DTB_TRY(init_common(opt, static_cast<uint32_t>(total)));
     n_edges = static_cast<uint64_t>(n) * s.in_degree;
+    fix_shift = fixed_shift_for(s.in_degree, 1.0, false);   // generated weights lie in [0, 1)
     P = s.n_pops;
     pop_ids.resize(P);
     pop_off.resize(P + 1);
@@ -632,6 +674,13 @@ int Engine::create_from_npz(const std::string& path, const dtb_options& opt) {
 int Engine::ensure_dj() {
     if (dJ) return DTB_OK;
     DTB_TRY(dalloc(dJ, static_cast<size_t>(n_pad) * 4));
+    DTB_CU(cudaStreamSynchronize(stream));
+    return refresh_view();
+}
+
+int Engine::ensure_djf() {
+    if (dJf) return DTB_OK;
+    DTB_TRY(dalloc(dJf, static_cast<size_t>(n_pad) * 2));
     DTB_CU(cudaStreamSynchronize(stream));
     return refresh_view();
 }
@@ -794,9 +843,12 @@ int Engine::finish_hist(uint32_t rows, uint32_t out_row0, const dtb_run_output& 
 int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     if (rq.iters == 0) return fail(DTB_INVALID_PARAMETER, "iter must be positive");
     if (rq.prop_mode > DTB_PROP_OR) return fail(DTB_INVALID_PARAMETER, "unknown prop_mode");
-    if (rq.syn_mode > DTB_SYN_PULL) return fail(DTB_INVALID_PARAMETER, "unknown syn_mode");
-    if (rq.syn_mode != DTB_SYN_PULL && !has_push) return fail(DTB_UNSUPPORTED, "network was built without the out-degree CSR");
-    if (rq.syn_mode == DTB_SYN_PULL && !has_pull) return fail(DTB_UNSUPPORTED, "network was built without the in-degree CSR");
+    if (rq.syn_mode > DTB_SYN_PUSH_FIXED) return fail(DTB_INVALID_PARAMETER, "unknown syn_mode");
+    const bool pull = rq.syn_mode == DTB_SYN_PULL;
+    if (!pull && !has_push) return fail(DTB_UNSUPPORTED, "network was built without the out-degree CSR");
+    if (pull && !has_pull) return fail(DTB_UNSUPPORTED, "network was built without the in-degree CSR");
+    if (rq.syn_mode == DTB_SYN_PUSH_FIXED && fix_shift == 0)
+        return fail(DTB_UNSUPPORTED, "fixed-point push needs non-negative weights whose in-degree sums fit 32 bits");
     const bool freq = (rq.flags & DTB_RUN_FREQ) != 0;
     const bool vmean = (rq.flags & DTB_RUN_VMEAN) != 0;
     const bool record = (rq.flags & DTB_RUN_RECORD_SPIKES) != 0;
@@ -815,7 +867,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     const bool imean = (rq.flags & DTB_RUN_IMEAN) != 0, rimean = (rq.flags & DTB_RUN_RECEPTOR_IMEAN) != 0;
     if ((imean && !out.imeans) || (rimean && !out.receptor_imeans))
         return fail(DTB_INVALID_PARAMETER, "requested imean buffer is NULL");
-    if ((imean || rimean || sisyn) && rq.syn_mode == DTB_SYN_PULL)
+    if ((imean || rimean || sisyn) && pull)
         return fail(DTB_UNSUPPORTED, "synaptic-current outputs need a push mode (the pull kernel completes J one step later)");
     const bool isyn_any = imean || rimean || sisyn;
     const bool injected = noise_src == DTB_NOISE_INJECTED;
@@ -824,7 +876,9 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
         if (used + rq.iters > inj_rows) return fail(DTB_INVALID_PARAMETER, "not enough injected noise rows for this run");
         if (rq.prop_mode != DTB_PROP_THRESHOLD && !inj_u) return fail(DTB_INVALID_PARAMETER, "noise train needs injected uniforms");
     }
-    if (rq.syn_mode == DTB_SYN_PUSH_EXACT) DTB_TRY(ensure_dj());
+    const int acc = acc_of(rq.syn_mode);
+    if (acc == ACC_EXACT) DTB_TRY(ensure_dj());
+    if (acc == ACC_FIXED) DTB_TRY(ensure_djf());
     uint32_t cap = std::min<uint32_t>(rq.iters, 4096u);
     if (record) cap = std::min<uint32_t>(cap, std::max<uint32_t>(1u, static_cast<uint32_t>((512ull << 20) / (4ull * n_words))));
     DTB_TRY(ensure_hist(cap, record, samples));
@@ -834,16 +888,16 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     if (rq.flags & DTB_RUN_USE_OU) kflags |= kFlagUseOU;
     if (freq || vmean) kflags |= kFlagStats;
     if (record) kflags |= kFlagRecord;
-    if (rq.syn_mode != DTB_SYN_PULL) kflags |= kFlagList;
+    if (!pull) kflags |= kFlagList;
     if (injected) kflags |= kFlagInjected;
     const LaunchBatch b = single_batch();
     const int pm = static_cast<int>(rq.prop_mode);
+    const int wt = static_cast<int>(wtype);
     const bool time_k = (rq.flags & DTB_RUN_TIME_KERNELS) != 0;
-    const int exact = rq.syn_mode == DTB_SYN_PUSH_EXACT ? 1 : 0;
     uint64_t tune_at = ~0ull;   // run-relative step at which the push variants are timed
-    if (rq.syn_mode != DTB_SYN_PULL) {
-        DTB_CU(push_prepare(exact, static_cast<int>(wtype), push_cfg, sm_count, &push_ctas));
-        if (autotune && !push_tuned[exact]) {
+    if (!pull) {
+        DTB_CU(push_prepare(acc, wt, push_cfg, sm_count, &push_ctas));
+        if (autotune && !push_tuned[acc]) {
             // time the variants on a live spike list, once the network has left its quiet start
             const uint64_t settle = 300;
             tune_at = steps >= settle ? 1 : (settle - steps < rq.iters ? settle - steps : ~0ull);
@@ -857,11 +911,13 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     uint32_t done = 0;
     while (done < rq.iters) {
         const uint32_t rows = std::min(cap, rq.iters - done);
+        const bool last_chunk = done + rows == rq.iters;
         DTB_TRY(begin_run_chunk(steps, rows, freq || vmean));
         if (isyn_any) DTB_CU(cudaMemsetAsync(hist_isum, 0, sizeof(long long) * rows * P * 5, stream));
         ++launches;
         std::vector<std::pair<int, size_t>> timed;   // (kernel class, event pair index)
         if (time_k) DTB_TRY(ensure_timing_events(6 * static_cast<size_t>(rows) + 4));   // 2 events x (3 launches per step + 1)
+        uint32_t chunk_launches = 0;
         auto timed_launch = [&](int cls, auto&& fn) -> int {
             if (time_k) DTB_CU(cudaEventRecord(tev[2 * timed.size()], stream));
             DTB_CU(fn());
@@ -869,43 +925,63 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
                 DTB_CU(cudaEventRecord(tev[2 * timed.size() + 1], stream));
                 timed.emplace_back(cls, timed.size());
             }
-            ++launches;
+            ++chunk_launches;
+            return DTB_OK;
+        };
+        // the chunk's launches; `tuning` false while a graph is being captured
+        auto issue = [&](bool tuning) -> int {
+            for (uint32_t s = 0; s < rows; ++s) {
+                const bool first = (done + s) == 0;
+                if (pull) {
+                    DTB_TRY(timed_launch(2, [&] { return launch_pull(b, first ? 0 : 1, wt, kflags, pm, stream); }));
+                    continue;
+                }
+                DTB_TRY(timed_launch(0, [&] { return launch_lif(b, jmode_of(rq.syn_mode, first), kflags, pm, stream); }));
+                if (tuning && tune_at == done + s) {
+                    DTB_TRY(tune_push(b, acc));
+                    if (!push_tuned[acc]) tune_at = tune_acc[acc].next_step(tune_at);
+                }
+                DTB_TRY(timed_launch(1, [&] { return launch_push(b, acc, wt, push_cfg, push_ctas, stream); }));
+                chunk_launches += push_extra_launches(b, acc, push_cfg);
+                if (isyn_any) DTB_TRY(timed_launch(3, [&] { return launch_stat_isyn(b, acc, sm_count, stream); }));
+            }
+            if (last_chunk && (acc == ACC_EXACT || acc == ACC_FIXED) && !pull)
+                DTB_TRY(timed_launch(3, [&] { return launch_fold_finish(b, acc, stream); }));
+            if (last_chunk && pull) DTB_TRY(timed_launch(3, [&] { return launch_gather_finish(b, wt, stream); }));
             return DTB_OK;
         };
         DTB_CU(cudaEventRecord(ev0, stream));
-        for (uint32_t s = 0; s < rows; ++s) {
-            const bool first = (done + s) == 0;
-            switch (rq.syn_mode) {
-                case DTB_SYN_PUSH:
-                    DTB_TRY(timed_launch(0, [&] { return launch_lif(b, J_DIRECT, kflags, pm, stream); }));
-                    if (tune_at == done + s) {
-                        DTB_TRY(tune_push(b, 0));
-                        if (!push_tuned[0]) tune_at = tune_acc[0].next_step(tune_at);
-                    }
-                    DTB_TRY(timed_launch(1, [&] { return launch_push(b, 0, static_cast<int>(wtype), push_cfg, push_ctas, stream); }));
-                    launches += push_extra_launches(b, 0, push_cfg);
-                    if (isyn_any) DTB_TRY(timed_launch(3, [&] { return launch_stat_isyn(b, 0, sm_count, stream); }));
-                    break;
-                case DTB_SYN_PUSH_EXACT:
-                    DTB_TRY(timed_launch(0, [&] { return launch_lif(b, first ? J_ASIS : J_FOLD, kflags, pm, stream); }));
-                    if (tune_at == done + s) {
-                        DTB_TRY(tune_push(b, 1));
-                        if (!push_tuned[1]) tune_at = tune_acc[1].next_step(tune_at);
-                    }
-                    DTB_TRY(timed_launch(1, [&] { return launch_push(b, 1, static_cast<int>(wtype), push_cfg, push_ctas, stream); }));
-                    if (isyn_any) DTB_TRY(timed_launch(3, [&] { return launch_stat_isyn(b, 1, sm_count, stream); }));
-                    break;
-                default:
-                    DTB_TRY(timed_launch(2, [&] { return launch_pull(b, first ? 0 : 1, static_cast<int>(wtype), kflags, pm, stream); }));
-                    break;
-            }
+        // a push chunk with no tuning pending and no per-kernel timing: replay its graph once its
+        // shape has been seen before (the kernels read every per-run value from device memory)
+        const bool graphable = use_graph && !pull && !time_k && !(tune_at >= done && tune_at < done + rows);
+        const uint64_t key[10] = {rows, kflags, static_cast<uint64_t>(pm), rq.syn_mode,
+                                  static_cast<uint64_t>(push_cfg.kind) * 100000 + push_cfg.param * 100 + push_cfg.lpr,
+                                  push_ctas, done == 0, last_chunk, isyn_any, 1};
+        if (graphable && graph && std::memcmp(key, graph_key, sizeof(key)) == 0) {
+            DTB_CU(cudaGraphLaunch(graph, stream));
+            ++graph_launches;
+            // launches of the replayed chunk, counted as the eager path does
+            chunk_launches = rows * (2u + push_extra_launches(b, acc, push_cfg) + (isyn_any ? 1u : 0u)) +
+                             (last_chunk && acc != ACC_FLOAT ? 1u : 0u);
+        } else if (graphable && std::memcmp(key, seen_key, sizeof(key)) == 0) {
+            if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+            cudaGraph_t g = nullptr;
+            DTB_CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            const int st = issue(false);
+            const cudaError_t ee = cudaStreamEndCapture(stream, &g);
+            if (st != DTB_OK) { if (g) cudaGraphDestroy(g); return st; }
+            if (ee != cudaSuccess) return cuda_fail(ee, "cudaStreamEndCapture");
+            const cudaError_t ie = cudaGraphInstantiate(&graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) { graph = nullptr; return cuda_fail(ie, "cudaGraphInstantiate"); }
+            std::memcpy(graph_key, key, sizeof(key));
+            DTB_CU(cudaGraphLaunch(graph, stream));
+            ++graph_launches;
+        } else {
+            if (graphable) std::memcpy(seen_key, key, sizeof(key));
+            DTB_TRY(issue(true));
         }
-        if (done + rows == rq.iters) {
-            if (rq.syn_mode == DTB_SYN_PUSH_EXACT)
-                DTB_TRY(timed_launch(3, [&] { return launch_fold_finish(b, stream); }));
-            if (rq.syn_mode == DTB_SYN_PULL)
-                DTB_TRY(timed_launch(3, [&] { return launch_gather_finish(b, static_cast<int>(wtype), stream); }));
-        }
+        launches += chunk_launches;
         DTB_CU(cudaEventRecord(ev1, stream));
         DTB_CU(cudaEventSynchronize(ev1));
         float ms = 0.f;
@@ -967,7 +1043,7 @@ static void pick_best(TuneResult& res) {
 // Time every push variant on the spike list the LIF kernel just wrote, into
 // scratch accumulators so the simulation state is untouched, and return the
 // fastest.  `views` are the host copies of the launch's networks.
-int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int exact, int wtype, int sm_count,
+int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int acc, int wtype, int sm_count,
                     cudaStream_t stream, cudaEvent_t ev[2], TuneResult& res) {
     uint32_t count = 0;
     DTB_CU(cudaMemcpyAsync(&count, b.spikes.count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
@@ -986,7 +1062,7 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
         return DTB_OK;
     }
     res.sampled = true;
-    const size_t per = exact ? sizeof(long long) * 4 : sizeof(float4);
+    const size_t per = acc == ACC_EXACT ? sizeof(long long) * 4 : acc == ACC_FIXED ? sizeof(unsigned long long) * 2 : sizeof(float4);
     void* scratch = nullptr;
     NetView* tview = nullptr;
     DTB_CU(cudaMalloc(&scratch, per * total_n));
@@ -998,7 +1074,9 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
     size_t off = 0;
     for (NetView& v : tv) {
         char* base = static_cast<char*>(scratch) + off * per;
-        if (exact) v.dJ = reinterpret_cast<long long*>(base); else v.J = reinterpret_cast<float4*>(base);
+        if (acc == ACC_EXACT) v.dJ = reinterpret_cast<long long*>(base);
+        else if (acc == ACC_FIXED) v.dJf = reinterpret_cast<unsigned long long*>(base);
+        else v.J = reinterpret_cast<float4*>(base);
         off += v.n_pad;
     }
     std::vector<TuneEntry> step;
@@ -1008,14 +1086,14 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
         LaunchBatch tb = b;
         tb.nets = tview;
         for (const PushCfg& c : kPushCands) {
-            if (c.kind == PUSH_LOCAL && (exact || b.windows_total == 0)) continue;
+            if (c.kind == PUSH_LOCAL && (acc == ACC_EXACT || b.windows_total == 0)) continue;
             uint32_t ctas = 0;
-            DTB_CU(push_prepare(exact, wtype, c, sm_count, &ctas));
+            DTB_CU(push_prepare(acc, wtype, c, sm_count, &ctas));
             float ms_min = 1e30f;
             for (int rep = 0; rep < 3; ++rep) {
                 set_u32_kernel<<<1, 1, 0, stream>>>(b.spikes.count, count);
                 DTB_CU(cudaEventRecord(ev[0], stream));
-                DTB_CU(launch_push(tb, exact, wtype, c, ctas, stream));
+                DTB_CU(launch_push(tb, acc, wtype, c, ctas, stream));
                 DTB_CU(cudaEventRecord(ev[1], stream));
                 DTB_CU(cudaEventSynchronize(ev[1]));
                 float ms = 0.f;
@@ -1048,19 +1126,19 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
     return DTB_OK;
 }
 
-int Engine::tune_push(const LaunchBatch& b, int exact) {
+int Engine::tune_push(const LaunchBatch& b, int acc) {
     if (!tune_ev[0]) {
         DTB_CU(cudaEventCreate(&tune_ev[0]));
         DTB_CU(cudaEventCreate(&tune_ev[1]));
     }
-    TuneResult& res = tune_acc[exact];
-    DTB_TRY(tune_push_views(b, {view}, exact, static_cast<int>(wtype), sm_count, stream, tune_ev, res));
+    TuneResult& res = tune_acc[acc];
+    DTB_TRY(tune_push_views(b, {view}, acc, static_cast<int>(wtype), sm_count, stream, tune_ev, res));
     if (!res.tuned) return DTB_OK;
     push_cfg = res.best;
-    push_tuned[exact] = true;
+    push_tuned[acc] = true;
     tuned_ms = res.best_ms;
     tune_report = res.report;
-    DTB_CU(push_prepare(exact, static_cast<int>(wtype), push_cfg, sm_count, &push_ctas));
+    DTB_CU(push_prepare(acc, static_cast<int>(wtype), push_cfg, sm_count, &push_ctas));
     return DTB_OK;
 }
 
@@ -1088,6 +1166,8 @@ int Engine::info(dtb_engine_info& inf) const {
     inf.push_param = static_cast<uint32_t>(push_cfg.lpr != 32 ? 1000 + push_cfg.lpr : push_cfg.param);
     inf.push_tuned_ms = tuned_ms;
     inf.local_windows = n_windows;
+    inf.fixed_shift = fix_shift;
+    inf.graph_launches = graph_launches;
     return DTB_OK;
 }
 
@@ -1386,6 +1466,7 @@ int Engine::load_state(const void* blob, uint64_t bytes) {
     DTB_CU(cudaMemcpyAsync(bits0, p, 4ull * n_words, cudaMemcpyHostToDevice, stream)); p += 4ull * n_words;
     DTB_CU(cudaMemcpyAsync(bits1, p, 4ull * n_words, cudaMemcpyHostToDevice, stream));
     if (dJ) DTB_CU(cudaMemsetAsync(dJ, 0, sizeof(long long) * 4 * n_pad, stream));
+    if (dJf) DTB_CU(cudaMemsetAsync(dJf, 0, sizeof(unsigned long long) * 2 * n_pad, stream));
     set_clock_kernel<<<1, 1, 0, stream>>>(clock, h.t, h.steps);
     DTB_CU(cudaGetLastError());
     DTB_CU(cudaStreamSynchronize(stream));
@@ -1509,15 +1590,29 @@ int32_t dtb_set_push_variant(void* engine, int32_t kind, int32_t param) {
     Engine* e = as_engine(engine);
     if (kind < 0) {
         e->autotune = true;
-        e->push_tuned[0] = e->push_tuned[1] = false;
-        e->tune_acc[0].reset();
-        e->tune_acc[1].reset();
+        for (int a = 0; a < 3; ++a) {
+            e->push_tuned[a] = false;
+            e->tune_acc[a].reset();
+        }
         return DTB_OK;
     }
     dtb::PushCfg cfg;
     if (!dtb::push_cfg_from_abi(kind, param, cfg)) return dtb::fail(DTB_INVALID_PARAMETER, "unknown push variant");
     e->push_cfg = cfg;
     e->autotune = false;
+    return DTB_OK;
+}
+
+int32_t dtb_set_graph(void* engine, int32_t enable) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    Engine* e = as_engine(engine);
+    e->use_graph = enable != 0;
+    if (!e->use_graph && e->graph) {
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+    }
+    std::memset(e->graph_key, 0, sizeof(e->graph_key));
+    std::memset(e->seen_key, 0, sizeof(e->seen_key));
     return DTB_OK;
 }
 

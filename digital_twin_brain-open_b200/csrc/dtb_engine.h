@@ -57,8 +57,16 @@ __global__ void set_u32_kernel(uint32_t* p, uint32_t v);
 // Reads the live spike count and, when the step qualifies as a sample (TuneResult),
 // times every push variant on it and adds the times to `res`.  A list of fewer than
 // 0.2 % of the neurons never qualifies.
-int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int exact, int wtype, int sm_count,
+int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int acc, int wtype, int sm_count,
                     cudaStream_t stream, cudaEvent_t ev[2], TuneResult& res);
+// AccMode of a push syn_mode, and the LIF kernel's J mode for a step of that mode
+// (the first step of a run takes J as complete).
+int acc_of(uint32_t syn_mode);
+int jmode_of(uint32_t syn_mode, bool first);
+// Largest fixed-point exponent s <= 32 with in_degree x (max_w x 2^s + 1/2) < 2^32,
+// so no packed 32-bit field of DTB_SYN_PUSH_FIXED can carry; 0 (mode unavailable)
+// for negative weights or when s would fall below 12.
+uint32_t fixed_shift_for(uint64_t max_in_degree, double max_w, bool negative);
 
 class Engine {
 public:
@@ -90,6 +98,7 @@ public:
     LaunchBatch single_batch() const;
     int refresh_view();
     int ensure_dj();
+    int ensure_djf();
     int ensure_hist(uint32_t rows, bool record, bool samples = false);
     int begin_run_chunk(uint64_t run_base, uint32_t rows, bool stats);
     int finish_hist(uint32_t rows, uint32_t out_row0, const dtb_run_output& out, bool freq, bool vmean, bool record);
@@ -133,6 +142,8 @@ public:
     float* tlast = nullptr;
     float4* J = nullptr;
     long long* dJ = nullptr;
+    unsigned long long* dJf = nullptr;   // fixed-mode sums, allocated on first use
+    uint32_t fix_shift = 0;              // fixed_shift_for() of the network (0: mode unavailable)
     PopParams* pop_dev = nullptr;
     uint32_t* pop_off_dev = nullptr;
     float* np_dev = nullptr;
@@ -187,11 +198,19 @@ public:
     PushCfg push_cfg{PUSH_REG, 8, 32};
     uint32_t push_ctas = 0;
     bool autotune = true;
-    bool push_tuned[2] = {false, false};
-    TuneResult tune_acc[2];               // samples gathered so far (float push, exact push)
+    bool push_tuned[3] = {false, false, false};
+    TuneResult tune_acc[3];               // samples gathered so far (float, exact and fixed push)
     float tuned_ms = 0.0f;
     std::vector<TuneEntry> tune_report;
-    int tune_push(const LaunchBatch& b, int exact);
+    int tune_push(const LaunchBatch& b, int acc);
+    // Window graphs of the plain path: a chunk of push-mode steps is launched eagerly
+    // the first time its shape is seen, captured into a CUDA graph the second time
+    // and replayed from then on (one graph kept per engine).
+    bool use_graph = true;
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_key[10] = {};
+    uint64_t seen_key[10] = {};
+    uint32_t graph_launches = 0;
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     NetView view{};
 

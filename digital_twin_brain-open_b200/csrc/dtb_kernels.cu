@@ -430,6 +430,14 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
                 in.J[3] = decay_add(Jk.w, pp.decay[3], fix_to_float(d23.y));
                 dq[0] = make_longlong2(0, 0);
                 dq[1] = make_longlong2(0, 0);
+            } else if constexpr (JM == J_FIXF) {
+                ulonglong2* dq = reinterpret_cast<ulonglong2*>(nv.dJf) + i;
+                const ulonglong2 d = *dq;
+                in.J[0] = decay_add(Jk.x, pp.decay[0], fixed_field(d.x, 0, nv.fix_unscale));
+                in.J[1] = decay_add(Jk.y, pp.decay[1], fixed_field(d.x, 1, nv.fix_unscale));
+                in.J[2] = decay_add(Jk.z, pp.decay[2], fixed_field(d.y, 0, nv.fix_unscale));
+                in.J[3] = decay_add(Jk.w, pp.decay[3], fixed_field(d.y, 1, nv.fix_unscale));
+                *dq = make_ulonglong2(0ull, 0ull);
             } else {
                 in.J[0] = Jk.x; in.J[1] = Jk.y; in.J[2] = Jk.z; in.J[3] = Jk.w;
             }
@@ -440,7 +448,7 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
             if constexpr (JM == J_DIRECT) {
                 sJ[ks] = make_float4(__fmul_rn(in.J[0], pp.decay[0]), __fmul_rn(in.J[1], pp.decay[1]),
                                      __fmul_rn(in.J[2], pp.decay[2]), __fmul_rn(in.J[3], pp.decay[3]));
-            } else if constexpr (JM == J_FOLD) {
+            } else if constexpr (JM == J_FOLD || JM == J_FIXF) {
                 sJ[ks] = make_float4(in.J[0], in.J[1], in.J[2], in.J[3]);
             }
             const bool sp = propagated(prop_mode, o.active, u[k], pp.noise_rate);
@@ -593,6 +601,8 @@ __device__ __forceinline__ void push_rows(const NetView* __restrict__ nets, cons
     const void* wts = nets[0].out_w;
     float4* J = nets[0].J;
     long long* dJ = nets[0].dJ;
+    unsigned long long* dJf = nets[0].dJf;
+    float fscale = nets[0].fix_scale;
     const uint2* own = LOCAL ? nets[0].own_seg : nullptr;
     uint32_t vb = 0;
     for (uint32_t r = gw; r < count; r += nw) {
@@ -605,6 +615,8 @@ __device__ __forceinline__ void push_rows(const NetView* __restrict__ nets, cons
             wts = nets[k].out_w;
             J = nets[k].J;
             dJ = nets[k].dJ;
+            dJf = nets[k].dJf;
+            fscale = nets[k].fix_scale;
             if constexpr (LOCAL) own = nets[k].own_seg;
         }
         const uint32_t j = v - vb;
@@ -637,8 +649,10 @@ __device__ __forceinline__ void push_rows(const NetView* __restrict__ nets, cons
                 if (xq < len) {
                     const uint32_t target = c[q] & kIndexMask;
                     const uint32_t kind = c[q] >> 31;
-                    if constexpr (ACC == 0) {
+                    if constexpr (ACC == ACC_FLOAT) {
                         red_add_f32x2(reinterpret_cast<float2*>(J + target) + kind, w[q]);
+                    } else if constexpr (ACC == ACC_FIXED) {
+                        red_add_u64(dJf + 2ull * target + kind, pack_fixed(w[q], fscale));
                     } else {
                         unsigned long long* d = reinterpret_cast<unsigned long long*>(dJ) + static_cast<size_t>(target) * 4 + 2 * kind;
                         red_add_u64(d, static_cast<unsigned long long>(float_to_fix(w[q].x)));
@@ -819,16 +833,27 @@ local_scan_kernel(uint32_t* scratch, uint32_t windows) {
 }
 
 // Add the window's fixed-point sums to J (coalesced 16-byte reductions of the
-// touched neurons) and clear them.
+// touched neurons) and clear them.  FIX: the sums are already in the network's
+// fixed-mode units and go to dJf as two packed 64-bit integer reductions, so the
+// result does not depend on which CTA flushes first.
+template <bool FIX>
 __device__ __forceinline__ void local_flush(const LocalWindow& W, int* acc) {
     __syncthreads();
     float4* J = W.nv->J + W.lo;
+    unsigned long long* dJf = FIX ? W.nv->dJf + 2ull * W.lo : nullptr;
     const uint32_t width = W.hi - W.lo;
     for (uint32_t i = threadIdx.x; i < width; i += blockDim.x) {
         const int4 v = make_int4(acc[i], acc[kLocalWin + i], acc[2 * kLocalWin + i], acc[3 * kLocalWin + i]);
         if (v.x | v.y | v.z | v.w) {
-            red_add_f32x4(J + i, make_float4(__fmul_rn(__int2float_rn(v.x), W.unscale), __fmul_rn(__int2float_rn(v.y), W.unscale),
-                                             __fmul_rn(__int2float_rn(v.z), W.unscale), __fmul_rn(__int2float_rn(v.w), W.unscale)));
+            if constexpr (FIX) {
+                const unsigned long long u0 = static_cast<uint32_t>(v.x), u1 = static_cast<uint32_t>(v.y);
+                const unsigned long long u2 = static_cast<uint32_t>(v.z), u3 = static_cast<uint32_t>(v.w);
+                if (u0 | u1) red_add_u64(dJf + 2ull * i, (u1 << 32) | u0);
+                if (u2 | u3) red_add_u64(dJf + 2ull * i + 1, (u3 << 32) | u2);
+            } else {
+                red_add_f32x4(J + i, make_float4(__fmul_rn(__int2float_rn(v.x), W.unscale), __fmul_rn(__int2float_rn(v.y), W.unscale),
+                                                 __fmul_rn(__int2float_rn(v.z), W.unscale), __fmul_rn(__int2float_rn(v.w), W.unscale)));
+            }
             acc[i] = 0;
             acc[kLocalWin + i] = 0;
             acc[2 * kLocalWin + i] = 0;
@@ -840,7 +865,7 @@ __device__ __forceinline__ void local_flush(const LocalWindow& W, int* acc) {
 
 // launch bound of the full CTA for every NT: 64 registers, so the 768-thread form leaves a
 // 256-thread push CTA room on the SM
-template <int WT, int NT, int RL = 32>
+template <int WT, int NT, int RL = 32, bool FIX = false>
 __global__ void __launch_bounds__(kLocalThreads, 1)
 push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ win_prefix, uint32_t n_nets,
                   uint32_t windows, uint32_t* scratch) {
@@ -872,8 +897,9 @@ push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__
         }
         const uint32_t gw = lo_w;
         if (gw != cur) {
-            if (cur != 0xFFFFFFFFu) local_flush(W, acc);
+            if (cur != 0xFFFFFFFFu) local_flush<FIX>(W, acc);
             load_window(nets, win_prefix, n_nets, gw, W);
+            if constexpr (FIX) W.scale = W.nv->fix_scale;   // sums in the network's fixed-mode units
             cur = gw;
         }
         const uint32_t r_lo = (u - upre[gw]) * kLocalUnitRows;
@@ -936,15 +962,20 @@ push_local_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__
                 for (int q = 0; q < kLocalUnroll; ++q) {
                     if (e + static_cast<unsigned long long>(RL) * q < e1) {
                         const int* d = acc + (cc[q] >> 31) * (2u * kLocalWin) + ((cc[q] & kIndexMask) - W.lo);
-                        red_add_shared_u32(d, static_cast<uint32_t>(__float2int_rn(__fmul_rn(w[q].x, W.scale))));
-                        red_add_shared_u32(d + kLocalWin, static_cast<uint32_t>(__float2int_rn(__fmul_rn(w[q].y, W.scale))));
+                        if constexpr (FIX) {
+                            red_add_shared_u32(d, __float2uint_rn(__fmul_rn(w[q].x, W.scale)));
+                            red_add_shared_u32(d + kLocalWin, __float2uint_rn(__fmul_rn(w[q].y, W.scale)));
+                        } else {
+                            red_add_shared_u32(d, static_cast<uint32_t>(__float2int_rn(__fmul_rn(w[q].x, W.scale))));
+                            red_add_shared_u32(d + kLocalWin, static_cast<uint32_t>(__float2int_rn(__fmul_rn(w[q].y, W.scale))));
+                        }
                     }
                 }
             }
         }
         __syncthreads();
     }
-    if (cur != 0xFFFFFFFFu) local_flush(W, acc);
+    if (cur != 0xFFFFFFFFu) local_flush<FIX>(W, acc);
 }
 
 __device__ inline uint32_t row_lower_bound(const uint32_t* __restrict__ col, unsigned long long beg,
@@ -1119,13 +1150,17 @@ push_tma_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ v
         const uint32_t cnt = s_cnt[st], ow = s_ow[st];
         float4* J = nets[s_net[st]].J;
         long long* dJ = nets[s_net[st]].dJ;
+        unsigned long long* dJf = nets[s_net[st]].dJf;
+        const float fscale = nets[s_net[st]].fix_scale;
 #pragma unroll 4
         for (uint32_t e = lane; e < cnt; e += 32) {
             const uint32_t c = scol[e];
             const float2 w = smem_weight<WT>(sw, ow + e);
             const uint32_t target = c & kIndexMask, kind = c >> 31;
-            if constexpr (ACC == 0) {
+            if constexpr (ACC == ACC_FLOAT) {
                 red_add_f32x2(reinterpret_cast<float2*>(J + target) + kind, w);
+            } else if constexpr (ACC == ACC_FIXED) {
+                red_add_u64(dJf + 2ull * target + kind, pack_fixed(w, fscale));
             } else {
                 unsigned long long* d = reinterpret_cast<unsigned long long*>(dJ) + static_cast<size_t>(target) * 4 + 2 * kind;
                 red_add_u64(d, static_cast<unsigned long long>(float_to_fix(w.x)));
@@ -1323,7 +1358,9 @@ lif_pull_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ t
     advance_clock(nv, nv.n_pad / kPullTile, t, n, err);
 }
 
-// End of an exact-push run: J <- J*decay + dJ, dJ <- 0 (J becomes complete).
+// End of an exact- or fixed-push run: J <- J*decay + dJ (or dJf), the sums <- 0
+// (J becomes complete).
+template <int ACC>
 __global__ void __launch_bounds__(kLifThreads)
 fold_finish_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_prefix, uint32_t n_nets) {
     const uint32_t k = n_nets > 1 ? find_net(tile_prefix, n_nets, blockIdx.x) : 0u;
@@ -1340,9 +1377,17 @@ fold_finish_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict_
         load_pop_params(nv, p, i, pp);
         float4 Jv = nv.J[i];
         float* Jc = reinterpret_cast<float*>(&Jv);
-        long long* d = nv.dJ + static_cast<size_t>(i) * 4;
+        if constexpr (ACC == ACC_FIXED) {
+            unsigned long long* d = nv.dJf + 2ull * i;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) { Jc[c] = decay_add(Jc[c], pp.decay[c], fix_to_float(d[c])); d[c] = 0; }
+            for (int c = 0; c < 4; ++c) Jc[c] = decay_add(Jc[c], pp.decay[c], fixed_field(d[c >> 1], c & 1, nv.fix_unscale));
+            d[0] = 0ull;
+            d[1] = 0ull;
+        } else {
+            long long* d = nv.dJ + static_cast<size_t>(i) * 4;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) { Jc[c] = decay_add(Jc[c], pp.decay[c], fix_to_float(d[c])); d[c] = 0; }
+        }
         nv.J[i] = Jv;
     }
 }
@@ -1423,6 +1468,10 @@ stat_isyn_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ 
                 const long long* d = nv.dJ + static_cast<size_t>(i) * 4;
 #pragma unroll
                 for (int c = 0; c < 4; ++c) J[c] = decay_add(J[c], pp.decay[c], fix_to_float(d[c]));
+            } else if constexpr (JM == J_FIXF) {
+                const unsigned long long* d = nv.dJf + 2ull * i;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) J[c] = decay_add(J[c], pp.decay[c], fixed_field(d[c >> 1], c & 1, nv.fix_unscale));
             }
             float I[4];
 #pragma unroll
@@ -1488,7 +1537,7 @@ cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop
     if (e != cudaSuccess) return e;
     const uint32_t bit = 1u << (dev & 31);
     if (!(attr_set.load() & bit)) {
-        for (auto fn : {lif_kernel<J_DIRECT>, lif_kernel<J_FOLD>, lif_kernel<J_ASIS>}) {
+        for (auto fn : {lif_kernel<J_DIRECT>, lif_kernel<J_FOLD>, lif_kernel<J_ASIS>, lif_kernel<J_FIXF>}) {
             e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kLifSmem));
             if (e != cudaSuccess) return e;
         }
@@ -1499,6 +1548,7 @@ cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop
     switch (jmode) {
         case J_DIRECT: lif_kernel<J_DIRECT><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net); break;
         case J_FOLD: lif_kernel<J_FOLD><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net); break;
+        case J_FIXF: lif_kernel<J_FIXF><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net); break;
         default: lif_kernel<J_ASIS><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net); break;
     }
     return cudaGetLastError();
@@ -1506,7 +1556,8 @@ cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop
 
 template <int ACC, int WT>
 static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint32_t ctas, cudaStream_t s) {
-    if (cfg.kind == PUSH_LOCAL && ACC == 0 &&
+    constexpr bool FIX = ACC == ACC_FIXED;
+    if (cfg.kind == PUSH_LOCAL && ACC != ACC_EXACT &&
         (cfg.param == kLocalConcurrent || cfg.param == kLocalConcurrent2 || cfg.param == kLocalConcurrentHalf) &&
         b.aux && b.windows_total) {
         // cross-population spans on the auxiliary stream, one (two) 256-thread CTA(s) per SM, next
@@ -1524,19 +1575,19 @@ static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint
         local_count_kernel<<<b.windows_total, 256, 0, s>>>(b.nets, b.win_prefix, b.n_nets, b.local_scratch);
         local_scan_kernel<<<1, 1024, 0, s>>>(b.local_scratch, b.windows_total);
         if (two)
-            push_local_kernel<WT, kLocalThreadsShared2><<<b.sm_count, kLocalThreadsShared2, kLocalSmem, s>>>(
+            push_local_kernel<WT, kLocalThreadsShared2, 32, FIX><<<b.sm_count, kLocalThreadsShared2, kLocalSmem, s>>>(
                 b.nets, b.win_prefix, b.n_nets, b.windows_total, b.local_scratch);
         else if (cfg.param == kLocalConcurrentHalf)
-            push_local_kernel<WT, kLocalThreadsShared, 16><<<b.sm_count, kLocalThreadsShared, kLocalSmem, s>>>(
+            push_local_kernel<WT, kLocalThreadsShared, 16, FIX><<<b.sm_count, kLocalThreadsShared, kLocalSmem, s>>>(
                 b.nets, b.win_prefix, b.n_nets, b.windows_total, b.local_scratch);
         else
-            push_local_kernel<WT, kLocalThreadsShared><<<b.sm_count, kLocalThreadsShared, kLocalSmem, s>>>(
+            push_local_kernel<WT, kLocalThreadsShared, 32, FIX><<<b.sm_count, kLocalThreadsShared, kLocalSmem, s>>>(
                 b.nets, b.win_prefix, b.n_nets, b.windows_total, b.local_scratch);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b.ev_join, 0);
         return e;
     }
-    if (cfg.kind == PUSH_LOCAL && ACC == 0) {
+    if (cfg.kind == PUSH_LOCAL && ACC != ACC_EXACT) {
         const dim3 grid(ctas), block(kPushThreads);
         if (cfg.lpr == 16)
             push_kernel<ACC, WT, 8, 16, 1><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes);
@@ -1545,7 +1596,7 @@ static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint
         if (b.windows_total) {
             local_count_kernel<<<b.windows_total, 256, 0, s>>>(b.nets, b.win_prefix, b.n_nets, b.local_scratch);
             local_scan_kernel<<<1, 1024, 0, s>>>(b.local_scratch, b.windows_total);
-            push_local_kernel<WT, kLocalThreads><<<b.sm_count, kLocalThreads, kLocalSmem, s>>>(
+            push_local_kernel<WT, kLocalThreads, 32, FIX><<<b.sm_count, kLocalThreads, kLocalSmem, s>>>(
                 b.nets, b.win_prefix, b.n_nets, b.windows_total, b.local_scratch);
         }
     } else if (cfg.kind == PUSH_REG || cfg.kind == PUSH_LOCAL) {
@@ -1578,18 +1629,12 @@ template <int ACC, int WT>
 static cudaError_t push_prepare_wt(const PushCfg& cfg, int sm_count, uint32_t* ctas) {
     int per_sm = 0;
     cudaError_t e = cudaSuccess;
-    if (cfg.kind == PUSH_LOCAL && ACC == 0) {
-        e = cudaFuncSetAttribute(push_local_kernel<WT, kLocalThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(kLocalSmem));
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(push_local_kernel<WT, kLocalThreadsShared>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(kLocalSmem));
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(push_local_kernel<WT, kLocalThreadsShared2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(kLocalSmem));
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(push_local_kernel<WT, kLocalThreadsShared, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(kLocalSmem));
+    if (cfg.kind == PUSH_LOCAL && ACC != ACC_EXACT) {
+        constexpr bool FIX = ACC == ACC_FIXED;
+        for (auto fn : {push_local_kernel<WT, kLocalThreads, 32, FIX>, push_local_kernel<WT, kLocalThreadsShared, 32, FIX>,
+                        push_local_kernel<WT, kLocalThreadsShared2, 32, FIX>, push_local_kernel<WT, kLocalThreadsShared, 16, FIX>})
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kLocalSmem));
         // the cross-population CTAs land on an SM first: ask for the largest shared-memory
         // carve-out so a window CTA (229 KB) can join them there
         for (auto fn : {push_kernel<ACC, WT, 8, 32, 1>, push_kernel<ACC, WT, 8, 16, 1>, push_kernel_cross64<ACC, WT>})
@@ -1644,25 +1689,30 @@ const PushCfg kPushCands[kPushCandidates] = {{PUSH_REG, 4, 32}, {PUSH_REG, 8, 32
                                              {PUSH_LOCAL, kLocalConcurrent, 32}, {PUSH_LOCAL, kLocalConcurrent2, 32},
                                              {PUSH_LOCAL, kLocalConcurrentHalf, 32}};
 
-cudaError_t push_prepare(int exact, int wt, const PushCfg& cfg, int sm_count, uint32_t* ctas) {
-    if (exact) {
-        switch (wt) {
-            case W_F32: return push_prepare_wt<1, W_F32>(cfg, sm_count, ctas);
-            case W_BF16: return push_prepare_wt<1, W_BF16>(cfg, sm_count, ctas);
-            case W_F16: return push_prepare_wt<1, W_F16>(cfg, sm_count, ctas);
-            default: return push_prepare_wt<1, W_U8>(cfg, sm_count, ctas);
-        }
-    }
+template <int ACC>
+static cudaError_t push_prepare_acc(int wt, const PushCfg& cfg, int sm_count, uint32_t* ctas) {
     switch (wt) {
-        case W_F32: return push_prepare_wt<0, W_F32>(cfg, sm_count, ctas);
-        case W_BF16: return push_prepare_wt<0, W_BF16>(cfg, sm_count, ctas);
-        case W_F16: return push_prepare_wt<0, W_F16>(cfg, sm_count, ctas);
-        default: return push_prepare_wt<0, W_U8>(cfg, sm_count, ctas);
+        case W_F32: return push_prepare_wt<ACC, W_F32>(cfg, sm_count, ctas);
+        case W_BF16: return push_prepare_wt<ACC, W_BF16>(cfg, sm_count, ctas);
+        case W_F16: return push_prepare_wt<ACC, W_F16>(cfg, sm_count, ctas);
+        default: return push_prepare_wt<ACC, W_U8>(cfg, sm_count, ctas);
     }
 }
 
-cudaError_t launch_push(const LaunchBatch& b, int exact, int wt, const PushCfg& cfg, uint32_t ctas, cudaStream_t s) {
-    return exact ? push_launch_acc<1>(b, wt, cfg, ctas, s) : push_launch_acc<0>(b, wt, cfg, ctas, s);
+cudaError_t push_prepare(int acc, int wt, const PushCfg& cfg, int sm_count, uint32_t* ctas) {
+    switch (acc) {
+        case ACC_EXACT: return push_prepare_acc<ACC_EXACT>(wt, cfg, sm_count, ctas);
+        case ACC_FIXED: return push_prepare_acc<ACC_FIXED>(wt, cfg, sm_count, ctas);
+        default: return push_prepare_acc<ACC_FLOAT>(wt, cfg, sm_count, ctas);
+    }
+}
+
+cudaError_t launch_push(const LaunchBatch& b, int acc, int wt, const PushCfg& cfg, uint32_t ctas, cudaStream_t s) {
+    switch (acc) {
+        case ACC_EXACT: return push_launch_acc<ACC_EXACT>(b, wt, cfg, ctas, s);
+        case ACC_FIXED: return push_launch_acc<ACC_FIXED>(b, wt, cfg, ctas, s);
+        default: return push_launch_acc<ACC_FLOAT>(b, wt, cfg, ctas, s);
+    }
 }
 
 cudaError_t build_local_offsets(const unsigned long long* out_ptr, const uint32_t* out_col, const void* out_w, int wt,
@@ -1697,17 +1747,21 @@ cudaError_t launch_pull(const LaunchBatch& b, int gather, int wt, uint32_t flags
     return cudaGetLastError();
 }
 
-cudaError_t launch_stat_isyn(const LaunchBatch& b, int exact, int sm_count, cudaStream_t s) {
+cudaError_t launch_stat_isyn(const LaunchBatch& b, int acc, int sm_count, cudaStream_t s) {
     if (b.lif_tiles_total == 0) return cudaSuccess;
     const dim3 grid(std::min<uint32_t>(b.lif_tiles_total, static_cast<uint32_t>(sm_count) * 8u)), block(256);
-    if (exact) stat_isyn_kernel<J_FOLD><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.n_nets, b.lif_tiles_total);
+    if (acc == ACC_EXACT) stat_isyn_kernel<J_FOLD><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.n_nets, b.lif_tiles_total);
+    else if (acc == ACC_FIXED) stat_isyn_kernel<J_FIXF><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.n_nets, b.lif_tiles_total);
     else stat_isyn_kernel<J_DIRECT><<<grid, block, 0, s>>>(b.nets, b.lif_prefix, b.n_nets, b.lif_tiles_total);
     return cudaGetLastError();
 }
 
-cudaError_t launch_fold_finish(const LaunchBatch& b, cudaStream_t s) {
+cudaError_t launch_fold_finish(const LaunchBatch& b, int acc, cudaStream_t s) {
     if (b.lif_tiles_total == 0) return cudaSuccess;
-    fold_finish_kernel<<<b.lif_tiles_total, kLifThreads, 0, s>>>(b.nets, b.lif_prefix, b.n_nets);
+    if (acc == ACC_FIXED)
+        fold_finish_kernel<ACC_FIXED><<<b.lif_tiles_total, kLifThreads, 0, s>>>(b.nets, b.lif_prefix, b.n_nets);
+    else
+        fold_finish_kernel<ACC_EXACT><<<b.lif_tiles_total, kLifThreads, 0, s>>>(b.nets, b.lif_prefix, b.n_nets);
     return cudaGetLastError();
 }
 

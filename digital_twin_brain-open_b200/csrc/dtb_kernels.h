@@ -48,18 +48,19 @@ constexpr int kLocalConcurrent2 = 2016;  // ... with two push CTAs per SM beside
 constexpr int kLocalConcurrentHalf = 3008;  // ... as 2008 with half-warp rows in the window kernel (short spans)
 extern const PushCfg kPushCands[kPushCandidates];
 // Sets kernel attributes and returns the persistent grid (max resident CTAs).
-cudaError_t push_prepare(int exact, int weight_type, const PushCfg& cfg, int sm_count, uint32_t* ctas);
-cudaError_t launch_push(const LaunchBatch& b, int exact, int weight_type, const PushCfg& cfg, uint32_t ctas,
+// `acc` is the AccMode of the launch (float, exact or fixed-point accumulators).
+cudaError_t push_prepare(int acc, int weight_type, const PushCfg& cfg, int sm_count, uint32_t* ctas);
+cudaError_t launch_push(const LaunchBatch& b, int acc, int weight_type, const PushCfg& cfg, uint32_t ctas,
                         cudaStream_t s);
 // Kernels launch_push issues beyond the first (the local variant's count, scan and window passes).
-inline uint32_t push_extra_launches(const LaunchBatch& b, int exact, const PushCfg& cfg) {
-    return (cfg.kind == PUSH_LOCAL && !exact && b.windows_total) ? 3u : 0u;   // concurrent form: same count
+inline uint32_t push_extra_launches(const LaunchBatch& b, int acc, const PushCfg& cfg) {
+    return (cfg.kind == PUSH_LOCAL && acc != ACC_EXACT && b.windows_total) ? 3u : 0u;   // concurrent form: same count
 }
 cudaError_t launch_pull(const LaunchBatch& b, int gather, int weight_type, uint32_t flags, int prop_mode, cudaStream_t s);
-cudaError_t launch_fold_finish(const LaunchBatch& b, cudaStream_t s);
+cudaError_t launch_fold_finish(const LaunchBatch& b, int acc, cudaStream_t s);
 // Per-population sums of the end-of-step synaptic currents (after the push of
-// the step; exact = J still holds its folded form plus dJ).
-cudaError_t launch_stat_isyn(const LaunchBatch& b, int exact, int sm_count, cudaStream_t s);
+// the step; with exact or fixed accumulators J still lacks the step's sums).
+cudaError_t launch_stat_isyn(const LaunchBatch& b, int acc, int sm_count, cudaStream_t s);
 cudaError_t launch_gather_finish(const LaunchBatch& b, int weight_type, cudaStream_t s);
 
 // Population-local push tables (rows must be sorted by postsynaptic neuron;

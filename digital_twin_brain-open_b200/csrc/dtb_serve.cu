@@ -359,7 +359,7 @@ void dtb_server_default_options(dtb_server_options* o) {
 int32_t dtb_server_create(const dtb_server_options* opt, void** server) {
     if (!opt || !server) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
     if (opt->slice_steps == 0 || opt->max_batch == 0) return dtb::fail(DTB_INVALID_PARAMETER, "slice_steps and max_batch must be positive");
-    if (opt->syn_mode > DTB_SYN_PULL) return dtb::fail(DTB_INVALID_PARAMETER, "unknown syn_mode");
+    if (opt->syn_mode > DTB_SYN_PUSH_FIXED) return dtb::fail(DTB_INVALID_PARAMETER, "unknown syn_mode");
     return server_guarded([&] {
         auto* s = new Server();
         s->o = *opt;

@@ -22,7 +22,7 @@ OUT_OF_MEMORY, CUDA_ERROR, DEVICE_FAULT, IO_ERROR, NO_DEVICE = 16, 17, 18, 19, 2
 
 W_F32, W_BF16, W_F16, W_U8, W_F64 = 0, 1, 2, 3, 4
 PROP_THRESHOLD, PROP_NOISE, PROP_OR = 0, 1, 2
-SYN_PUSH, SYN_PUSH_EXACT, SYN_PULL = 0, 1, 2
+SYN_PUSH, SYN_PUSH_EXACT, SYN_PULL, SYN_PUSH_FIXED = 0, 1, 2, 3
 PUSH_REG, PUSH_TMA, PUSH_LOCAL = 0, 1, 2
 NOISE_PHILOX, NOISE_INJECTED = 0, 1
 RUN_USE_OU, RUN_FREQ, RUN_VMEAN, RUN_RECORD_SPIKES, RUN_TIME_KERNELS = 1, 2, 4, 8, 16
@@ -68,7 +68,8 @@ class EngineInfo(C.Structure):
                 ("device_bytes", C.c_uint64), ("step", C.c_uint64), ("t", C.c_float),
                 ("weight_type", C.c_uint32), ("has_push", C.c_uint32), ("has_pull", C.c_uint32),
                 ("per_neuron_params", C.c_uint32), ("push_kind", C.c_uint32), ("push_param", C.c_uint32),
-                ("push_tuned_ms", C.c_float), ("local_windows", C.c_uint32)]
+                ("push_tuned_ms", C.c_float), ("local_windows", C.c_uint32), ("fixed_shift", C.c_uint32),
+                ("graph_launches", C.c_uint32)]
 
 
 class RunRequest(C.Structure):
@@ -100,6 +101,7 @@ SIGNATURES = {
     "dtb_info": (_I32, [_P, _P]),
     "dtb_get_stream": (_I32, [_P, C.POINTER(C.c_void_p)]),
     "dtb_set_push_variant": (_I32, [_P, _I32, _I32]),
+    "dtb_set_graph": (_I32, [_P, _I32]),
     "dtb_tuning_report": (_I32, [_P, _P, _P, _P, _P]),
     "dtb_populations": (_I32, [_P, _P, _P]),
     "dtb_update_props": (_I32, [_P, _U32, _P, _P, _P]),
@@ -363,6 +365,10 @@ class Engine:
         """kind 0: register-staged (param 4/8/16, 1016/1008 sub-warp rows), 1: TMA-staged
         (param 256/512), 2: population-local windows (param 8/1016), -1: autotune."""
         _check(LIB.dtb_set_push_variant(self._h, kind, param))
+
+    def set_graph(self, enable):
+        """Replay repeated run chunks from captured CUDA graphs (default on)."""
+        _check(LIB.dtb_set_graph(self._h, int(enable)))
 
     def tuning_report(self):
         """[(kind, param, ms)] of the push variants timed by the autotuner."""

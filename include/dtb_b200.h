@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define DTB_ABI_VERSION 1
+#define DTB_ABI_VERSION 2
 
 /* Status codes.  0-5 are snn.proto's SnnStatus (protos/snn.proto:44-51). */
 typedef enum dtb_status {
@@ -67,7 +67,16 @@ typedef enum dtb_prop_mode {
 typedef enum dtb_syn_mode {
     DTB_SYN_PUSH = 0,        /* out-degree CSR, fp32 vector reductions into J (fastest)       */
     DTB_SYN_PUSH_EXACT = 1,  /* out-degree CSR, 64-bit fixed-point atomics: deterministic     */
-    DTB_SYN_PULL = 2         /* in-degree CSR gather fused into the LIF step: deterministic   */
+    DTB_SYN_PULL = 2,        /* in-degree CSR gather fused into the LIF step: deterministic   */
+    DTB_SYN_PUSH_FIXED = 3   /* out-degree CSR, each step's input summed as two unsigned      */
+                             /* 32-bit fixed-point fields packed in one 64-bit reduction per  */
+                             /* synapse (units of 2^-fixed_shift, chosen at creation from the */
+                             /* largest in-degree and weight so no field can carry): the float*/
+                             /* push's kernels with integer reductions, deterministic (a run  */
+                             /* gives the same bits alone, batched or served), bit-exact      */
+                             /* against the oracle whenever every weight is a multiple of     */
+                             /* 2^-fixed_shift.  Needs                                        */
+                             /* non-negative weights (dtb_engine_info.fixed_shift != 0)       */
 } dtb_syn_mode;
 
 /* Source of the OU normal draws and the noise-train uniforms. */
@@ -143,6 +152,8 @@ typedef struct dtb_engine_info {
     uint32_t push_param;         /* synapses in flight per lane (0, 2) or per stage (1)       */
     float push_tuned_ms;         /* push time of the chosen variant when it was tuned, ms     */
     uint32_t local_windows;      /* population-local push windows (0: variant 2 = variant 0)  */
+    uint32_t fixed_shift;        /* DTB_SYN_PUSH_FIXED units 2^-fixed_shift (0: unavailable)   */
+    uint32_t graph_launches;     /* window graphs replayed by dtb_run so far                   */
 } dtb_engine_info;
 
 /* RunRequest (snn.proto:63-77) flags. */
@@ -219,6 +230,12 @@ int32_t dtb_info(void* engine, dtb_engine_info* info);
  * 47 or more steps apart, and keeps the variant with the smallest mean; it gives
  * up (keeping the best so far, or kind 0 param 8) after 400 reads of quiet steps. */
 int32_t dtb_set_push_variant(void* engine, int32_t kind, int32_t param);
+/* Window graphs of dtb_run (no reference counterpart): with enable != 0 (the
+ * default) a chunk of push-mode steps is launched kernel by kernel the first time
+ * its shape (steps, flags, modes, push variant) is seen, captured into a CUDA
+ * graph the second time and replayed from then on; results are the same bits
+ * either way.  enable = 0 launches every chunk kernel by kernel. */
+int32_t dtb_set_graph(void* engine, int32_t enable);
 /* The autotuner's last measurement: on entry *n is the capacity of the arrays,
  * on return the number of variants timed (kind, param, push time in ms). */
 int32_t dtb_tuning_report(void* engine, uint32_t* n, int32_t* kinds, int32_t* params, float* ms);

@@ -32,7 +32,7 @@ def test_binding_covers_the_header():
 
 
 def test_versions_and_status_strings():
-    assert E.LIB.dtb_abi_version() == 1
+    assert E.LIB.dtb_abi_version() == 2
     v = E.LIB.dtb_engine_version()
     assert (v // 1000, (v % 1000) // 100, v % 100) == (1, 0, 0)
     assert E.status_string(0) == "SNN_OK"

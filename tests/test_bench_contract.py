@@ -16,3 +16,7 @@ def test_reference_arm_prints_its_line():
     assert line["e2e"]["value"] == line["value"] and line["e2e"]["h2d_bytes_per_step"] == 0
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["higher_is_better"] is True
+    # the line names the sample it times and counts the bench steps it timed
+    assert line["steps"] == 1 and line["warmup"] == 3
+    assert "50,000-neuron" in line["config"]["workload"] and line["config"]["timed_sim_steps"] == 75
+    assert line["cpu_baseline"]["value"] == line["value"]
