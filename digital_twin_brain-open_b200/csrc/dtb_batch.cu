@@ -134,6 +134,8 @@ int Batch::set_members(Engine* const* engines, uint32_t n) {
         graph = nullptr;
     }
     std::memset(graph_key, 0, sizeof(graph_key));
+    std::memset(seen_key, 0, sizeof(seen_key));
+    seen_count = 0;
     DTB_CU(cudaStreamSynchronize(stream));
     return DTB_OK;
 }
@@ -149,6 +151,7 @@ int Batch::refresh_views() {
 int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
     if (rq.iters == 0) return fail(DTB_INVALID_PARAMETER, "iter must be positive");
     if (rq.prop_mode > DTB_PROP_OR || rq.syn_mode > DTB_SYN_PUSH_FIXED) return fail(DTB_INVALID_PARAMETER, "unknown mode");
+    if (rq.t_steps > 1) return fail(DTB_UNSUPPORTED, "substeps (t_steps > 1) run through dtb_run, one engine at a time");
     const bool freq = (rq.flags & DTB_RUN_FREQ) != 0;
     const bool vmean = (rq.flags & DTB_RUN_VMEAN) != 0;
     const bool record = (rq.flags & DTB_RUN_RECORD_SPIKES) != 0;
@@ -240,29 +243,43 @@ int Batch::run(const dtb_run_request& rq, dtb_run_output* outs) {
         // exact or fixed run ends by folding the sums into J, so both are in the key.
         const bool last_chunk = done + rows == rq.iters;
         const bool graphable = use_graph && !pull && !(tune_at >= done && tune_at < done + rows);
+        bool replay = false;
         if (graphable) {
             const uint64_t key[9] = {rows, kflags, static_cast<uint64_t>(pm),
                                      static_cast<uint64_t>(push_cfg.kind) * 100000 + push_cfg.param * 100 + push_cfg.lpr,
                                      push_ctas, rq.syn_mode, done == 0, last_chunk, 1};
-            if (!graph || std::memcmp(key, graph_key, sizeof(key)) != 0) {
-                if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
-                cudaGraph_t g = nullptr;
-                DTB_CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-                cudaError_t ce = cudaSuccess;
-                for (uint32_t s = 0; s < rows && ce == cudaSuccess; ++s) {
-                    ce = launch_lif(lb, jmode_of(rq.syn_mode, done + s == 0), kflags, pm, stream);
-                    if (ce == cudaSuccess) ce = launch_push(lb, acc, wt, push_cfg, push_ctas, stream);
-                    if (ce == cudaSuccess && isyn_any) ce = launch_stat_isyn(lb, acc, sm_count, stream);
+            if (graph && std::memcmp(key, graph_key, sizeof(key)) == 0) {
+                replay = true;
+            } else {
+                // the same shape twice in a row under this membership before it is captured:
+                // a serving batch whose membership changes every slice keeps launching eagerly
+                if (std::memcmp(key, seen_key, sizeof(key)) != 0) {
+                    std::memcpy(seen_key, key, sizeof(key));
+                    seen_count = 0;
                 }
-                if (ce == cudaSuccess && last_chunk && acc != ACC_FLOAT) ce = launch_fold_finish(lb, acc, stream);
-                const cudaError_t ee = cudaStreamEndCapture(stream, &g);
-                if (ce != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(ce, "graph capture"); }
-                if (ee != cudaSuccess) return cuda_fail(ee, "cudaStreamEndCapture");
-                const cudaError_t ie = cudaGraphInstantiate(&graph, g, 0);
-                cudaGraphDestroy(g);
-                if (ie != cudaSuccess) { graph = nullptr; return cuda_fail(ie, "cudaGraphInstantiate"); }
-                std::memcpy(graph_key, key, sizeof(key));
+                if (++seen_count >= 3) {
+                    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+                    cudaGraph_t g = nullptr;
+                    DTB_CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+                    cudaError_t ce = cudaSuccess;
+                    for (uint32_t s = 0; s < rows && ce == cudaSuccess; ++s) {
+                        ce = launch_lif(lb, jmode_of(rq.syn_mode, done + s == 0), kflags, pm, stream);
+                        if (ce == cudaSuccess) ce = launch_push(lb, acc, wt, push_cfg, push_ctas, stream);
+                        if (ce == cudaSuccess && isyn_any) ce = launch_stat_isyn(lb, acc, sm_count, stream);
+                    }
+                    if (ce == cudaSuccess && last_chunk && acc != ACC_FLOAT) ce = launch_fold_finish(lb, acc, stream);
+                    const cudaError_t ee = cudaStreamEndCapture(stream, &g);
+                    if (ce != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(ce, "graph capture"); }
+                    if (ee != cudaSuccess) return cuda_fail(ee, "cudaStreamEndCapture");
+                    const cudaError_t ie = cudaGraphInstantiate(&graph, g, 0);
+                    cudaGraphDestroy(g);
+                    if (ie != cudaSuccess) { graph = nullptr; return cuda_fail(ie, "cudaGraphInstantiate"); }
+                    std::memcpy(graph_key, key, sizeof(key));
+                    replay = true;
+                }
             }
+        }
+        if (replay) {
             DTB_CU(cudaGraphLaunch(graph, stream));
             ++graph_launches;
             launches += (2 + push_extra_launches(lb, acc, push_cfg) + (isyn_any ? 1u : 0u)) * rows +

@@ -48,6 +48,8 @@ public:
     bool use_graph = true;
     cudaGraphExec_t graph = nullptr;
     uint64_t graph_key[9] = {};
+    uint64_t seen_key[9] = {};        // shape of the last chunks launched eagerly, and how often in a row
+    uint32_t seen_count = 0;
     uint32_t graph_launches = 0;
 };
 

@@ -64,6 +64,12 @@ constexpr uint32_t kFlagList = 8u;       // write the spike list for the push ke
 constexpr uint32_t kFlagInjected = 16u;
 constexpr uint32_t kFlagSample = 32u;     // record the sampled neurons
 constexpr uint32_t kFlagIsyn = 64u;       // synaptic-current statistics after the push (host-side marker)
+// Substeps (RunRequest.t_steps > 1, tools/dist_simulator.cpp:2085-2112): a LIF launch
+// may be substep `k` of `ts` of one step; both ride in the flags word.  The device
+// clock's step count advances after the last substep only, its time after every one.
+constexpr uint32_t kSubShift = 16u;       // bits 16-23: substep index k
+constexpr uint32_t kTsShift = 24u;        // bits 24-31: substeps per step (0 = 1)
+__host__ __device__ inline uint32_t substep_flags(uint32_t k, uint32_t ts) { return (k << kSubShift) | (ts << kTsShift); }
 
 // Derived per-population constants (host computes them once per property change).
 struct __align__(16) PopParams {

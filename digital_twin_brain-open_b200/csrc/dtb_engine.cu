@@ -122,6 +122,7 @@ int Engine::setup_populations_from_property(const float* prop) {
 }
 
 int Engine::upload_params() {
+    ++params_version;
     std::vector<PopParams> pp(P);
     for (uint32_t p = 0; p < P; ++p) pp[p] = derive(pop_raw[p], dt);
     DTB_CU(cudaMemcpyAsync(pop_dev, pp.data(), sizeof(PopParams) * P, cudaMemcpyHostToDevice, stream));
@@ -175,6 +176,11 @@ int Engine::refresh_view() {
     v.n_pops = P;
     v.dt = dt;
     v.per_neuron = per_neuron ? 1u : 0u;
+    if (view_ts > 1) {
+        // a t_steps run: every kernel steps by dt / t_steps with constants derived for it
+        volatile float dts = dt / static_cast<float>(view_ts);
+        v.dt = dts;
+    }
     v.weight_type = wtype;
     v.hist_cap = hist_cap;
     v.V = V;
@@ -182,9 +188,9 @@ int Engine::refresh_view() {
     v.tlast = tlast;
     v.J = J;
     v.dJ = dJ;
-    v.pop = pop_dev;
+    v.pop = view_ts > 1 ? pop_sub_dev : pop_dev;
     v.pop_off = pop_off_dev;
-    v.np_params = np_dev;
+    v.np_params = view_ts > 1 ? np_sub_dev : np_dev;
     v.out_ptr = out_ptr;
     v.out_col = out_col;
     v.out_w = out_w;
@@ -678,6 +684,37 @@ int Engine::ensure_dj() {
     return refresh_view();
 }
 
+// Constants for substeps of dt / ts (the reference derives OU, decay and membrane factors
+// from delta_t / t_steps: src/block.cpp:304, 317, 668, 1275), derived again whenever the
+// properties changed since; ts = 1 returns the view to the plain constants.
+int Engine::use_substep_params(uint32_t ts) {
+    const uint32_t want = ts > 1 ? ts : 1u;
+    if (want > 1 && (sub_ts != want || sub_version != params_version)) {
+        volatile float dts = dt / static_cast<float>(want);
+        const float d = dts;
+        if (!pop_sub_dev) DTB_TRY(dalloc(pop_sub_dev, P));
+        std::vector<PopParams> pp(P);
+        for (uint32_t p = 0; p < P; ++p) pp[p] = derive(pop_raw[p], d);
+        DTB_CU(cudaMemcpyAsync(pop_sub_dev, pp.data(), sizeof(PopParams) * P, cudaMemcpyHostToDevice, stream));
+        if (per_neuron) {
+            if (!np_sub_dev) DTB_TRY(dalloc(np_sub_dev, static_cast<size_t>(kParamFloats) * n_pad));
+            std::vector<float> soa(static_cast<size_t>(kParamFloats) * n_pad, 0.0f);
+            for (uint32_t i = 0; i < n; ++i) {
+                const PopParams q = derive(neuron_raw[i], d);
+                const float* f = reinterpret_cast<const float*>(&q);
+                for (int k = 0; k < kParamFloats; ++k) soa[static_cast<size_t>(k) * n_pad + i] = f[k];
+            }
+            DTB_CU(cudaMemcpyAsync(np_sub_dev, soa.data(), soa.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
+        }
+        DTB_CU(cudaStreamSynchronize(stream));
+        sub_ts = want;
+        sub_version = params_version;
+    }
+    if (view_ts == want) return DTB_OK;
+    view_ts = want;
+    return refresh_view();
+}
+
 int Engine::ensure_djf() {
     if (dJf) return DTB_OK;
     DTB_TRY(dalloc(dJf, static_cast<size_t>(n_pad) * 2));
@@ -870,12 +907,28 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     if ((imean || rimean || sisyn) && pull)
         return fail(DTB_UNSUPPORTED, "synaptic-current outputs need a push mode (the pull kernel completes J one step later)");
     const bool isyn_any = imean || rimean || sisyn;
+    const uint32_t ts = std::max(1u, rq.t_steps);
+    if (ts > 1) {
+        // the reference's Run validation (dist_simulator.cpp:3225-3234) and this engine's limits
+        if (ts > 255) return fail(DTB_INVALID_PARAMETER, "t_steps must be at most 255");
+        if (!(rq.flags & DTB_RUN_USE_OU)) return fail(DTB_INVALID_PARAMETER, "t_steps > 1 needs use_ou_background");
+        if (pull) return fail(DTB_UNSUPPORTED, "substeps need a push mode");
+        if (rq.prop_mode != DTB_PROP_THRESHOLD) return fail(DTB_UNSUPPORTED, "substeps propagate threshold spikes only");
+    }
     const bool injected = noise_src == DTB_NOISE_INJECTED;
     if (injected) {
-        const uint64_t used = steps - inj_first;
-        if (used + rq.iters > inj_rows) return fail(DTB_INVALID_PARAMETER, "not enough injected noise rows for this run");
+        // rows are consumed t_steps per step (every step since dtb_set_noise at this t_steps)
+        const uint64_t used = (steps - inj_first) * ts;
+        if (used + static_cast<uint64_t>(rq.iters) * ts > inj_rows)
+            return fail(DTB_INVALID_PARAMETER, "not enough injected noise rows for this run");
         if (rq.prop_mode != DTB_PROP_THRESHOLD && !inj_u) return fail(DTB_INVALID_PARAMETER, "noise train needs injected uniforms");
     }
+    DTB_TRY(use_substep_params(ts));
+    struct PlainView {
+        Engine* e;
+        bool on;
+        ~PlainView() { if (on) e->use_substep_params(1); }
+    } restore{this, ts > 1};
     const int acc = acc_of(rq.syn_mode);
     if (acc == ACC_EXACT) DTB_TRY(ensure_dj());
     if (acc == ACC_FIXED) DTB_TRY(ensure_djf());
@@ -897,7 +950,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
     uint64_t tune_at = ~0ull;   // run-relative step at which the push variants are timed
     if (!pull) {
         DTB_CU(push_prepare(acc, wt, push_cfg, sm_count, &push_ctas));
-        if (autotune && !push_tuned[acc]) {
+        if (autotune && !push_tuned[acc] && ts == 1) {
             // time the variants on a live spike list, once the network has left its quiet start
             const uint64_t settle = 300;
             tune_at = steps >= settle ? 1 : (settle - steps < rq.iters ? settle - steps : ~0ull);
@@ -936,7 +989,13 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
                     DTB_TRY(timed_launch(2, [&] { return launch_pull(b, first ? 0 : 1, wt, kflags, pm, stream); }));
                     continue;
                 }
-                DTB_TRY(timed_launch(0, [&] { return launch_lif(b, jmode_of(rq.syn_mode, first), kflags, pm, stream); }));
+                for (uint32_t k = 0; k < ts; ++k) {
+                    // substeps after the first fold nothing new: J decays with no input
+                    const int jm = jmode_of(rq.syn_mode, first && k == 0);
+                    const int jmk = k == 0 ? jm : (jm == J_ASIS ? jmode_of(rq.syn_mode, false) : jm);
+                    const uint32_t f = ts > 1 ? (kflags | substep_flags(k, ts)) : kflags;
+                    DTB_TRY(timed_launch(0, [&] { return launch_lif(b, jmk, f, pm, stream); }));
+                }
                 if (tuning && tune_at == done + s) {
                     DTB_TRY(tune_push(b, acc));
                     if (!push_tuned[acc]) tune_at = tune_acc[acc].next_step(tune_at);
@@ -956,14 +1015,14 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
         const bool graphable = use_graph && !pull && !time_k && !(tune_at >= done && tune_at < done + rows);
         const uint64_t key[10] = {rows, kflags, static_cast<uint64_t>(pm), rq.syn_mode,
                                   static_cast<uint64_t>(push_cfg.kind) * 100000 + push_cfg.param * 100 + push_cfg.lpr,
-                                  push_ctas, done == 0, last_chunk, isyn_any, 1};
+                                  push_ctas, done == 0, last_chunk, isyn_any, ts};
         if (graphable && graph && std::memcmp(key, graph_key, sizeof(key)) == 0) {
             DTB_CU(cudaGraphLaunch(graph, stream));
             ++graph_launches;
             // launches of the replayed chunk, counted as the eager path does
-            chunk_launches = rows * (2u + push_extra_launches(b, acc, push_cfg) + (isyn_any ? 1u : 0u)) +
+            chunk_launches = rows * (ts + 1u + push_extra_launches(b, acc, push_cfg) + (isyn_any ? 1u : 0u)) +
                              (last_chunk && acc != ACC_FLOAT ? 1u : 0u);
-        } else if (graphable && std::memcmp(key, seen_key, sizeof(key)) == 0) {
+        } else if (graphable && std::memcmp(key, seen_key, sizeof(key)) == 0 && ++seen_count >= 2) {
             if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
             cudaGraph_t g = nullptr;
             DTB_CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
@@ -978,7 +1037,10 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
             DTB_CU(cudaGraphLaunch(graph, stream));
             ++graph_launches;
         } else {
-            if (graphable) std::memcpy(seen_key, key, sizeof(key));
+            if (graphable && std::memcmp(key, seen_key, sizeof(key)) != 0) {
+                std::memcpy(seen_key, key, sizeof(key));
+                seen_count = 0;
+            }
             DTB_TRY(issue(true));
         }
         launches += chunk_launches;
@@ -992,8 +1054,8 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
             DTB_CU(cudaEventElapsedTime(&km, tev[2 * tp.second], tev[2 * tp.second + 1]));
             kms[tp.first] += km;
         }
-        for (uint32_t s = 0; s < rows; ++s) {
-            volatile float tt = t + dt;
+        for (uint32_t s = 0; s < rows * ts; ++s) {
+            volatile float tt = t + view.dt;    // dt, or dt / t_steps per substep
             t = tt;
         }
         steps += rows;

@@ -99,6 +99,7 @@ public:
     int refresh_view();
     int ensure_dj();
     int ensure_djf();
+    int use_substep_params(uint32_t ts);   // point the view at the dt / ts constants (ts 1: the plain ones)
     int ensure_hist(uint32_t rows, bool record, bool samples = false);
     int begin_run_chunk(uint64_t run_base, uint32_t rows, bool stats);
     int finish_hist(uint32_t rows, uint32_t out_row0, const dtb_run_output& out, bool freq, bool vmean, bool record);
@@ -145,6 +146,11 @@ public:
     unsigned long long* dJf = nullptr;   // fixed-mode sums, allocated on first use
     uint32_t fix_shift = 0;              // fixed_shift_for() of the network (0: mode unavailable)
     PopParams* pop_dev = nullptr;
+    PopParams* pop_sub_dev = nullptr;    // constants for substeps of dt / sub_ts (t_steps runs)
+    float* np_sub_dev = nullptr;         // the same per neuron (per-neuron mode)
+    uint32_t sub_ts = 0;                 // substeps the *_sub tables were derived for (0: none)
+    uint32_t view_ts = 1;                // substeps the device view steps by (1 outside t_steps runs)
+    uint64_t params_version = 0, sub_version = ~0ull;   // property changes since creation
     uint32_t* pop_off_dev = nullptr;
     float* np_dev = nullptr;
     unsigned long long* out_ptr = nullptr;
@@ -204,12 +210,15 @@ public:
     std::vector<TuneEntry> tune_report;
     int tune_push(const LaunchBatch& b, int acc);
     // Window graphs of the plain path: a chunk of push-mode steps is launched eagerly
-    // the first time its shape is seen, captured into a CUDA graph the second time
-    // and replayed from then on (one graph kept per engine).
+    // the first two times its shape is seen in a row, captured into a CUDA graph the
+    // third time and replayed from then on (one graph kept per engine).  Capturing a
+    // 500-step window costs about as much as 20 eager steps of the 5M network, so a
+    // shape that does not repeat is never captured.
     bool use_graph = true;
     cudaGraphExec_t graph = nullptr;
     uint64_t graph_key[10] = {};
     uint64_t seen_key[10] = {};
+    uint32_t seen_count = 0;
     uint32_t graph_launches = 0;
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     NetView view{};

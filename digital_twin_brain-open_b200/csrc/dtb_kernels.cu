@@ -75,11 +75,13 @@ constexpr uint32_t kSlotsPerTile = kLifThreads;
 static_assert(kLifTile == 4 * kLifThreads, "a LIF thread steps four neurons");
 
 // Normal draws (OU) and uniforms (noise train) for the four neurons of a slot.
+// Substep k of ts draws from its own streams: injected row (n - inj_base - 1) ts + k,
+// Philox stream word XOR k << 20 (k = 0 is the plain step's stream).
 __device__ inline void draw_noise(const NetView& nv, uint32_t tile_first, uint32_t slot, unsigned long long n,
                                   unsigned long long inj_base, bool injected, bool need_u, float z[4], float u[4],
-                                  uint32_t& err) {
+                                  uint32_t& err, uint32_t sub = 0, uint32_t ts = 1) {
     if (injected) {
-        const unsigned long long row = n - inj_base - 1;
+        const unsigned long long row = (n - inj_base - 1) * ts + sub;
         if (row < nv.inj_rows && nv.inj_z != nullptr) {
             const float* zr = nv.inj_z + row * nv.n_pad + tile_first + slot;
 #pragma unroll
@@ -102,11 +104,11 @@ __device__ inline void draw_noise(const NetView& nv, uint32_t tile_first, uint32
     } else {
         const uint32_t k0 = static_cast<uint32_t>(nv.seed), k1 = static_cast<uint32_t>(nv.seed >> 32);
         const uint32_t ctr = (tile_first >> 2) + slot;
-        const U4 r = philox4x32_10(U4{ctr, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamOU}, k0, k1);
+        const U4 r = philox4x32_10(U4{ctr, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamOU ^ (sub << 20)}, k0, k1);
         box_muller(r.x, r.y, z[0], z[1]);
         box_muller(r.z, r.w, z[2], z[3]);
         if (need_u) {
-            const U4 q = philox4x32_10(U4{ctr, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamNoise}, k0, k1);
+            const U4 q = philox4x32_10(U4{ctr, static_cast<uint32_t>(n), static_cast<uint32_t>(n >> 32), kStreamNoise ^ (sub << 20)}, k0, k1);
             u[0] = u01(q.x); u[1] = u01(q.y); u[2] = u01(q.z); u[3] = u01(q.w);
         }
     }
@@ -311,6 +313,12 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
     const bool use_ou = (flags & kFlagUseOU) != 0;
     const bool need_u = prop_mode != PROP_THRESHOLD;
     const bool injected = (flags & kFlagInjected) != 0;
+    // substep k of ts: spikes OR into the step's bitmap and list (a neuron enters the list
+    // once), counts are of neurons newly spiking, V statistics and samples come from the
+    // last substep, and the clock's step count advances after it (dist_simulator.cpp:2085-2112)
+    const uint32_t sub = (flags >> kSubShift) & 0xFFu;
+    const uint32_t ts = max(1u, (flags >> kTsShift) & 0xFFu);
+    const bool last_sub = sub + 1 >= ts;
     uint32_t late = 0;                 // a bulk-copy wait ran out
     uint32_t done_here = 0;            // tiles of cur_net this CTA finished (thread 0's ticket)
     float t_last_tile = 0.f;
@@ -377,10 +385,19 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
         if ((stats || record) && (row < 0 || row >= static_cast<long long>(nv.hist_cap))) {
             stats = false; record = false; err |= kErrHistOverflow;
         }
-        const bool sample = (flags & kFlagSample) && nv.n_samples && row >= 0 && row < static_cast<long long>(nv.hist_cap);
+        const bool sample = (flags & kFlagSample) && nv.n_samples && row >= 0 && row < static_cast<long long>(nv.hist_cap) &&
+                            last_sub;
         StatAcc sa{s_cnt, s_vs, p_tile};
         float z[4], u[4] = {1.f, 1.f, 1.f, 1.f};
-        draw_noise(nv, tile_first, tid, n, inj_base, injected, need_u, z, u, err);
+        draw_noise(nv, tile_first, tid, n, inj_base, injected, need_u, z, u, err, sub, ts);
+        // propagated spikes of this step's earlier substeps, one word per k of this warp
+        uint32_t old_w[4] = {0u, 0u, 0u, 0u};
+        if (sub) {
+            const uint32_t* bits = parity ? nv.bits1 : nv.bits0;
+            const uint32_t word0 = (tile_first >> 5) + (tid >> 5);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) old_w[k] = bits[word0 + (kSlotsPerTile / 32) * k];
+        }
         if (!mbar_wait_bounded(&s_bar[stg], (it >> 1) & 1u)) {
             late = 1;
             mbar_wait_bounded(&s_bar[stg], (it >> 1) & 1u);
@@ -452,30 +469,33 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
                 sJ[ks] = make_float4(in.J[0], in.J[1], in.J[2], in.J[3]);
             }
             const bool sp = propagated(prop_mode, o.active, u[k], pp.noise_rate);
+            const bool seen = (old_w[k] >> lane) & 1u;     // spiked in an earlier substep of this step
             nib_prop |= static_cast<uint32_t>(sp) << k;
             nib_act |= static_cast<uint32_t>(o.active) << k;
-            if (sp) ev += __ldg(nv.out_deg + i);
+            if (sp && !seen) ev += __ldg(nv.out_deg + i);
             // sampled neurons (stat_samples_kernel, src/stage/stat_result.cpp:393-431)
             if (sample) {
                 const uint32_t sbw = __ldg(nv.sample_bits + (i >> 5)), sh = i & 31u;
                 if ((sbw >> sh) & 1u) {
                     const size_t so = static_cast<size_t>(row) * nv.n_samples + __ldg(nv.sample_pre + (i >> 5)) +
                                       __popc(sbw & ((1u << sh) - 1u));
-                    nv.hist_sspk[so] = static_cast<uint8_t>(o.active);
+                    nv.hist_sspk[so] = static_cast<uint8_t>(o.active || seen);
                     nv.hist_sv[so] = o.V;
                     nv.hist_siou[so] = o.iou;
                 }
             }
             if (stats) {
                 if (excluded(nv, i)) { uniform = false; continue; }
+                const int fresh = o.active && !seen;
+                const long long vq = last_sub ? v_fix(o.V) : 0ll;
                 if (p == p_first) {
-                    cnt_acc += o.active;
-                    vs_acc += v_fix(o.V);
+                    cnt_acc += fresh;
+                    vs_acc += vq;
                 } else if (p == p_first + 1) {
-                    cnt_nxt += o.active;
-                    vs_nxt += v_fix(o.V);
+                    cnt_nxt += fresh;
+                    vs_nxt += vq;
                 } else {                      // a population narrower than a thread's span
-                    stat_add(nv, sa, row, p, o.active, v_fix(o.V));
+                    stat_add(nv, sa, row, p, fresh, vq);
                 }
             }
         }
@@ -489,13 +509,17 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
             uint32_t wprop[4], wtotal = 0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                wprop[k] = __ballot_sync(0xffffffffu, (nib_prop >> k) & 1u);
+                const uint32_t all = __ballot_sync(0xffffffffu, (nib_prop >> k) & 1u);
+                wprop[k] = all & ~old_w[k];                     // new to the step's list
                 wtotal += __popc(wprop[k]);
                 const uint32_t wact = __ballot_sync(0xffffffffu, (nib_act >> k) & 1u);
                 if (lane == 0) {
                     const uint32_t word = word0 + (kSlotsPerTile / 32) * k;
-                    bits[word] = wprop[k];
-                    if (record) nv.rec_bits[static_cast<size_t>(row) * nv.n_words + word] = wact;
+                    bits[word] = all | old_w[k];
+                    if (record) {
+                        uint32_t* rw = nv.rec_bits + static_cast<size_t>(row) * nv.n_words + word;
+                        *rw = sub ? (*rw | wact) : wact;
+                    }
                 }
             }
             if ((flags & kFlagList) && wtotal) {
@@ -553,7 +577,7 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
         if (lane == 0 && err) atomicOr(&nv.clock->err, err);
         if (tid == 0) {
             t_last_tile = t;
-            n_last_tile = n;
+            n_last_tile = last_sub ? n : n_prev;
             ++done_here;
         }
     }

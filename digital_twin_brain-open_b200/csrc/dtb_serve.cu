@@ -216,7 +216,7 @@ int Server::play_sequential(uint32_t n, dtb_request* reqs) {
             scratch.resize(static_cast<size_t>(r.iters) * sn.P);
             fr = scratch.data();
         }
-        dtb_run_request rq{r.iters, flags, DTB_PROP_THRESHOLD, o.syn_mode, {0, 0, 0, 0}};
+        dtb_run_request rq{r.iters, flags, DTB_PROP_THRESHOLD, o.syn_mode, 1, {0, 0, 0}};
         dtb_run_output out{};
         out.freqs = fr;
         r.status = sn.eng->run(rq, out);
@@ -283,7 +283,7 @@ int Server::play_batched(uint32_t n, dtb_request* reqs) {
             outs[i] = dtb_run_output{};
             outs[i].freqs = fr + static_cast<size_t>(done_steps[q]) * nets[reqs[q].net].P;
         }
-        dtb_run_request rq{slice, flags, DTB_PROP_THRESHOLD, o.syn_mode, {0, 0, 0, 0}};
+        dtb_run_request rq{slice, flags, DTB_PROP_THRESHOLD, o.syn_mode, 1, {0, 0, 0}};
         DTB_TRY(batch->run(rq, outs.data()));
         ++stats.slices;
         stats.batch_members_sum += inflight.size();

@@ -74,7 +74,7 @@ class EngineInfo(C.Structure):
 
 class RunRequest(C.Structure):
     _fields_ = [("iters", C.c_uint32), ("flags", C.c_uint32), ("prop_mode", C.c_uint32),
-                ("syn_mode", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+                ("syn_mode", C.c_uint32), ("t_steps", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 class RunOutput(C.Structure):
@@ -426,8 +426,9 @@ class Engine:
     def run(self, iters, use_ou=True, freq=True, vmean=False, record_spikes=False,
             prop_mode=PROP_THRESHOLD, syn_mode=SYN_PUSH, time_kernels=False, out=None,
             sample_spike=False, sample_v=False, sample_iou=False, imean=False, receptor_imean=False,
-            sample_isyn=False):
-        """Advance ``iters`` steps (RunRequest, snn.proto:63-77).
+            sample_isyn=False, t_steps=1):
+        """Advance ``iters`` steps (RunRequest, snn.proto:63-77), each of ``t_steps``
+        substeps of dt / t_steps when t_steps > 1.
 
         ``out`` may pass preallocated (freqs, vmeans) host arrays of shape [iters, P].
         """
@@ -444,7 +445,7 @@ class Engine:
         sv = np.zeros((iters, ns), np.float32) if sample_v else None
         si = np.zeros((iters, ns), np.float32) if sample_iou else None
         sy = np.zeros((iters, ns), np.float32) if sample_isyn else None
-        rq = RunRequest(iters, flags, prop_mode, syn_mode)
+        rq = RunRequest(iters, flags, prop_mode, syn_mode, t_steps)
         if out is not None:
             fr, vm = out
         else:

@@ -166,8 +166,8 @@ class SnnService(pbg.SnnServicer):
             status = pb.SNN_INVALID_PARAMETER
         elif request.t_steps > 1 and not request.use_ou_background:
             status = pb.SNN_INVALID_PARAMETER
-        elif request.t_steps > 1:
-            status = pb.SNN_UNSUPPORTED
+        elif request.t_steps > 255 or (request.t_steps > 1 and self.syn_mode == E.SYN_PULL):
+            status = pb.SNN_UNSUPPORTED     # substeps need a push mode; at most 255 per step
         elif ((request.output_imean or request.output_receptor_imeas or request.output_sample_isynaptic)
               and self.syn_mode == E.SYN_PULL):
             status = pb.SNN_UNSUPPORTED     # the pull kernel completes J one step later
@@ -184,7 +184,7 @@ class SnnService(pbg.SnnServicer):
                                  sample_spike=request.output_sample_spike, sample_v=request.output_sample_vmemb,
                                  sample_iou=request.output_sample_iou, imean=request.output_imean,
                                  receptor_imean=request.output_receptor_imeas,
-                                 sample_isyn=request.output_sample_isynaptic)
+                                 sample_isyn=request.output_sample_isynaptic, t_steps=max(1, request.t_steps))
                 for k in range(it):
                     resp = pb.RunResponse(status=pb.SNN_OK)
                     if request.output_freq:

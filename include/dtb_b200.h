@@ -174,7 +174,16 @@ typedef struct dtb_run_request {
     uint32_t flags;      /* DTB_RUN_*                                                            */
     uint32_t prop_mode;  /* dtb_prop_mode                                                        */
     uint32_t syn_mode;   /* dtb_syn_mode                                                         */
-    uint32_t reserved[4];
+    uint32_t t_steps;    /* RunRequest.t_steps: substeps per step (0 or 1: none; at most 255).
+                            Each step then runs t_steps substeps of dt / t_steps -- OU, membrane
+                            update and threshold, receptor decay with no input between them --
+                            spikes OR-ed over the substeps and propagated once after the last
+                            (tools/dist_simulator.cpp:2085-2112, src/block.cpp:729-737, 875-888);
+                            outputs stay per step: counts are of neurons that spiked in any
+                            substep, V means and samples are taken after the last substep.
+                            Needs DTB_RUN_USE_OU, threshold propagation and a push mode, as the
+                            reference's Run validation requires OU (dist_simulator.cpp:3225-3234) */
+    uint32_t reserved[3];
 } dtb_run_request;
 
 typedef struct dtb_run_output {

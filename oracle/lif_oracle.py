@@ -223,6 +223,41 @@ class LifOracle:
         self.steps_done += 1
         return active, prop
 
+    def step_substeps(self, zs):
+        """One step of ``len(zs)`` substeps, the C++ engine's ``t_steps`` loop
+        (tools/dist_simulator.cpp:2085-2112), on an oracle built with ``dt = dt_step /
+        t_steps`` in float32 (src/block.cpp:304, 317, 668, 1275 derive every factor from
+        ``delta_t_ / t_steps_``).  Each substep: OU, membrane update and threshold with
+        block_new's equations, its spikes OR-ed into the step's record
+        (``update_F_accumulated_spike_gpu``, src/block.cpp:729-737) and t_last set;
+        between substeps J decays with no input and I_syn is recomputed
+        (``update_J_presynaptic_per_step_gpu``, src/block.cpp:875-888); after the last,
+        the recorded spikes are propagated once: J = J*decay + W.s.  Threshold
+        propagation only (the reference requires the OU background for substeps,
+        dist_simulator.cpp:3225-3234).  Returns the recorded spikes [N] bool.
+        """
+        d = self.dtype
+        rec = np.zeros(self.n, bool)
+        for k, z in enumerate(zs):
+            self.t = _f(d, self.t + _f(d, self.dt))
+            self.i_bg = self.i_bg + (self.ou_f1 * (self.ou_mean - self.i_bg) + self.ou_f2s * np.asarray(z, d))
+            main = self.neg_gL * (self.V - self.V_L)
+            cd = ((main + self.I_syn) + self.i_ext) + self.i_bg
+            v_normal = self.V + self.dtC * cd
+            v = np.where(self.t >= (self.t_last + self.T_ref), v_normal, self.V_reset)
+            active = v >= self.V_th
+            self.V = np.minimum(v, self.V_th)
+            rec |= active
+            self.t_last = np.where(active, self.t, self.t_last)
+            if k + 1 < len(zs):
+                self.J = self.J * self.decay
+            else:
+                self.J = self.J * self.decay + self.synaptic_input(rec)
+            self.I_u = (self.g_u * (self.V_u - self.V)) * self.J
+            self.I_syn = ((self.I_u[0] + self.I_u[1]) + self.I_u[2]) + self.I_u[3]
+        self.steps_done += 1
+        return rec
+
     def population_stats(self, active, pop_ids=None):
         """(spike count [P] int64, mean V [P] float64) over each population.
 

@@ -115,7 +115,7 @@ def test_ensemble_members_equal_their_solo_runs(gpu):
     graph-replayed 800-step windows with g_AMPA multiplied per population between
     windows (DA_voxel.py:309-353): every member equals its solo run bit for bit."""
     specs = _member_specs()
-    windows, W = 3, 800
+    windows, W = 4, 800
     g_ampa = E.PROP_IDS["CONDUCT_G_AMPA"]
     rng = np.random.default_rng(7)
     factors = [[rng.uniform(0.97, 1.03, s.n_pops).astype(np.float32) for s in specs] for _ in range(windows)]
