@@ -655,8 +655,22 @@ int Engine::create_from_npz(const std::string& path, const dtb_options& opt) {
     if (w.dtype == "<f4") wt = DTB_W_F32;
     else if (w.dtype == "<f8") wt = DTB_W_F64;
     else if (w.dtype == "<f2") wt = DTB_W_F16;
-    else if (w.dtype == "|u1" || w.dtype == "|i1") wt = DTB_W_U8;
+    else if (w.dtype == "|u1" || w.dtype == "|i1") wt = DTB_W_U8;   // bytes read as unsigned, value / 255
     else return fail(DTB_UNSUPPORTED, "weight dtype " + w.dtype);
+    // The reference takes the weight type from the directory in the path
+    // (src/configuration.cpp:1411-1435: "/double", "/single", "/half", "/int8" or "/uint8",
+    // the first of them found from the end wins in that order of tests); the file's own
+    // dtype must agree.  A path with none of them is taken by its dtype (the reference
+    // refuses it as an unknown block type).
+    const struct { const char* dir; uint32_t type; } rule[] = {
+        {"/double", DTB_W_F64}, {"/single", DTB_W_F32}, {"/half", DTB_W_F16}, {"/int8", DTB_W_U8}, {"/uint8", DTB_W_U8}};
+    for (const auto& r : rule) {
+        if (path.rfind(r.dir) == std::string::npos) continue;
+        if (r.type != wt)
+            return fail(DTB_INVALID_NETWORK, "weight dtype " + w.dtype + " does not match the directory " + r.dir +
+                                                 " of " + path);
+        break;
+    }
     std::vector<int16_t> blk;
     if (found[1]) {
         const NpyArray& b = arr[1];
@@ -1326,6 +1340,20 @@ int Engine::update_gamma(uint32_t cnt, const uint32_t* pid, const uint32_t* pop,
     return upload_params();
 }
 
+int Engine::read_property(uint32_t prop_id, float* dst) const {
+    if (!dst) return fail(DTB_INVALID_PARAMETER, "NULL destination");
+    if (prop_id >= DTB_N_PROPS) return fail(DTB_INVALID_PARAMETER, "unknown property id");
+    for (uint32_t p = 0; p < P; ++p) {
+        for (uint32_t i = pop_off[p]; i < pop_off[p + 1]; ++i) {
+            RawParams r = per_neuron ? neuron_raw[i] : pop_raw[p];
+            float* f = nullptr;
+            raw_field(r, prop_id, &f);
+            dst[i] = *f;
+        }
+    }
+    return DTB_OK;
+}
+
 int Engine::set_ou(uint32_t cnt, const uint32_t* pop, const float* mean, const float* sigma, const float* tau) {
     if (cnt == 0) return DTB_OK;
     if (!pop || !mean || !sigma || !tau) return fail(DTB_INVALID_PARAMETER, "NULL array");
@@ -1716,6 +1744,11 @@ int32_t dtb_update_prop_cols(void* engine, uint32_t n, const uint32_t* pid, cons
 int32_t dtb_update_gamma(void* engine, uint32_t n, const uint32_t* pid, const uint32_t* pop, const float* alpha, const float* beta) {
     if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
     return guarded([&] { return as_engine(engine)->update_gamma(n, pid, pop, alpha, beta); });
+}
+
+int32_t dtb_read_property(void* engine, uint32_t prop_id, float* values) {
+    if (!engine) return dtb::fail(DTB_INVALID_PARAMETER, "NULL engine");
+    return guarded([&] { return as_engine(engine)->read_property(prop_id, values); });
 }
 
 int32_t dtb_set_ou(void* engine, uint32_t n, const uint32_t* pop, const float* mean, const float* sigma, const float* tau) {

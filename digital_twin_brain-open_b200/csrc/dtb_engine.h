@@ -84,6 +84,7 @@ public:
     int update_prop_cols(uint32_t n, const uint32_t* pid, const uint32_t* pop, const float* val, int assign);
     int update_gamma(uint32_t n, const uint32_t* pid, const uint32_t* pop, const float* alpha, const float* beta);
     int set_ou(uint32_t n, const uint32_t* pop, const float* mean, const float* sigma, const float* tau);
+    int read_property(uint32_t prop_id, float* dst) const;
     int set_noise(uint32_t source, uint32_t steps, const float* z, const float* u);
     int set_samples(uint32_t count, const uint32_t* idx);
     int read_state(int which, void* dst);

@@ -108,6 +108,7 @@ SIGNATURES = {
     "dtb_update_prop_cols": (_I32, [_P, _U32, _P, _P, _P, _I32]),
     "dtb_update_gamma": (_I32, [_P, _U32, _P, _P, _P, _P]),
     "dtb_set_ou": (_I32, [_P, _U32, _P, _P, _P, _P]),
+    "dtb_read_property": (_I32, [_P, _U32, _P]),
     "dtb_set_noise": (_I32, [_P, _U32, _U32, _P, _P]),
     "dtb_set_samples": (_I32, [_P, _U32, _P]),
     "dtb_run": (_I32, [_P, _P, _P]),
@@ -404,6 +405,12 @@ class Engine:
     def update_gamma(self, prop_ids, pop_ids, alpha, beta):
         pid, pop, a, b = _u32(prop_ids), _u32(pop_ids), _f32(alpha), _f32(beta)
         _check(LIB.dtb_update_gamma(self._h, pid.shape[0], _ptr(pid), _ptr(pop), _ptr(a), _ptr(b)))
+
+    def read_property(self, prop_id):
+        """Per-neuron value of property ``prop_id`` (PROP_IDS) as the updates left it."""
+        a = np.empty(self.n, np.float32)
+        _check(LIB.dtb_read_property(self._h, int(prop_id), _ptr(a)))
+        return a
 
     def set_ou(self, pop_ids, mean, sigma, tau):
         pop, m, s, t = _u32(pop_ids), _f32(mean), _f32(sigma), _f32(tau)

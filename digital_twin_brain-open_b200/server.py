@@ -96,7 +96,12 @@ def merge_blocks(files):
 class SnnService(pbg.SnnServicer):
     """The ``snn.Snn`` service backed by one engine."""
 
-    def __init__(self, syn_mode=E.SYN_PUSH, device_weight=None, seed=0, chunk=1000, stop_event=None):
+    def __init__(self, syn_mode=E.SYN_PUSH, device_weight=None, seed=0, chunk=1000, stop_event=None,
+                 engine_factory=None):
+        """``engine_factory(net, **options)`` builds the engine of an Init (default
+        ``engine.Engine.from_arrays``, the CUDA engine); a test can hand in another
+        object with the same methods."""
+        self.engine_factory = engine_factory or E.Engine.from_arrays
         self.syn_mode = syn_mode
         self.device_weight = device_weight
         self.seed = seed
@@ -141,8 +146,8 @@ class SnnService(pbg.SnnServicer):
                 dev_wt = {E.W_F64: E.W_F32, E.W_F32: E.W_F32, E.W_F16: E.W_F16, E.W_U8: E.W_U8}[in_wt]
             if self.eng is not None:
                 self.eng.close()
-            self.eng = E.Engine.from_arrays(net, dt=request.delta_t or 1.0, weight_type=dev_wt, seed=self.seed,
-                                            push=self.syn_mode != E.SYN_PULL, pull=self.syn_mode == E.SYN_PULL)
+            self.eng = self.engine_factory(net, dt=request.delta_t or 1.0, weight_type=dev_wt, seed=self.seed,
+                                           push=self.syn_mode != E.SYN_PULL, pull=self.syn_mode == E.SYN_PULL)
             self.blocks = blocks
             self.iterations = 0
             self.n_samples = 0

@@ -267,6 +267,10 @@ int32_t dtb_update_prop_cols(void* engine, uint32_t n, const uint32_t* prop_ids,
  * population (src/stage/property.cpp:494-651). */
 int32_t dtb_update_gamma(void* engine, uint32_t n, const uint32_t* prop_ids,
                          const uint32_t* pop_ids, const float* alpha, const float* beta);
+/* The current value of one property (dtb_prop_id) for every neuron [n_neurons], as
+ * creation and the Update* calls left it (REF_T in ms).  No reference counterpart:
+ * the reference keeps the properties on the device and offers no read. */
+int32_t dtb_read_property(void* engine, uint32_t prop_id, float* values);
 /* Updateoubackgroundparam: per-population OU mean, sigma, tau
  * (src/block.cpp:222-281). A population's OU current is reset to its mean the
  * first time it is configured, as the reference does. */

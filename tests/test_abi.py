@@ -121,3 +121,15 @@ def test_server_rejects_bad_traces_without_a_device():
     o.slice_steps = 0
     h = C.c_void_p()
     assert E.LIB.dtb_server_create(C.byref(o), C.byref(h)) == E.INVALID_PARAMETER
+
+
+def test_npz_directory_must_agree_with_the_weight_dtype(tmp_path):
+    """The weight type named by the path's directory (src/configuration.cpp:1411-1435)
+    must match the file's dtype; the check happens before any device work."""
+    net = nw.make_uniform_block(50, 5, seed=1)
+    d = tmp_path / "half"
+    os.makedirs(d)
+    nw.write_npz(str(d / "block_0.npz"), net)             # float32 weights under half/
+    with pytest.raises(E.DtbError) as ei:
+        E.Engine.from_npz(str(d / "block_0.npz"))
+    assert ei.value.status == E.INVALID_NETWORK and "/half" in str(ei.value)

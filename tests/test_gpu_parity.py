@@ -204,14 +204,6 @@ def test_property_updates_follow_oracle(gpu):
         assert np.array_equal(eng.read_state(E.STATE_V), o.V)
 
 
-def test_gamma_resample(gpu):
-    spec = nw.structured_spec(8000, 4, 40, seed=1)
-    with E.Engine.structured(spec) as eng:
-        eng.update_gamma([E.PROP_IDS["CONDUCT_G_AMPA"]], [1], [4.0], [400.0])
-        assert eng.info().per_neuron_params == 1
-        eng.run(50)   # runs with per-neuron parameters
-
-
 def test_save_load_round_trip(gpu):
     net = nw.make_uniform_block(5000, 50, seed=8)
     z, _ = lo.torch_noise_stream(5, 5000, 300, False)

@@ -59,7 +59,9 @@ def test_server_matches_direct_engine(gpu, tmp_path):
         r2 = _run(stub, iter=200, output_freq=True, freq_char=True, use_ou_background=True,
                   output_sample_spike=True, output_sample_vmemb=True, output_imean=True,
                   output_receptor_imeas=True, output_sample_isynaptic=True)
-        assert _run(stub, iter=5, t_steps=2, use_ou_background=True)[0].status == pb.SNN_UNSUPPORTED
+        sub = _run(stub, iter=5, t_steps=2, use_ou_background=True, output_freq=True)   # substeps run
+        assert len(sub) == 5 and all(r.status == pb.SNN_OK for r in sub)
+        assert _run(stub, iter=5, t_steps=2, use_ou_background=False)[0].status == pb.SNN_INVALID_PARAMETER
         assert not stub.Updatedopaminecurrentparam(iter([pb.UpdateDopamineCurrentParamRequest(block_id=0)])).success
         assert stub.Shutdown(pb.ShutdownRequest()).shutdown
         ch.close()

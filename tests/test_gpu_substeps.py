@@ -20,9 +20,12 @@ pytestmark = pytest.mark.gpu
 V_RTOL = 1e-5
 
 
+OU = (0.7, 0.2, 10.0)     # OU mean 0.7: the 3000-neuron block fires from step ~50 with substeps
+
+
 def _oracle(net, z, steps, ts):
     dts = float(np.float32(0.1) / np.float32(ts))
-    o = lo.LifOracle(net, dt=dts)
+    o = lo.LifOracle(net, dt=dts, ou=OU)
     rec = np.array([o.step_substeps(z[ts * s:ts * (s + 1)]) for s in range(steps)])
     return o, rec
 
@@ -34,7 +37,7 @@ def test_substeps_bit_exact(gpu, syn, ts):
     steps = 300
     z, _ = lo.torch_noise_stream(7, 3000, steps * ts, False)
     o, rec = _oracle(net, z, steps, ts)
-    with E.Engine.from_arrays(net, seed=1) as eng:
+    with E.Engine.from_arrays(net, seed=1, ou=OU) as eng:
         eng.set_noise_injected(z)
         eng.set_samples(np.arange(0, 3000, 97))
         r = eng.run(steps, record_spikes=True, vmean=True, sample_spike=True, sample_v=True, syn_mode=syn,
@@ -56,13 +59,13 @@ def test_substeps_float_push_until_divergence(gpu):
     net = nw.make_uniform_block(3000, 100, seed=2)
     steps, ts = 300, 2
     z, _ = lo.torch_noise_stream(8, 3000, steps * ts, False)
-    o = lo.LifOracle(net, dt=float(np.float32(0.1) / np.float32(ts)))
+    o = lo.LifOracle(net, dt=float(np.float32(0.1) / np.float32(ts)), ou=OU)
     vs, rec = [], []
     for s in range(steps):
         rec.append(o.step_substeps(z[ts * s:ts * (s + 1)]))
         vs.append(o.V[:64].copy())
     rec = np.array(rec)
-    with E.Engine.from_arrays(net, seed=1) as eng:
+    with E.Engine.from_arrays(net, seed=1, ou=OU) as eng:
         eng.set_noise_injected(z)
         eng.set_samples(np.arange(64))
         r = eng.run(steps, record_spikes=True, sample_v=True, syn_mode=E.SYN_PUSH, t_steps=ts)

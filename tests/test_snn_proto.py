@@ -8,7 +8,9 @@ import pytest
 from dtb_b200 import network as nw
 from dtb_b200 import snn_pb2 as pb
 
-REF_PROTO = "/root/reference/protos/snn.proto"
+# the reference checkout, when one is named (e.g. DTB_REFERENCE=/path/to/Digital_twin_brain-open)
+REF_ROOT = os.environ.get("DTB_REFERENCE", "")
+REF_PROTO = os.path.join(REF_ROOT, "protos", "snn.proto") if REF_ROOT else ""
 _TYPES = {"int32": pb.T_INT32, "float": pb.T_FLOAT, "double": pb.T_DOUBLE, "bool": pb.T_BOOL,
           "string": pb.T_STRING, "bytes": pb.T_BYTES}
 
@@ -24,7 +26,7 @@ def test_messages_round_trip():
     assert pb.PropType.NOISE_RATE == 19
 
 
-@pytest.mark.skipif(not os.path.exists(REF_PROTO), reason="reference checkout not present")
+@pytest.mark.skipif(not REF_PROTO or not os.path.exists(REF_PROTO), reason="DTB_REFERENCE names no reference checkout")
 def test_descriptor_matches_reference_proto():
     """Every message field (name, number, type, label) equals protos/snn.proto's."""
     text = re.sub(r"//.*", "", open(REF_PROTO).read())
