@@ -15,6 +15,7 @@
 namespace dtb {
 
 void set_error(const std::string& msg);
+const char* last_error();        // message of the last failure on the calling thread
 int fail(int status, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
 

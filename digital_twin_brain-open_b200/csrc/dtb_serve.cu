@@ -25,17 +25,24 @@
 // the OU parameters are re-applied, then the state blob (V, J, OU current,
 // t_last, spike bitmaps, clock) is loaded, and the device noise is keyed by
 // (seed, step, neuron).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <limits>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 
 #include "dtb_batch.h"
 
 namespace dtb {
+
+using WallClock = std::chrono::steady_clock;
 
 struct ServedNet {
     // how to rebuild it
@@ -58,11 +65,22 @@ struct ServedNet {
     std::vector<float> ou_mean, ou_sigma, ou_tau;
 };
 
+// A request submitted to the online scheduler (dtb_server_submit): the caller's
+// struct receives the outputs; the OU parameters are copied at submission.
+struct Job {
+    dtb_request* r = nullptr;
+    uint64_t ticket = 0;
+    std::vector<float> ou_mean, ou_sigma, ou_tau;
+    std::vector<int32_t> scratch;        // per-step counts when the caller passed no buffer
+    uint32_t done_steps = 0;
+    bool finished = false;
+};
+
 class Server {
 public:
     ~Server();
     dtb_server_options o{};
-    std::vector<ServedNet> nets;
+    std::deque<ServedNet> nets;           // stable addresses: engines are reached through references
     uint64_t resident_bytes = 0;
     uint64_t clock = 0;                   // LRU clock
     dtb_server_stats stats{};
@@ -76,9 +94,30 @@ public:
     int play(uint32_t n, dtb_request* reqs, uint32_t policy);
     int play_sequential(uint32_t n, dtb_request* reqs);
     int play_batched(uint32_t n, dtb_request* reqs);
+
+    // ---- online serving: a scheduler thread admits submitted requests as slots and
+    // device memory free up, between slices of the requests in flight
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::thread worker;
+    bool running = false, stopping = false;
+    uint32_t online_policy = DTB_SERVE_BATCHED;
+    int worker_status = DTB_OK;
+    std::string worker_error;
+    uint64_t next_ticket = 1;
+    std::deque<Job*> submitted;                       // not yet admitted, arrival order
+    std::map<uint64_t, std::unique_ptr<Job>> jobs;    // every job until its result is collected
+    WallClock::time_point t0_online;
+    int start(uint32_t policy);
+    int submit(dtb_request* r, uint64_t* ticket);
+    int poll(uint64_t ticket, uint32_t wait_ms, int32_t* done);
+    int stop();
+    void serve_online();
+    int online_slice(std::vector<Job*>& inflight, bool& changed, std::vector<Engine*>& members);
 };
 
 Server::~Server() {
+    stop();
     delete batch;
     for (ServedNet& sn : nets) delete sn.eng;
 }
@@ -114,16 +153,30 @@ int Server::evict(ServedNet& sn) {
     return DTB_OK;
 }
 
-// Bring network `id` into HBM, evicting idle networks (least recently used
-// first) while the cap would be exceeded.  *ok = false when only networks with
-// requests in flight stand in the way (the caller retries after a slice).
+// Device memory kept free beyond a network's own bytes when it is rebuilt (the
+// device CSR build sorts through temporary buffers).
+constexpr uint64_t kRebuildReserve = 1ull << 30;
+
+// Bring network `id` into HBM.  It is admitted when the resident networks stay
+// within the cap AND the device has the bytes free (cudaMemGetInfo: other engines
+// and other processes count too); idle networks are evicted, least recently used
+// first, until both hold.  *ok = false when only networks with requests in flight
+// stand in the way (the caller retries after a slice).
 int Server::make_resident(uint32_t id, bool* ok) {
     ServedNet& sn = nets[id];
     *ok = true;
     sn.last_use = ++clock;
     if (sn.eng) return DTB_OK;
     const uint64_t need = sn.bytes;
-    while (resident_bytes + need > o.hbm_cap_bytes) {
+    auto fits = [&](bool* yes) -> int {
+        size_t free_b = 0, total_b = 0;
+        DTB_CU(cudaMemGetInfo(&free_b, &total_b));
+        *yes = resident_bytes + need <= o.hbm_cap_bytes && free_b >= need + kRebuildReserve;
+        return DTB_OK;
+    };
+    bool yes = false;
+    DTB_TRY(fits(&yes));
+    while (!yes) {
         ServedNet* victim = nullptr;
         for (ServedNet& c : nets)
             if (c.eng && c.busy < 0 && &c != &sn && (!victim || c.last_use < victim->last_use)) victim = &c;
@@ -132,6 +185,7 @@ int Server::make_resident(uint32_t id, bool* ok) {
             return DTB_OK;
         }
         DTB_TRY(evict(*victim));
+        DTB_TRY(fits(&yes));
     }
     DTB_TRY(build(sn));
     ++stats.restores;
@@ -139,6 +193,10 @@ int Server::make_resident(uint32_t id, bool* ok) {
 }
 
 int Server::add(ServedNet&& sn_in, uint32_t* id) {
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (running) return fail(DTB_UNSUPPORTED, "networks are added before dtb_server_start or after dtb_server_stop");
+    }
     nets.push_back(std::move(sn_in));
     ServedNet& sn = nets.back();
     if (sn.structured) {
@@ -186,8 +244,6 @@ int Server::begin_request(dtb_request& r) {
     r.events = 0;
     return DTB_OK;
 }
-
-using WallClock = std::chrono::steady_clock;
 
 static double seconds_since(WallClock::time_point t0) {
     return std::chrono::duration<double>(WallClock::now() - t0).count();
@@ -309,7 +365,229 @@ int Server::play_batched(uint32_t n, dtb_request* reqs) {
     return DTB_OK;
 }
 
+int Server::start(uint32_t policy) {
+    if (policy > DTB_SERVE_SEQUENTIAL) return fail(DTB_INVALID_PARAMETER, "unknown serving policy");
+    std::lock_guard<std::mutex> lk(mu);
+    if (running) return fail(DTB_INVALID_PARAMETER, "the server is already serving");
+    for (ServedNet& sn : nets) sn.busy = -1;
+    online_policy = policy;
+    stopping = false;
+    worker_status = DTB_OK;
+    worker_error.clear();
+    t0_online = WallClock::now();
+    int dev = 0;
+    DTB_CU(cudaGetDevice(&dev));
+    running = true;
+    worker = std::thread([this, dev] {
+        cudaSetDevice(dev);
+        serve_online();
+    });
+    return DTB_OK;
+}
+
+int Server::submit(dtb_request* r, uint64_t* ticket) {
+    if (!r || !ticket) return fail(DTB_INVALID_PARAMETER, "NULL argument");
+    std::lock_guard<std::mutex> lk(mu);
+    if (!running || stopping) return fail(DTB_INVALID_PARAMETER, "the server is not serving (dtb_server_start)");
+    if (r->net >= nets.size()) return fail(DTB_INVALID_PARAMETER, "request for an unknown network");
+    if (r->iters == 0) return fail(DTB_INVALID_PARAMETER, "request with zero steps");
+    if (r->ou_mean && (!r->ou_sigma || !r->ou_tau)) return fail(DTB_INVALID_PARAMETER, "OU mean without sigma or tau");
+    auto job = std::make_unique<Job>();
+    job->r = r;
+    job->ticket = next_ticket++;
+    const uint32_t P = nets[r->net].P;
+    if (r->ou_mean) {
+        job->ou_mean.assign(r->ou_mean, r->ou_mean + P);
+        job->ou_sigma.assign(r->ou_sigma, r->ou_sigma + P);
+        job->ou_tau.assign(r->ou_tau, r->ou_tau + P);
+    }
+    if (!r->freqs) job->scratch.resize(static_cast<size_t>(r->iters) * P);
+    r->status = -1;
+    r->arrival_s = seconds_since(t0_online);
+    r->start_s = r->finish_s = 0.0;
+    r->events = 0;
+    *ticket = job->ticket;
+    submitted.push_back(job.get());
+    jobs[job->ticket] = std::move(job);
+    cv_work.notify_one();
+    return DTB_OK;
+}
+
+int Server::poll(uint64_t ticket, uint32_t wait_ms, int32_t* done) {
+    if (!done) return fail(DTB_INVALID_PARAMETER, "NULL argument");
+    std::unique_lock<std::mutex> lk(mu);
+    auto it = jobs.find(ticket);
+    if (it == jobs.end()) return fail(DTB_INVALID_PARAMETER, "unknown ticket (never submitted, or already collected)");
+    Job* j = it->second.get();
+    cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), [&] { return j->finished || !running; });
+    *done = j->finished ? 1 : 0;
+    if (j->finished) {
+        jobs.erase(it);      // collected: the caller's struct holds the outputs
+        return DTB_OK;
+    }
+    if (!running && worker_status != DTB_OK) return fail(worker_status, worker_error);
+    return DTB_OK;
+}
+
+int Server::stop() {
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!running) return DTB_OK;
+        stopping = true;
+        cv_work.notify_all();
+    }
+    if (worker.joinable()) worker.join();
+    std::lock_guard<std::mutex> lk(mu);
+    running = false;
+    cv_done.notify_all();
+    if (worker_status != DTB_OK) return fail(worker_status, worker_error);
+    return DTB_OK;
+}
+
+// One pass of the scheduler: admit waiting requests in arrival order (a network
+// holds one request at a time; room under the cap and in free device memory),
+// then advance every request in flight by one slice (batched) or run the oldest
+// to completion (sequential), and hand back the finished ones.
+int Server::online_slice(std::vector<Job*>& inflight, bool& changed, std::vector<Engine*>& members) {
+    std::vector<Job*> waiting;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        waiting.assign(submitted.begin(), submitted.end());
+    }
+    const uint32_t cap = online_policy == DTB_SERVE_SEQUENTIAL ? 1u : o.max_batch;
+    std::vector<Job*> admitted;
+    for (Job* j : waiting) {
+        if (inflight.size() >= cap) break;
+        dtb_request& r = *j->r;
+        if (nets[r.net].busy >= 0) continue;
+        bool ok = false;
+        DTB_TRY(make_resident(r.net, &ok));
+        if (!ok) break;
+        ServedNet& sn = nets[r.net];
+        sn.busy = static_cast<int>(j->ticket & 0x7FFFFFFF);
+        if (!j->ou_mean.empty()) {
+            sn.ou_mean = j->ou_mean;
+            sn.ou_sigma = j->ou_sigma;
+            sn.ou_tau = j->ou_tau;
+            DTB_TRY(sn.eng->set_ou(sn.P, sn.pop_ids.data(), j->ou_mean.data(), j->ou_sigma.data(), j->ou_tau.data()));
+        }
+        r.start_s = seconds_since(t0_online);
+        inflight.push_back(j);
+        admitted.push_back(j);
+        changed = true;
+    }
+    if (!admitted.empty()) {
+        std::lock_guard<std::mutex> lk(mu);
+        for (Job* j : admitted) submitted.erase(std::find(submitted.begin(), submitted.end(), j));
+    }
+    if (inflight.empty()) return DTB_OK;
+    const uint32_t flags = o.flags | DTB_RUN_FREQ;
+    std::vector<Job*> finished;
+    if (online_policy == DTB_SERVE_SEQUENTIAL) {
+        Job* j = inflight.front();
+        dtb_request& r = *j->r;
+        ServedNet& sn = nets[r.net];
+        dtb_run_request rq{r.iters, flags, DTB_PROP_THRESHOLD, o.syn_mode, 1, {0, 0, 0}};
+        dtb_run_output out{};
+        out.freqs = r.freqs ? r.freqs : j->scratch.data();
+        DTB_TRY(sn.eng->run(rq, out));
+        r.events = out.events;
+        j->done_steps = r.iters;
+        sn.last_use = ++clock;
+        finished.push_back(j);
+        inflight.clear();
+        ++stats.slices;
+        stats.batch_members_sum += 1;
+    } else {
+        uint32_t slice = o.slice_steps;
+        for (Job* j : inflight) slice = std::min(slice, j->r->iters - j->done_steps);
+        if (changed) {
+            members.clear();
+            for (Job* j : inflight) members.push_back(nets[j->r->net].eng);
+            if (!batch) {
+                batch = new Batch();
+                DTB_TRY(batch->create(members.data(), static_cast<uint32_t>(members.size())));
+                batch->push_cfg = PushCfg{PUSH_REG, 8, 32};
+                batch->autotune = o.autotune != 0;
+            } else {
+                DTB_TRY(batch->set_members(members.data(), static_cast<uint32_t>(members.size())));
+            }
+            changed = false;
+        }
+        std::vector<dtb_run_output> outs(inflight.size());
+        for (size_t i = 0; i < inflight.size(); ++i) {
+            Job* j = inflight[i];
+            int32_t* fr = j->r->freqs ? j->r->freqs : j->scratch.data();
+            outs[i] = dtb_run_output{};
+            outs[i].freqs = fr + static_cast<size_t>(j->done_steps) * nets[j->r->net].P;
+        }
+        dtb_run_request rq{slice, flags, DTB_PROP_THRESHOLD, o.syn_mode, 1, {0, 0, 0}};
+        DTB_TRY(batch->run(rq, outs.data()));
+        ++stats.slices;
+        stats.batch_members_sum += inflight.size();
+        for (size_t i = 0; i < inflight.size();) {
+            Job* j = inflight[i];
+            j->done_steps += slice;
+            j->r->events += outs[i].events;
+            nets[j->r->net].last_use = ++clock;
+            if (j->done_steps == j->r->iters) {
+                finished.push_back(j);
+                inflight.erase(inflight.begin() + static_cast<long>(i));
+                outs.erase(outs.begin() + static_cast<long>(i));
+                changed = true;
+            } else {
+                ++i;
+            }
+        }
+    }
+    if (!finished.empty()) {
+        const double t = seconds_since(t0_online);
+        std::lock_guard<std::mutex> lk(mu);
+        for (Job* j : finished) {
+            nets[j->r->net].busy = -1;
+            j->r->finish_s = t;
+            j->r->status = DTB_OK;
+            j->finished = true;
+        }
+        cv_done.notify_all();
+    }
+    return DTB_OK;
+}
+
+void Server::serve_online() {
+    std::vector<Job*> inflight;
+    std::vector<Engine*> members;
+    bool changed = true;
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_work.wait(lk, [&] { return stopping || !submitted.empty() || !inflight.empty(); });
+            if (stopping && submitted.empty() && inflight.empty()) break;
+        }
+        const int st = online_slice(inflight, changed, members);
+        if (st != DTB_OK) {
+            // a failure ends the scheduler: every unfinished request carries the status
+            std::lock_guard<std::mutex> lk(mu);
+            worker_status = st;
+            worker_error = last_error();
+            for (auto& kv : jobs) {
+                if (kv.second->finished) continue;
+                kv.second->r->status = st;
+                kv.second->finished = true;
+            }
+            for (ServedNet& sn : nets) sn.busy = -1;
+            submitted.clear();
+            cv_done.notify_all();
+            break;
+        }
+    }
+}
+
 int Server::play(uint32_t n, dtb_request* reqs, uint32_t policy) {
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (running) return fail(DTB_INVALID_PARAMETER, "the server is serving online (dtb_server_stop first)");
+    }
     for (uint32_t i = 0; i < n; ++i) {
         dtb_request& r = reqs[i];
         if (r.net >= nets.size()) return fail(DTB_INVALID_PARAMETER, "request for an unknown network");
@@ -406,6 +684,26 @@ int32_t dtb_server_add_npz(void* server, const char* path, const dtb_options* op
 int32_t dtb_server_play(void* server, uint32_t n, dtb_request* reqs, uint32_t policy) {
     if (!server || (n && !reqs)) return dtb::fail(DTB_INVALID_PARAMETER, "NULL argument");
     return server_guarded([&] { return static_cast<Server*>(server)->play(n, reqs, policy); });
+}
+
+int32_t dtb_server_start(void* server, uint32_t policy) {
+    if (!server) return dtb::fail(DTB_INVALID_PARAMETER, "NULL server");
+    return server_guarded([&] { return static_cast<Server*>(server)->start(policy); });
+}
+
+int32_t dtb_server_submit(void* server, dtb_request* req, uint64_t* ticket) {
+    if (!server) return dtb::fail(DTB_INVALID_PARAMETER, "NULL server");
+    return server_guarded([&] { return static_cast<Server*>(server)->submit(req, ticket); });
+}
+
+int32_t dtb_server_poll(void* server, uint64_t ticket, uint32_t wait_ms, int32_t* done) {
+    if (!server) return dtb::fail(DTB_INVALID_PARAMETER, "NULL server");
+    return server_guarded([&] { return static_cast<Server*>(server)->poll(ticket, wait_ms, done); });
+}
+
+int32_t dtb_server_stop(void* server) {
+    if (!server) return dtb::fail(DTB_INVALID_PARAMETER, "NULL server");
+    return server_guarded([&] { return static_cast<Server*>(server)->stop(); });
 }
 
 int32_t dtb_server_info(void* server, dtb_server_stats* info) {

@@ -137,6 +137,10 @@ SIGNATURES = {
     "dtb_server_add_npz": (_I32, [_P, C.c_char_p, _P, _P]),
     "dtb_server_play": (_I32, [_P, _U32, _P, _U32]),
     "dtb_server_info": (_I32, [_P, _P]),
+    "dtb_server_start": (_I32, [_P, _U32]),
+    "dtb_server_submit": (_I32, [_P, _P, C.POINTER(C.c_uint64)]),
+    "dtb_server_poll": (_I32, [_P, C.c_uint64, _U32, C.POINTER(C.c_int32)]),
+    "dtb_server_stop": (_I32, [_P]),
 }
 
 
@@ -577,6 +581,52 @@ class Server:
         inf = ServerInfo()
         _check(LIB.dtb_server_info(self._h, C.byref(inf)))
         return {f: getattr(inf, f) for f, _ in ServerInfo._fields_}
+
+    # ---- online serving (dtb_server_start / submit / poll / stop)
+    def start(self, policy=SERVE_BATCHED):
+        self._pending = {}
+        _check(LIB.dtb_server_start(self._h, policy))
+
+    def submit(self, net, iters, ou=None):
+        """Submit a request now (thread-safe); returns its ticket."""
+        P = self.n_pops[net] if 0 <= net < len(self.n_pops) else 1
+        req = Request()
+        req.net, req.iters = net, iters
+        fr = np.zeros((iters, P), np.int32)
+        req.freqs = fr.ctypes.data
+        keep = [fr]
+        if ou is not None:
+            m, sd, tau = (np.ascontiguousarray(x, np.float32) for x in ou)
+            keep.extend((m, sd, tau))
+            req.ou_mean, req.ou_sigma, req.ou_tau = m.ctypes.data, sd.ctypes.data, tau.ctypes.data
+        t = C.c_uint64()
+        _check(LIB.dtb_server_submit(self._h, C.byref(req), C.byref(t)))
+        self._pending[t.value] = (req, fr, keep)
+        return t.value
+
+    def poll(self, ticket, wait_s=0.0):
+        """None while the request runs; its result dict once done."""
+        done = C.c_int32()
+        _check(LIB.dtb_server_poll(self._h, ticket, int(wait_s * 1000), C.byref(done)))
+        if not done.value:
+            return None
+        req, fr, _ = self._pending.pop(ticket)
+        return dict(freqs=fr, start_s=req.start_s, finish_s=req.finish_s, arrival_s=req.arrival_s,
+                    latency_s=req.finish_s - req.arrival_s, events=int(req.events), status=req.status)
+
+    def wait(self, ticket, timeout_s=600.0):
+        """Block until the request is done (or raise after timeout_s)."""
+        import time
+        end = time.monotonic() + timeout_s
+        while True:
+            r = self.poll(ticket, wait_s=min(1.0, max(0.0, end - time.monotonic())))
+            if r is not None:
+                return r
+            if time.monotonic() >= end:
+                raise TimeoutError(f"request {ticket} not done after {timeout_s} s")
+
+    def stop(self):
+        _check(LIB.dtb_server_stop(self._h))
 
     def close(self):
         if self._h is not None and self._h.value:

@@ -370,6 +370,28 @@ int32_t dtb_server_add_npz(void* server, const char* path, const dtb_options* op
 int32_t dtb_server_play(void* server, uint32_t n, dtb_request* reqs, uint32_t policy);
 int32_t dtb_server_info(void* server, dtb_server_stats* info);
 
+/* Online serving: requests that are not known in advance, the gRPC Run path.
+ * dtb_server_start starts a scheduler thread on the calling thread's device with
+ * `policy`: DTB_SERVE_BATCHED admits submitted requests in arrival order as slots
+ * (max_batch) and device memory free up, between slices of slice_steps steps of the
+ * requests already in flight, which advance together; DTB_SERVE_SEQUENTIAL runs
+ * one request at a time.  A network is admitted while the resident networks stay
+ * within hbm_cap_bytes and the device has its bytes free (cudaMemGetInfo, plus
+ * 1 GiB for a rebuild); idle networks are evicted to the host otherwise.
+ * dtb_server_submit may be called from any thread: it copies the OU arrays, stamps
+ * arrival_s (seconds since start) and returns a ticket; `req` and its freqs buffer
+ * stay the caller's and must remain valid until the request is reported done.
+ * dtb_server_poll waits up to wait_ms for the ticket; *done = 1 once start_s,
+ * finish_s, events, freqs and status are filled in (the ticket is then retired).
+ * dtb_server_stop finishes every submitted request, then ends the thread; networks
+ * are added only while the scheduler is stopped, and dtb_server_play is refused
+ * while it runs.  A scheduler failure ends it: every unfinished request carries
+ * the status, and polls return it. */
+int32_t dtb_server_start(void* server, uint32_t policy);
+int32_t dtb_server_submit(void* server, dtb_request* req, uint64_t* ticket);
+int32_t dtb_server_poll(void* server, uint64_t ticket, uint32_t wait_ms, int32_t* done);
+int32_t dtb_server_stop(void* server);
+
 /* --- BOLD signal (data assimilation) ----------------------------------------
  * models/bold_model_pytorch.py:61-96, driven per simulated step by
  * data_assimilation/DA_voxel.py:314-331.  Parameters are doubles, as the

@@ -90,3 +90,73 @@ def test_eviction_round_trip_keeps_results(gpu):
     assert info["resident_bytes"] <= cap
     for g, r in zip(got, ref):
         assert np.array_equal(g["freqs"], r)
+
+
+@pytest.mark.parametrize("syn,wt", [(E.SYN_PUSH_EXACT, E.W_F32), (E.SYN_PUSH_FIXED, E.W_BF16)], ids=["exact-f32", "fixed-bf16"])
+def test_online_requests_from_two_threads_equal_solo_runs(gpu, syn, wt):
+    """dtb_server_submit from two client threads while slices run (each thread owns two
+    of the networks, so each network's requests keep their order): every request is
+    admitted as slots free up and its counts equal the request run alone."""
+    import threading
+    import time
+    specs = _specs()
+    reqs = _trace(specs, n_req=16, seed=9)
+    solo = [None] * len(reqs)
+    for i, s in enumerate(specs):
+        with E.Engine.structured(s, seed=i, weight_type=wt) as eng:
+            for j, r in enumerate(reqs):
+                if r["net"] == i:
+                    eng.set_ou(eng.pop_ids, *r["ou"])
+                    solo[j] = eng.run(r["iters"], syn_mode=syn).freqs
+    got = [None] * len(reqs)
+    with E.Server(slice_steps=50, max_batch=3, syn_mode=syn) as srv:
+        for i, s in enumerate(specs):
+            srv.add_structured(s, seed=i, weight_type=wt)
+        srv.start(E.SERVE_BATCHED)
+
+        def client(nets, pause):
+            tickets = []
+            for j, r in enumerate(reqs):
+                if r["net"] in nets:
+                    tickets.append((j, srv.submit(r["net"], r["iters"], r["ou"])))
+                    time.sleep(pause)
+            for j, t in tickets:
+                got[j] = srv.wait(t, timeout_s=300)
+
+        threads = [threading.Thread(target=client, args=({0, 1}, 0.004)),
+                   threading.Thread(target=client, args=({2, 3}, 0.007))]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        srv.stop()
+        info = srv.info()
+    assert all(g is not None for g in got)
+    assert info["batch_members_sum"] > info["slices"]                  # requests shared slices
+    starts = sorted(g["start_s"] for g in got)
+    assert any(g["arrival_s"] > starts[0] and g["arrival_s"] < max(x["finish_s"] for x in got) for g in got)
+    for j, (g, r) in enumerate(zip(got, solo)):
+        assert g["status"] == E.OK
+        assert g["finish_s"] >= g["start_s"] >= g["arrival_s"]
+        assert np.array_equal(g["freqs"], r), f"request {j}"
+    assert sum(int(r.sum()) for r in solo) > 0
+
+
+def test_online_rejects_and_recovers(gpu):
+    specs = _specs()[:1]
+    with E.Server(slice_steps=40) as srv:
+        srv.add_structured(specs[0], seed=0)
+        with pytest.raises(E.DtbError):
+            srv.submit(0, 100)                       # not serving yet
+        srv.start()
+        with pytest.raises(E.DtbError):
+            srv.add_structured(specs[0], seed=1)     # networks are added while stopped
+        with pytest.raises(E.DtbError):
+            srv.play([dict(net=0, iters=10, arrival_s=0.0)])
+        t = srv.submit(0, 120)
+        r = srv.wait(t)
+        assert r["status"] == E.OK and r["freqs"].shape == (120, specs[0].n_pops)
+        with pytest.raises(E.DtbError):
+            srv.poll(t)                              # already collected
+        srv.stop()
+        assert srv.add_structured(specs[0], seed=1) == 1
