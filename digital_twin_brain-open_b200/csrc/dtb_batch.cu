@@ -20,6 +20,10 @@
 
 namespace dtb {
 
+// Consecutive LIF tiles per CTA in a batch of several members (lif_kernel): a member
+// switch costs a chain of dependent loads that miss the L1, paid once per chunk.
+constexpr uint32_t kBatchLifChunk = 4;
+
 Batch::~Batch() {
     if (stream) cudaStreamSynchronize(stream);
     if (graph) cudaGraphExecDestroy(graph);
@@ -120,6 +124,7 @@ int Batch::set_members(Engine* const* engines, uint32_t n) {
     lb.pull_tiles_total = pre[(n + 1) + n];
     lb.push_ctas = static_cast<uint32_t>(sm_count) * 8u;
     lb.lif_ctas = static_cast<uint32_t>(sm_count) * m[0]->lif_ctas_per_sm;
+    lb.lif_chunk = n > 1 ? kBatchLifChunk : 1u;
     lb.spikes = SpikeList{list, list_count, list_ticket, static_cast<uint32_t>(total)};
     lb.tile_net = tile_net;
     lb.win_prefix = d_prefix + 3 * (n + 1);

@@ -248,6 +248,7 @@ LaunchBatch Engine::single_batch() const {
     b.pull_tiles_total = n_pad / kPullTile;
     b.push_ctas = static_cast<uint32_t>(sm_count) * 8u;
     b.lif_ctas = static_cast<uint32_t>(sm_count) * lif_ctas_per_sm;
+    b.lif_chunk = 1;
     b.spikes = SpikeList{list, list_count, list_ticket, n_pad};
     b.win_prefix = prefix_dev + 6;
     b.windows_total = n_windows;

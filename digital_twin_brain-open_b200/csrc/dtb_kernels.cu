@@ -298,11 +298,20 @@ __device__ __forceinline__ void lif_ticket(const NetView& nv, uint32_t cnt, floa
     }
 }
 
+// A CTA steps chunks of `chunk` consecutive tiles, chunks strided by the grid:
+// tile gt is followed by gt + 1 inside its chunk, else by the CTA's next chunk.
+// Chunks of several tiles keep a batch CTA on one member for several tiles, so the
+// member's view, clock and parameters are fetched once per chunk, not per tile.
+__device__ __forceinline__ uint32_t lif_next_tile(uint32_t gt, uint32_t chunk, uint32_t total_tiles) {
+    if (gt % chunk + 1 < chunk && gt + 1 < total_tiles) return gt + 1;
+    return (gt / chunk + gridDim.x) * chunk;
+}
+
 template <int JM>
 __global__ void __launch_bounds__(kLifThreads, 3)
 lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_prefix,
            const uint32_t* __restrict__ vbase, uint32_t n_nets, uint32_t total_tiles, SpikeList sl, uint32_t flags,
-           int prop_mode, const uint32_t* __restrict__ tile_net) {
+           int prop_mode, const uint32_t* __restrict__ tile_net, uint32_t chunk) {
     extern __shared__ __align__(128) float lsm[];
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ int s_cnt[kStatSlots];
@@ -334,12 +343,13 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (blockIdx.x < total_tiles) lif_prefetch(nets, tile_prefix, tile_net, n_nets, blockIdx.x, lsm, &s_bar[0]);
+        if (blockIdx.x * chunk < total_tiles)
+            lif_prefetch(nets, tile_prefix, tile_net, n_nets, blockIdx.x * chunk, lsm, &s_bar[0]);
     }
     __syncthreads();
 
     uint32_t it = 0;
-    for (uint32_t gt = blockIdx.x; gt < total_tiles; gt += gridDim.x, ++it) {
+    for (uint32_t gt = blockIdx.x * chunk; gt < total_tiles; gt = lif_next_tile(gt, chunk, total_tiles), ++it) {
         const uint32_t net = tile_to_net(tile_net, tile_prefix, n_nets, gt);
         const uint32_t stg = it & 1u;
         if (net != cur_net) {
@@ -361,9 +371,10 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
         }
         // barrier A: the other stage's readers (previous tile) are done and its
         // store has been issued; refill it with the tile after this one
-        if (tid == 0 && gt + gridDim.x < total_tiles) {
+        const uint32_t gn = lif_next_tile(gt, chunk, total_tiles);
+        if (tid == 0 && gn < total_tiles) {
             bulk_wait_read();
-            lif_prefetch(nets, tile_prefix, tile_net, n_nets, gt + gridDim.x, lsm + (stg ^ 1u) * kLifStageFloats, &s_bar[stg ^ 1u]);
+            lif_prefetch(nets, tile_prefix, tile_net, n_nets, gn, lsm + (stg ^ 1u) * kLifStageFloats, &s_bar[stg ^ 1u]);
         }
         __syncthreads();
         const NetView& nv = nets[net];
@@ -1567,13 +1578,14 @@ cudaError_t launch_lif(const LaunchBatch& b, int jmode, uint32_t flags, int prop
         }
         attr_set.fetch_or(bit);
     }
-    const dim3 grid(std::min(b.lif_tiles_total, b.lif_ctas)), block(kLifThreads);
     const uint32_t T = b.lif_tiles_total;
+    const uint32_t chunk = std::max(1u, b.lif_chunk);
+    const dim3 grid(std::min((T + chunk - 1) / chunk, b.lif_ctas)), block(kLifThreads);
     switch (jmode) {
-        case J_DIRECT: lif_kernel<J_DIRECT><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net); break;
-        case J_FOLD: lif_kernel<J_FOLD><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net); break;
-        case J_FIXF: lif_kernel<J_FIXF><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net); break;
-        default: lif_kernel<J_ASIS><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net); break;
+        case J_DIRECT: lif_kernel<J_DIRECT><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net, chunk); break;
+        case J_FOLD: lif_kernel<J_FOLD><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net, chunk); break;
+        case J_FIXF: lif_kernel<J_FIXF><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net, chunk); break;
+        default: lif_kernel<J_ASIS><<<grid, block, kLifSmem, s>>>(b.nets, b.lif_prefix, b.vbase, b.n_nets, T, b.spikes, flags, prop_mode, b.tile_net, chunk); break;
     }
     return cudaGetLastError();
 }

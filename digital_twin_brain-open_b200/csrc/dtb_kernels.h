@@ -20,6 +20,7 @@ struct LaunchBatch {
     uint32_t pull_tiles_total;
     uint32_t push_ctas;
     uint32_t lif_ctas;            // persistent grid of the LIF kernel
+    uint32_t lif_chunk;           // consecutive tiles a LIF CTA steps before striding (0 or 1: one)
     const uint32_t* win_prefix;   // device [n_nets + 1] cumulative local-push windows
     uint32_t windows_total;
     uint32_t* local_scratch;      // device [2 * windows_total + 2]: rows per window, unit prefix, unit counter

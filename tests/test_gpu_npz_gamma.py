@@ -63,15 +63,18 @@ def test_block_files_in_every_weight_type(gpu, tmp_path, directory, dtype, devic
 
 @pytest.mark.parametrize("alpha,beta", [(4.0, 2000.0), (0.5, 50.0)])
 def test_gamma_draws(gpu, alpha, beta):
-    spec = nw.structured_spec(130_000, 2, 20, seed=3)
+    """About 1.1M draws: the sample mean's relative spread is 1 / sqrt(alpha n) (0.14 % at
+    alpha = 0.5) and the sample variance's sqrt((2 + 6 / alpha) / n) (0.36 %), so the 1 %
+    and 3 % bars sit beyond six standard deviations for both shapes."""
+    spec = nw.structured_spec(1_300_000, 2, 5, seed=3)
     g = E.PROP_IDS["CONDUCT_G_AMPA"]
     with E.Engine.structured(spec) as eng:
         before = {p: eng.read_property(p) for p in range(20)}
-        eng.update_gamma([g], [0], [alpha], [beta])                     # population 0: 118,129 neurons
+        eng.update_gamma([g], [0], [alpha], [beta])                     # population 0: 1,181,350 neurons
         after = {p: eng.read_property(p) for p in range(20)}
         lo_, hi_ = spec.pop_offsets[0], spec.pop_offsets[1]
         x = after[g][lo_:hi_].astype(np.float64)
-        assert x.size > 100_000
+        assert x.size > 1_000_000
         assert abs(x.mean() / (alpha / beta) - 1.0) < 0.01
         assert abs(x.var() / (alpha / beta ** 2) - 1.0) < 0.03
         assert np.array_equal(after[g][hi_:], before[g][hi_:])          # other population untouched
