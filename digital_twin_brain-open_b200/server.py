@@ -13,6 +13,15 @@ id is made absolute as adjust_relative_conn_bid does, src/configuration.cpp:956)
 each (block, population id) pair becomes one population.  Every RPC keeps the
 reference's per-block addressing: neuron ids relative to their block, population
 (``brain_id``) ids as the block's own subblock ids, responses in block order.
+
+``--serve``: many clients share the GPU.  Each client connection (gRPC peer) Inits
+its own network, resident in a pool under an HBM cap (``dtb_server_*``); Run
+requests of all clients go to the pool's online scheduler, which batches the
+requests in flight slice by slice (continuous batching) with the deterministic
+fixed-point push, so each client's counts are the same as its network run alone.
+Served Runs carry the OU background and output_freq / freq_char;
+Updateoubackgroundparam is applied with the client's next Run; the other outputs
+and property updates answer SNN_UNSUPPORTED / success = False in this mode.
 """
 from __future__ import annotations
 
@@ -22,6 +31,8 @@ import glob
 import math
 import os
 import re
+import shutil
+import tempfile
 import threading
 
 import grpc
@@ -97,11 +108,18 @@ class SnnService(pbg.SnnServicer):
     """The ``snn.Snn`` service backed by one engine."""
 
     def __init__(self, syn_mode=E.SYN_PUSH, device_weight=None, seed=0, chunk=1000, stop_event=None,
-                 engine_factory=None):
+                 engine_factory=None, serve=False, hbm_cap_gb=150.0, slice_steps=100):
         """``engine_factory(net, **options)`` builds the engine of an Init (default
         ``engine.Engine.from_arrays``, the CUDA engine); a test can hand in another
-        object with the same methods."""
+        object with the same methods.  ``serve``: one network per client in a pool
+        with continuous batching (module docstring)."""
         self.engine_factory = engine_factory or E.Engine.from_arrays
+        self.serve = serve
+        self.sessions = {}
+        if serve:
+            self.pool = E.Server(hbm_cap_bytes=hbm_cap_gb * 1e9, slice_steps=slice_steps, syn_mode=E.SYN_PUSH_FIXED)
+            self.pool.start(E.SERVE_BATCHED)
+            self.pool_dir = tempfile.mkdtemp(prefix="dtb_pool_")
         self.syn_mode = syn_mode
         self.device_weight = device_weight
         self.seed = seed
@@ -114,8 +132,8 @@ class SnnService(pbg.SnnServicer):
         self.n_samples = 0
 
     # ---- helpers
-    def _global_pops(self, block_id, brain_ids):
-        b = self.blocks[block_id]
+    def _global_pops(self, block_id, brain_ids, blocks=None):
+        b = (self.blocks if blocks is None else blocks)[block_id]
         out, idx = [], []
         for k, sid in enumerate(brain_ids):
             for g in b["by_subblk"].get(int(sid), []):
@@ -128,6 +146,9 @@ class SnnService(pbg.SnnServicer):
         return pb.Version(version=VERSION)
 
     def Init(self, request, context):
+        if self.serve:
+            yield from self._init_served(request, context)
+            return
         with self.lock:
             if not request.file_path:
                 yield pb.InitResponse(status=pb.SNN_INVALID_PARAMETER)
@@ -156,7 +177,80 @@ class SnnService(pbg.SnnServicer):
                                       subblk_info=[pb.SubblockInfo(subblk_id=s, subblk_num=c) for s, c in blk["subblk"]],
                                       total_gpu_mem=float(self.eng.info().device_bytes))
 
+    # ---- serving mode: one network per client connection in the pool
+    def _init_served(self, request, context):
+        with self.lock:
+            if not request.file_path:
+                yield pb.InitResponse(status=pb.SNN_INVALID_PARAMETER)
+                return
+            files = _block_files(request.file_path)
+            if not files:
+                yield pb.InitResponse(status=pb.SNN_INVALID_NETWORK)
+                return
+            net, blocks = merge_blocks(files)
+            if not any(b["subblk"] for b in blocks):
+                yield pb.InitResponse(status=pb.SNN_INVALID_NETWORK)
+                return
+            in_wt = _weight_type(request.file_path, net["weight"].dtype)
+            dev_wt = self.device_weight if self.device_weight is not None else \
+                {E.W_F64: E.W_F32, E.W_F32: E.W_F32, E.W_F16: E.W_F16, E.W_U8: E.W_U8}[in_wt]
+            # the pool rebuilds evicted networks from a file: the merged network, written once
+            k = len(self.sessions)
+            path = os.path.join(self.pool_dir, f"net_{k}.npz")
+            nw_arrays = dict(net, input_block_idx=np.zeros(net["input_neuron_idx"].shape[0], np.int16))
+            np.savez(path, **nw_arrays)
+            P = sum(len(b["subblk"]) for b in blocks)
+            self.pool.stop()                          # networks join the pool between scheduler runs
+            try:
+                nid = self.pool.add_npz(path, P, dt=request.delta_t or 1.0, weight_type=dev_wt, seed=self.seed + k)
+            finally:
+                self.pool.start(E.SERVE_BATCHED)
+            self.sessions[context.peer()] = dict(net=nid, blocks=blocks, P=P, counts=np.concatenate(
+                [[c for _, c in b["subblk"]] for b in blocks]).astype(np.float32),
+                ou=[np.full(P, 0.6, np.float32), np.full(P, 0.2, np.float32), np.full(P, 10.0, np.float32)],
+                ou_dirty=False)
+            for b, blk in enumerate(blocks):
+                yield pb.InitResponse(status=pb.SNN_OK, block_id=b, neurons_per_block=blk["n"],
+                                      subblk_info=[pb.SubblockInfo(subblk_id=s, subblk_num=c) for s, c in blk["subblk"]],
+                                      total_gpu_mem=0.0)
+
+    def _run_served(self, request, context):
+        sess = self.sessions.get(context.peer())
+        status = pb.SNN_OK
+        if sess is None:
+            status = pb.SNN_INVALID_NETWORK
+        elif request.iter <= 0 or (request.t_steps > 1 and not request.use_ou_background):
+            status = pb.SNN_INVALID_PARAMETER
+        elif (request.output_vmean or request.output_sample_spike or request.output_sample_vmemb or
+              request.output_sample_iou or request.output_sample_isynaptic or request.output_imean or
+              request.output_receptor_imeas or request.t_steps > 1 or not request.use_ou_background):
+            status = pb.SNN_UNSUPPORTED
+        if status != pb.SNN_OK:
+            yield pb.RunResponse(status=status)
+            return
+        ou = None
+        if sess["ou_dirty"]:
+            ou, sess["ou_dirty"] = tuple(a.copy() for a in sess["ou"]), False
+        ticket = self.pool.submit(sess["net"], request.iter, ou)
+        r = self.pool.wait(ticket)
+        if r["status"] != E.OK:
+            yield pb.RunResponse(status=pb.SNN_INVALID_PARAMETER)
+            return
+        for k in range(request.iter):
+            resp = pb.RunResponse(status=pb.SNN_OK)
+            if request.output_freq:
+                f = r["freqs"][k]
+                if request.freq_char:
+                    q = (np.float32(255) * f.astype(np.float32)) / sess["counts"]
+                    resp.freq.append(np.array([math.floor(x + 0.5) for x in q], np.uint8).tobytes())
+                else:
+                    resp.freq.append(f.astype(np.int32).tobytes())
+            yield resp
+
     def Run(self, request, context):
+        if self.serve:
+            yield from self._run_served(request, context)
+            return
         # validation of SnnImpl::Run (dist_simulator.cpp:3225-3234)
         samples_wanted = (request.output_sample_spike or request.output_sample_vmemb or request.output_sample_iou
                           or request.output_sample_isynaptic)
@@ -223,6 +317,10 @@ class SnnService(pbg.SnnServicer):
             self.iterations += request.iter
 
     def Updateprop(self, request_iterator, context):
+        if self.serve:                      # not part of the served path
+            for _ in request_iterator:
+                pass
+            return pb.UpdatePropResponse(success=False)
         with self.lock:
             for req in request_iterator:
                 b = self.blocks[req.block_id]
@@ -231,6 +329,10 @@ class SnnService(pbg.SnnServicer):
         return pb.UpdatePropResponse(success=True)
 
     def Updatehyperpara(self, request_iterator, context):
+        if self.serve:                      # not part of the served path
+            for _ in request_iterator:
+                pass
+            return pb.UpdateHyperParaResponse(success=False)
         with self.lock:
             for req in request_iterator:
                 pops, k = self._global_pops(req.block_id, req.brain_id)
@@ -240,6 +342,10 @@ class SnnService(pbg.SnnServicer):
         return pb.UpdateHyperParaResponse(success=True)
 
     def Updategamma(self, request_iterator, context):
+        if self.serve:                      # not part of the served path
+            for _ in request_iterator:
+                pass
+            return pb.UpdateGammaResponse(success=False)
         with self.lock:
             for req in request_iterator:
                 pops, k = self._global_pops(req.block_id, req.brain_id)
@@ -250,6 +356,17 @@ class SnnService(pbg.SnnServicer):
         return pb.UpdateGammaResponse(success=True)
 
     def Updateoubackgroundparam(self, request_iterator, context):
+        if self.serve:
+            # kept with the client's session and applied with its next Run
+            sess = self.sessions.get(context.peer())
+            for req in request_iterator:
+                if sess is None:
+                    continue
+                pops, k = self._global_pops(req.block_id, req.brain_id, sess["blocks"])
+                for arr, vals in zip(sess["ou"], (req.mean, req.deviation, req.correlation_time)):
+                    arr[pops] = np.asarray(vals, np.float32)[k]
+                sess["ou_dirty"] = True
+            return pb.UpdateOUBackgroundParamResponse(success=sess is not None)
         with self.lock:
             for req in request_iterator:
                 pops, k = self._global_pops(req.block_id, req.brain_id)
@@ -259,6 +376,10 @@ class SnnService(pbg.SnnServicer):
         return pb.UpdateOUBackgroundParamResponse(success=True)
 
     def Updatesample(self, request_iterator, context):
+        if self.serve:                      # not part of the served path
+            for _ in request_iterator:
+                pass
+            return pb.UpdateSampleResponse(success=False)
         with self.lock:
             ids = []
             for req in request_iterator:
@@ -292,6 +413,10 @@ class SnnService(pbg.SnnServicer):
         if self.eng is not None:
             self.eng.close()
             self.eng = None
+        if self.serve and self.pool is not None:
+            self.pool.close()
+            self.pool = None
+            shutil.rmtree(self.pool_dir, ignore_errors=True)
 
 
 def start(port=0, host="127.0.0.1", **kw):
@@ -314,9 +439,13 @@ def main():
     ap.add_argument("--host", default="0.0.0.0")
     ap.add_argument("--syn", default="push", choices=["push", "push_exact", "pull"])
     ap.add_argument("--bf16", action="store_true", help="store weights as bf16 pairs on the device")
+    ap.add_argument("--serve", action="store_true",
+                    help="one network per client connection, Runs batched on the GPU (continuous batching)")
+    ap.add_argument("--hbm-cap-gb", type=float, default=150.0, help="HBM cap of the resident networks (--serve)")
     args = ap.parse_args()
     syn = {"push": E.SYN_PUSH, "push_exact": E.SYN_PUSH_EXACT, "pull": E.SYN_PULL}[args.syn]
-    server, port, svc = start(args.port, args.host, syn_mode=syn, device_weight=E.W_BF16 if args.bf16 else None)
+    server, port, svc = start(args.port, args.host, syn_mode=syn, device_weight=E.W_BF16 if args.bf16 else None,
+                              serve=args.serve, hbm_cap_gb=args.hbm_cap_gb)
     print(f"snn.Snn serving on {args.host}:{port}", flush=True)
     svc.stop_event.wait()
     server.stop(grace=2)

@@ -96,3 +96,58 @@ def test_server_matches_direct_engine(gpu, tmp_path):
         assert np.array_equal(got, d2.receptor_imeans[:, c])
     si = np.stack([np.frombuffer(r.sample_isynaptic[0], np.float32) for r in r2])
     assert np.array_equal(si, d2.sample_isyn) and np.abs(si).max() > 0
+
+
+def test_served_clients_share_the_gpu(gpu, tmp_path):
+    """--serve: two client connections each Init their own network into the pool, and
+    their Runs, issued from two threads, advance together on the GPU (continuous
+    batching, fixed-point push).  Each client's counts equal its network run alone,
+    including an Updateoubackgroundparam applied with the second client's Run."""
+    import threading
+    dirs = []
+    for k in range(2):
+        net = nw.make_uniform_block(6000 + 2000 * k, 100, seed=10 + k)
+        net["property"][:, 3] = np.repeat([0, 1], [3000, 3000 + 2000 * k])
+        d = tmp_path / f"client{k}" / "single"
+        d.mkdir(parents=True)
+        nw.write_npz(str(d / "block_0.npz"), net)
+        dirs.append(str(d))
+    server, port, svc = S.start(0, serve=True, slice_steps=50, seed=3)
+    try:
+        chans = [grpc.insecure_channel(f"127.0.0.1:{port}") for _ in range(2)]
+        stubs = [pbg.SnnStub(c) for c in chans]
+        for st, d in zip(stubs, dirs):                   # sessions 0 and 1, in this order
+            init = list(st.Init(pb.InitRequest(file_path=d, delta_t=0.1)))
+            assert init[0].status == pb.SNN_OK and len(init[0].subblk_info) == 2
+        assert stubs[1].Updateoubackgroundparam(iter([pb.UpdateOUBackgroundParamRequest(
+            block_id=0, brain_id=[1], mean=[0.66], deviation=[0.22], correlation_time=[12.0])])).success
+        assert not stubs[0].Updateprop(iter([pb.UpdatePropRequest(block_id=0, neuron_id=[1], prop_id=[5],
+                                                                  prop_val=[-50.0])])).success
+        bad = _run(stubs[0], iter=10, output_freq=True, output_vmean=True, use_ou_background=True)
+        assert bad[0].status == pb.SNN_UNSUPPORTED
+        got = [None, None]
+
+        def client(k):
+            r = _run(stubs[k], iter=600, output_freq=True, use_ou_background=True)
+            got[k] = np.array([np.frombuffer(x.freq[0], np.int32) for x in r])
+
+        threads = [threading.Thread(target=client, args=(k,)) for k in range(2)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        info = svc.pool.info()
+        assert info["n_nets"] == 2 and info["batch_members_sum"] > info["slices"]   # the Runs shared slices
+        for k, d in enumerate(dirs):
+            net, _ = S.merge_blocks(S._block_files(d))
+            with E.Engine.from_arrays(net, seed=3 + k) as eng:
+                if k == 1:
+                    eng.set_ou(eng.pop_ids, np.float32([0.6, 0.66]), np.float32([0.2, 0.22]), np.float32([10.0, 12.0]))
+                ref = eng.run(600, syn_mode=E.SYN_PUSH_FIXED).freqs
+            assert ref.sum() > 0
+            assert np.array_equal(got[k], ref), f"client {k}"
+        for c in chans:
+            c.close()
+    finally:
+        server.stop(grace=1)
+        svc.close()
