@@ -106,8 +106,8 @@ def test_served_clients_share_the_gpu(gpu, tmp_path):
     import threading
     dirs = []
     for k in range(2):
-        net = nw.make_uniform_block(6000 + 2000 * k, 100, seed=10 + k)
-        net["property"][:, 3] = np.repeat([0, 1], [3000, 3000 + 2000 * k])
+        net = nw.make_uniform_block(20000 + 4000 * k, 100, seed=10 + k)
+        net["property"][:, 3] = np.repeat([0, 1], [10000, 10000 + 4000 * k])
         d = tmp_path / f"client{k}" / "single"
         d.mkdir(parents=True)
         nw.write_npz(str(d / "block_0.npz"), net)
@@ -128,7 +128,7 @@ def test_served_clients_share_the_gpu(gpu, tmp_path):
         got = [None, None]
 
         def client(k):
-            r = _run(stubs[k], iter=600, output_freq=True, use_ou_background=True)
+            r = _run(stubs[k], iter=4000, output_freq=True, use_ou_background=True)   # ~50 ms: the Runs overlap
             got[k] = np.array([np.frombuffer(x.freq[0], np.int32) for x in r])
 
         threads = [threading.Thread(target=client, args=(k,)) for k in range(2)]
@@ -143,7 +143,7 @@ def test_served_clients_share_the_gpu(gpu, tmp_path):
             with E.Engine.from_arrays(net, seed=3 + k) as eng:
                 if k == 1:
                     eng.set_ou(eng.pop_ids, np.float32([0.6, 0.66]), np.float32([0.2, 0.22]), np.float32([10.0, 12.0]))
-                ref = eng.run(600, syn_mode=E.SYN_PUSH_FIXED).freqs
+                ref = eng.run(4000, syn_mode=E.SYN_PUSH_FIXED).freqs
             assert ref.sum() > 0
             assert np.array_equal(got[k], ref), f"client {k}"
         for c in chans:
