@@ -24,6 +24,13 @@ namespace dtb {
 
 constexpr int kLifThreads = 256;
 constexpr int kLifTile = 1024;          // neurons per LIF CTA: 256 threads x 4 neurons
+// Depth of the LIF kernel's bulk-copy ring (tiles in flight = stages - 1) and the CTAs
+// that fit on an SM with it (28 KiB of shared memory per stage).
+#ifndef DTB_LIF_STAGES
+#define DTB_LIF_STAGES 2
+#endif
+constexpr int kLifStages = DTB_LIF_STAGES;
+constexpr int kLifCtasPerSm = kLifStages <= 2 ? 3 : (kLifStages == 3 ? 2 : 1);
 constexpr int kPullThreads = 256;
 constexpr int kPullTile = 256;          // neurons per pull CTA: 8 warps x 32 neurons
 constexpr int kPad = 1024;              // every per-neuron array is padded to a multiple of this

@@ -192,7 +192,7 @@ public:
     uint32_t* list_count = nullptr;
     uint32_t* list_ticket = nullptr;
     uint32_t* tile_pop = nullptr;
-    uint32_t lif_ctas_per_sm = 3;
+    uint32_t lif_ctas_per_sm = kLifCtasPerSm;
     // population-local push tables (built when every out-degree row is sorted)
     uint2* own_seg = nullptr;
     uint32_t* woff = nullptr;

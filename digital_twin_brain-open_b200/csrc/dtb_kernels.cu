@@ -253,7 +253,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // host turns it into DTB_DEVICE_FAULT) after one more bounded wait.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kLifStageFloats = 3 * kLifTile + 4 * kLifTile;   // V | i_ou | t_last | J (float4)
-constexpr size_t kLifSmem = 2ull * kLifStageFloats * sizeof(float);
+constexpr size_t kLifSmem = static_cast<size_t>(kLifStages) * kLifStageFloats * sizeof(float);
 
 __device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, uint32_t bytes) {
     uint64_t g;
@@ -308,12 +308,12 @@ __device__ __forceinline__ uint32_t lif_next_tile(uint32_t gt, uint32_t chunk, u
 }
 
 template <int JM>
-__global__ void __launch_bounds__(kLifThreads, 3)
+__global__ void __launch_bounds__(kLifThreads, kLifCtasPerSm)
 lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_prefix,
            const uint32_t* __restrict__ vbase, uint32_t n_nets, uint32_t total_tiles, SpikeList sl, uint32_t flags,
            int prop_mode, const uint32_t* __restrict__ tile_net, uint32_t chunk) {
     extern __shared__ __align__(128) float lsm[];
-    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ __align__(8) uint64_t s_bar[kLifStages];
     __shared__ int s_cnt[kStatSlots];
     __shared__ long long s_vs[kStatSlots];
 
@@ -340,18 +340,23 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
     uint32_t n_tk = 0;                 // thread 0's count of table entries
     if (tid < kStatSlots) { s_cnt[tid] = 0; s_vs[tid] = 0; }
     if (tid == 0) {
-        mbar_init(&s_bar[0], 1);
-        mbar_init(&s_bar[1], 1);
+        for (int s = 0; s < kLifStages; ++s) mbar_init(&s_bar[s], 1);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (blockIdx.x * chunk < total_tiles)
-            lif_prefetch(nets, tile_prefix, tile_net, n_nets, blockIdx.x * chunk, lsm, &s_bar[0]);
+    }
+    // thread 0: the next tile to prefetch; the first kLifStages - 1 tiles go in now
+    uint32_t pre = blockIdx.x * chunk;
+    if (tid == 0) {
+        for (int s = 0; s + 1 < kLifStages && pre < total_tiles; ++s) {
+            lif_prefetch(nets, tile_prefix, tile_net, n_nets, pre, lsm + s * kLifStageFloats, &s_bar[s]);
+            pre = lif_next_tile(pre, chunk, total_tiles);
+        }
     }
     __syncthreads();
 
     uint32_t it = 0;
     for (uint32_t gt = blockIdx.x * chunk; gt < total_tiles; gt = lif_next_tile(gt, chunk, total_tiles), ++it) {
         const uint32_t net = tile_to_net(tile_net, tile_prefix, n_nets, gt);
-        const uint32_t stg = it & 1u;
+        const uint32_t stg = it % kLifStages;
         if (net != cur_net) {
             // hand in the previous network's tiles (views are read through the
             // read-only cache, so switching needs no barrier)
@@ -369,12 +374,13 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
             done_here = 0;
             cur_net = net;
         }
-        // barrier A: the other stage's readers (previous tile) are done and its
-        // store has been issued; refill it with the tile after this one
-        const uint32_t gn = lif_next_tile(gt, chunk, total_tiles);
-        if (tid == 0 && gn < total_tiles) {
+        // barrier A: the previous tile's readers are done and its store has been
+        // issued; refill its stage with the tile kLifStages - 1 ahead of this one
+        if (tid == 0 && pre < total_tiles) {
+            const uint32_t sn = (it + kLifStages - 1) % kLifStages;
             bulk_wait_read();
-            lif_prefetch(nets, tile_prefix, tile_net, n_nets, gn, lsm + (stg ^ 1u) * kLifStageFloats, &s_bar[stg ^ 1u]);
+            lif_prefetch(nets, tile_prefix, tile_net, n_nets, pre, lsm + sn * kLifStageFloats, &s_bar[sn]);
+            pre = lif_next_tile(pre, chunk, total_tiles);
         }
         __syncthreads();
         const NetView& nv = nets[net];
@@ -409,9 +415,10 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
 #pragma unroll
             for (int k = 0; k < 4; ++k) old_w[k] = bits[word0 + (kSlotsPerTile / 32) * k];
         }
-        if (!mbar_wait_bounded(&s_bar[stg], (it >> 1) & 1u)) {
+        const uint32_t phase = (it / kLifStages) & 1u;
+        if (!mbar_wait_bounded(&s_bar[stg], phase)) {
             late = 1;
-            mbar_wait_bounded(&s_bar[stg], (it >> 1) & 1u);
+            mbar_wait_bounded(&s_bar[stg], phase);
         }
         if (late) err |= kErrTimeout;
         // stage accesses: each step of k reads and writes 32 consecutive neurons
