@@ -348,7 +348,8 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if wt == E.W_F32 else "bf16-weights/f32-state",
-            "data": "synthetic (seeded regional network generated on the device)",
+            "data": ("synthetic (seeded uniform block built on the host)" if args.net == "uniform"
+                     else "synthetic (seeded regional network generated on the device)"),
             "sim_ms_per_wall_s": args.steps * WINDOW * 0.1 / (ms / 1e3),
             "config": {"workload": f"{info.n_neurons}-neuron {args.net} LIF network, {P} populations, "
                                    f"in-degree {args.degree}, {args.weights} weights, OU background, "

@@ -1025,6 +1025,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
             return DTB_OK;
         };
         DTB_CU(cudaEventRecord(ev0, stream));
+        bool eager_graphable = false;
         // a push chunk with no tuning pending and no per-kernel timing: replay its graph once its
         // shape has been seen before (the kernels read every per-run value from device memory)
         const bool graphable = use_graph && !pull && !time_k && !(tune_at >= done && tune_at < done + rows);
@@ -1037,7 +1038,8 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
             // launches of the replayed chunk, counted as the eager path does
             chunk_launches = rows * (ts + 1u + push_extra_launches(b, acc, push_cfg) + (isyn_any ? 1u : 0u)) +
                              (last_chunk && acc != ACC_FLOAT ? 1u : 0u);
-        } else if (graphable && std::memcmp(key, seen_key, sizeof(key)) == 0 && ++seen_count >= 2) {
+        } else if (graphable && std::memcmp(key, seen_key, sizeof(key)) == 0 && ++seen_count >= 2 &&
+                   seen_ms_per_step < kGraphMaxMsPerStep) {
             if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
             cudaGraph_t g = nullptr;
             DTB_CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
@@ -1056,6 +1058,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
                 std::memcpy(seen_key, key, sizeof(key));
                 seen_count = 0;
             }
+            eager_graphable = graphable;
             DTB_TRY(issue(true));
         }
         launches += chunk_launches;
@@ -1064,6 +1067,7 @@ int Engine::run(const dtb_run_request& rq, dtb_run_output& out) {
         float ms = 0.f;
         DTB_CU(cudaEventElapsedTime(&ms, ev0, ev1));
         ms_total += ms;
+        if (eager_graphable) seen_ms_per_step = ms / static_cast<float>(rows);
         for (const auto& tp : timed) {
             float km = 0.f;
             DTB_CU(cudaEventElapsedTime(&km, tev[2 * tp.second], tev[2 * tp.second + 1]));

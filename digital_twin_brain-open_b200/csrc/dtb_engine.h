@@ -213,14 +213,18 @@ public:
     int tune_push(const LaunchBatch& b, int acc);
     // Window graphs of the plain path: a chunk of push-mode steps is launched eagerly
     // the first two times its shape is seen in a row, captured into a CUDA graph the
-    // third time and replayed from then on (one graph kept per engine).  Capturing a
-    // 500-step window costs about as much as 20 eager steps of the 5M network, so a
-    // shape that does not repeat is never captured.
+    // third time and replayed from then on (one graph kept per engine) -- but only when
+    // the eager chunk was launch-bound, under kGraphMaxMsPerStep of device time per
+    // step.  Replay saves a few microseconds of launch work per step; capturing a
+    // 500-step window costs about 70 ms, as much as 100 steps of the 5M-neuron network,
+    // where replay gains about 1 %, so such networks stay eager.
+    static constexpr float kGraphMaxMsPerStep = 0.2f;
     bool use_graph = true;
     cudaGraphExec_t graph = nullptr;
     uint64_t graph_key[10] = {};
     uint64_t seen_key[10] = {};
     uint32_t seen_count = 0;
+    float seen_ms_per_step = 0.0f;        // device time per step of the last eager chunk of seen_key
     uint32_t graph_launches = 0;
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     NetView view{};

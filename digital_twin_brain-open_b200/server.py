@@ -22,6 +22,10 @@ fixed-point push, so each client's counts are the same as its network run alone.
 Served Runs carry the OU background and output_freq / freq_char;
 Updateoubackgroundparam is applied with the client's next Run; the other outputs
 and property updates answer SNN_UNSUPPORTED / success = False in this mode.
+A session is keyed by the connection's peer address: gRPC Python channels of one
+process to the same target share one connection unless they are created with the
+channel option ``grpc.use_local_subchannel_pool``, so two clients in one process
+need that option (or separate processes) to hold separate networks.
 """
 from __future__ import annotations
 

@@ -114,11 +114,14 @@ def test_served_clients_share_the_gpu(gpu, tmp_path):
         dirs.append(str(d))
     server, port, svc = S.start(0, serve=True, slice_steps=50, seed=3)
     try:
-        chans = [grpc.insecure_channel(f"127.0.0.1:{port}") for _ in range(2)]
+        # two channels of one process share a connection (one peer) unless each keeps its own subchannels
+        chans = [grpc.insecure_channel(f"127.0.0.1:{port}", options=[("grpc.use_local_subchannel_pool", 1)])
+                 for _ in range(2)]
         stubs = [pbg.SnnStub(c) for c in chans]
         for st, d in zip(stubs, dirs):                   # sessions 0 and 1, in this order
             init = list(st.Init(pb.InitRequest(file_path=d, delta_t=0.1)))
             assert init[0].status == pb.SNN_OK and len(init[0].subblk_info) == 2
+        assert len(svc.sessions) == 2                    # one session per connection
         assert stubs[1].Updateoubackgroundparam(iter([pb.UpdateOUBackgroundParamRequest(
             block_id=0, brain_id=[1], mean=[0.66], deviation=[0.22], correlation_time=[12.0])])).success
         assert not stubs[0].Updateprop(iter([pb.UpdatePropRequest(block_id=0, neuron_id=[1], prop_id=[5],
