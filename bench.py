@@ -93,6 +93,10 @@ def parse():
     p.add_argument("--batched-syn", default="fixed", choices=["fixed", "push"],
                    help="synaptic mode of the batched / served side of the ensemble and serve forms: the "
                         "deterministic fixed-point push (a member equals its solo run) or the float push")
+    p.add_argument("--profile-steps", type=int, default=0,
+                   help="profiling run: after the warm-up windows, K single-step runs; prints their events and "
+                        "spikes per step (no bench line), so an ncu capture of those steps' push launches "
+                        "(launches 2 x warm-up steps + 1 .. of a forced local push) can be normalised per event")
     return p.parse_args()
 
 
@@ -268,6 +272,19 @@ def run_ours(args):
 
     for _ in range(args.warmup):
         eng.run(WINDOW, freq=True, out=(fr, None), syn_mode=syn)
+
+    if args.profile_steps:
+        steps = []
+        for _ in range(args.profile_steps):
+            r = eng.run(1, freq=True, out=(fr[:1], None), syn_mode=syn)
+            steps.append({"events": int(r.events), "spikes": int(fr[0].sum()), "launches": int(r.launches)})
+        torch.cuda.synchronize()
+        info = eng.info()
+        print(json.dumps({"profile_steps": steps, "warm_steps": args.warmup * WINDOW, "neurons": info.n_neurons,
+                          "push_variant": f"{PUSH_KINDS[info.push_kind]}:{info.push_param}",
+                          "local_windows": info.local_windows, "weights": args.weights}), flush=True)
+        eng.close()
+        return None
 
     uuid = str(getattr(torch.cuda.get_device_properties(dev), "uuid", ""))
     sampler = ClockSampler(uuid)

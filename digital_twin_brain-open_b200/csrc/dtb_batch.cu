@@ -105,9 +105,11 @@ int Batch::set_members(Engine* const* engines, uint32_t n) {
     if (windows > cap_windows) {
         if (local_scratch) cudaFree(local_scratch);
         local_scratch = nullptr;
-        DTB_CU(cudaMalloc(reinterpret_cast<void**>(&local_scratch), sizeof(uint32_t) * (2ull * windows + 2)));
+        DTB_CU(cudaMalloc(reinterpret_cast<void**>(&local_scratch), sizeof(uint32_t) * (2ull * windows + 3)));
         cap_windows = windows;
     }
+    // the prep kernel's block ticket sits after this membership's tables: start it at zero
+    if (local_scratch) DTB_CU(cudaMemsetAsync(local_scratch, 0, sizeof(uint32_t) * (2ull * cap_windows + 3), stream));
     if (!list_count) {
         DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_count), sizeof(uint32_t)));
         DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_ticket), sizeof(uint32_t)));

@@ -361,7 +361,7 @@ int Engine::build_local_tables() {
     DTB_TRY(dalloc(woff, rb, false));
     DTB_TRY(dalloc(pop_loc, P, false));
     DTB_TRY(dalloc(win_tab, wins.size(), false));
-    DTB_TRY(dalloc(local_scratch, 2 * wins.size() + 2));
+    DTB_TRY(dalloc(local_scratch, 2 * wins.size() + 3));
     DTB_CU(cudaMemcpyAsync(pop_loc, loc.data(), sizeof(uint4) * P, cudaMemcpyHostToDevice, stream));
     DTB_CU(cudaMemcpyAsync(win_tab, wins.data(), sizeof(uint4) * wins.size(), cudaMemcpyHostToDevice, stream));
     DTB_CU(build_local_offsets(out_ptr, out_col, out_w, static_cast<int>(wtype), pop_off_dev, P, n, pop_loc, nullptr,

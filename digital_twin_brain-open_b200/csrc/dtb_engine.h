@@ -199,7 +199,7 @@ public:
     uint4* pop_loc = nullptr;
     uint4* win_tab = nullptr;
     uint32_t n_windows = 0;
-    uint32_t* local_scratch = nullptr;   // [2 * n_windows + 2] per-step unit bookkeeping
+    uint32_t* local_scratch = nullptr;   // [2 * n_windows + 3] per-step unit bookkeeping (zeroed)
     int build_local_tables();
 
     // push kernel variant (autotuned on the first active run)

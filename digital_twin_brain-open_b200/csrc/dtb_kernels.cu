@@ -740,8 +740,9 @@ push_kernel_cross64(const NetView* __restrict__ nets, const uint32_t* __restrict
 // woff boundaries.  The work of a step is split into units of up to
 // kLocalUnitRows spiking rows of one window's population:
 //
-//   local_count_kernel   spiking rows of each window's population (bitmap popcount)
-//   local_scan_kernel    units per window -> exclusive prefix; resets the unit counter
+//   local_prep_kernel    spiking rows of each window's population (bitmap popcount);
+//                        its last block turns them into the units' exclusive prefix
+//                        and resets the unit counter
 //   push_local_kernel    persistent, one 1024-thread CTA per SM: takes units from an
 //                        atomic counter, finds the unit's rows by a block-wide prefix
 //                        over the population's bitmap, sums their window spans into
@@ -839,11 +840,15 @@ __device__ __forceinline__ void load_window(const NetView* __restrict__ nets, co
 }
 
 // scratch: [windows] spiking rows of each window's population, [windows + 1]
-// unit prefix, [1] unit counter.
+// unit prefix, [1] unit counter, [1] block ticket.  One block per window counts
+// its population's spiking rows; the last block to finish (ticket) turns the
+// counts into the unit prefix and resets the counter, so the window kernel that
+// follows needs one launch before it instead of a count and a scan.
 __global__ void __launch_bounds__(256)
-local_count_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ win_prefix, uint32_t n_nets,
-                   uint32_t* scratch) {
+local_prep_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ win_prefix, uint32_t n_nets,
+                  uint32_t windows, uint32_t* scratch) {
     __shared__ uint32_t s_warp[33];
+    __shared__ uint32_t s_last;
     LocalWindow W;
     load_window(nets, win_prefix, n_nets, blockIdx.x, W);
     const uint32_t* bits = (W.nv->clock->n & 1ull) ? W.nv->bits1 : W.nv->bits0;
@@ -852,25 +857,29 @@ local_count_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict_
         c += __popc(pop_word(bits, wi, W.p_lo, W.p_hi));
     uint32_t total;
     block_exclusive_scan(c, s_warp, &total);
-    if (threadIdx.x == 0) scratch[blockIdx.x] = total;
-}
-
-__global__ void __launch_bounds__(1024)
-local_scan_kernel(uint32_t* scratch, uint32_t windows) {
-    __shared__ uint32_t s_warp[33];
+    uint32_t* ticket = scratch + 2 * windows + 2;
+    if (threadIdx.x == 0) {
+        scratch[blockIdx.x] = total;
+        __threadfence();
+        s_last = atomicAdd(ticket, 1u) == windows - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
     uint32_t* upre = scratch + windows;
     uint32_t carry = 0;
     for (uint32_t base = 0; base < windows; base += blockDim.x) {
         const uint32_t i = base + threadIdx.x;
-        const uint32_t u = i < windows ? (scratch[i] + kLocalUnitRows - 1) / kLocalUnitRows : 0u;
-        uint32_t total;
-        const uint32_t ex = block_exclusive_scan(u, s_warp, &total);
+        const uint32_t u = i < windows ? (__ldcg(scratch + i) + kLocalUnitRows - 1) / kLocalUnitRows : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_exclusive_scan(u, s_warp, &tot);
         if (i < windows) upre[i] = carry + ex;
-        carry += total;
+        carry += tot;
     }
     if (threadIdx.x == 0) {
         upre[windows] = carry;
         upre[windows + 1] = 0u;      // the unit counter
+        *ticket = 0u;
     }
 }
 
@@ -1615,8 +1624,7 @@ static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint
             push_kernel<ACC, WT, 8, 32, 1><<<b.sm_count, kPushThreads, 0, b.aux>>>(b.nets, b.vbase, b.n_nets, b.spikes);
         e = cudaEventRecord(b.ev_join, b.aux);
         if (e != cudaSuccess) return e;
-        local_count_kernel<<<b.windows_total, 256, 0, s>>>(b.nets, b.win_prefix, b.n_nets, b.local_scratch);
-        local_scan_kernel<<<1, 1024, 0, s>>>(b.local_scratch, b.windows_total);
+        local_prep_kernel<<<b.windows_total, 256, 0, s>>>(b.nets, b.win_prefix, b.n_nets, b.windows_total, b.local_scratch);
         if (two)
             push_local_kernel<WT, kLocalThreadsShared2, 32, FIX><<<b.sm_count, kLocalThreadsShared2, kLocalSmem, s>>>(
                 b.nets, b.win_prefix, b.n_nets, b.windows_total, b.local_scratch);
@@ -1637,8 +1645,7 @@ static cudaError_t push_launch_wt(const LaunchBatch& b, const PushCfg& cfg, uint
         else
             push_kernel<ACC, WT, 8, 32, 1><<<grid, block, 0, s>>>(b.nets, b.vbase, b.n_nets, b.spikes);
         if (b.windows_total) {
-            local_count_kernel<<<b.windows_total, 256, 0, s>>>(b.nets, b.win_prefix, b.n_nets, b.local_scratch);
-            local_scan_kernel<<<1, 1024, 0, s>>>(b.local_scratch, b.windows_total);
+            local_prep_kernel<<<b.windows_total, 256, 0, s>>>(b.nets, b.win_prefix, b.n_nets, b.windows_total, b.local_scratch);
             push_local_kernel<WT, kLocalThreads, 32, FIX><<<b.sm_count, kLocalThreads, kLocalSmem, s>>>(
                 b.nets, b.win_prefix, b.n_nets, b.windows_total, b.local_scratch);
         }

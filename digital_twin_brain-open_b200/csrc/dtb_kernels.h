@@ -23,7 +23,7 @@ struct LaunchBatch {
     uint32_t lif_chunk;           // consecutive tiles a LIF CTA steps before striding (0 or 1: one)
     const uint32_t* win_prefix;   // device [n_nets + 1] cumulative local-push windows
     uint32_t windows_total;
-    uint32_t* local_scratch;      // device [2 * windows_total + 2]: rows per window, unit prefix, unit counter
+    uint32_t* local_scratch;      // device [2 * windows_total + 3]: rows per window, unit prefix, unit counter, ticket
     uint32_t sm_count;
     cudaStream_t aux;             // second stream of the concurrent local push (fork/join by events)
     cudaEvent_t ev_fork, ev_join;
@@ -53,9 +53,9 @@ extern const PushCfg kPushCands[kPushCandidates];
 cudaError_t push_prepare(int acc, int weight_type, const PushCfg& cfg, int sm_count, uint32_t* ctas);
 cudaError_t launch_push(const LaunchBatch& b, int acc, int weight_type, const PushCfg& cfg, uint32_t ctas,
                         cudaStream_t s);
-// Kernels launch_push issues beyond the first (the local variant's count, scan and window passes).
+// Kernels launch_push issues beyond the first (the local variant's prep and window passes).
 inline uint32_t push_extra_launches(const LaunchBatch& b, int acc, const PushCfg& cfg) {
-    return (cfg.kind == PUSH_LOCAL && acc != ACC_EXACT && b.windows_total) ? 3u : 0u;   // concurrent form: same count
+    return (cfg.kind == PUSH_LOCAL && acc != ACC_EXACT && b.windows_total) ? 2u : 0u;   // concurrent form: same count
 }
 cudaError_t launch_pull(const LaunchBatch& b, int gather, int weight_type, uint32_t flags, int prop_mode, cudaStream_t s);
 cudaError_t launch_fold_finish(const LaunchBatch& b, int acc, cudaStream_t s);
