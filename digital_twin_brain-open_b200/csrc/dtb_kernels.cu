@@ -32,11 +32,30 @@ constexpr int kTmaWarps = 4;
 constexpr uint32_t kWaitLimit = 1u << 22;   // mbarrier polls before a wait is declared failed
 
 // Fire-and-forget reductions (no returned value, so no scoreboard wait).
-__device__ __forceinline__ void red_add_f32x2(float2* addr, float2 v) {
-    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" :: "l"(addr), "f"(v.x), "f"(v.y) : "memory");
-}
 __device__ __forceinline__ void red_add_u64(unsigned long long* addr, unsigned long long v) {
     asm volatile("red.global.add.u64 [%0], %1;" :: "l"(addr), "l"(v) : "memory");
+}
+
+// The accumulators (J, or dJf in fixed-point mode: 80 MB at 5M neurons) are
+// reduced into with an L2 evict_last policy, so the CSR stream of the push
+// (gigabytes in a burst step, loaded evict_first by ld.global.cs) does not push
+// them out of L2.  Without it the scattered reductions of the cross-population
+// push missed L2 and wrote about 15 bytes of DRAM back per event.
+__device__ __forceinline__ unsigned long long l2_policy_keep() {
+    unsigned long long p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ void red_add_f32x2_keep(float2* addr, float2 v, unsigned long long pol) {
+    asm volatile("red.global.add.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" :: "l"(addr), "f"(v.x), "f"(v.y), "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ void red_add_f32x4_keep(float4* addr, float4 v, unsigned long long pol) {
+    asm volatile("red.global.add.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;"
+                 :: "l"(addr), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void red_add_u64_keep(unsigned long long* addr, unsigned long long v, unsigned long long pol) {
+    asm volatile("red.global.add.L2::cache_hint.u64 [%0], %1, %2;" :: "l"(addr), "l"(v), "l"(pol) : "memory");
 }
 
 __device__ inline uint32_t find_net(const uint32_t* __restrict__ prefix, uint32_t n_nets, uint32_t x) {
@@ -646,6 +665,7 @@ __device__ __forceinline__ void push_rows(const NetView* __restrict__ nets, cons
     unsigned long long* dJf = nets[0].dJf;
     float fscale = nets[0].fix_scale;
     const uint2* own = LOCAL ? nets[0].own_seg : nullptr;
+    const unsigned long long keep = l2_policy_keep();
     uint32_t vb = 0;
     for (uint32_t r = gw; r < count; r += nw) {
         const uint32_t v = __ldg(sl.list + r);
@@ -692,9 +712,9 @@ __device__ __forceinline__ void push_rows(const NetView* __restrict__ nets, cons
                     const uint32_t target = c[q] & kIndexMask;
                     const uint32_t kind = c[q] >> 31;
                     if constexpr (ACC == ACC_FLOAT) {
-                        red_add_f32x2(reinterpret_cast<float2*>(J + target) + kind, w[q]);
+                        red_add_f32x2_keep(reinterpret_cast<float2*>(J + target) + kind, w[q], keep);
                     } else if constexpr (ACC == ACC_FIXED) {
-                        red_add_u64(dJf + 2ull * target + kind, pack_fixed(w[q], fscale));
+                        red_add_u64_keep(dJf + 2ull * target + kind, pack_fixed(w[q], fscale), keep);
                     } else {
                         unsigned long long* d = reinterpret_cast<unsigned long long*>(dJ) + static_cast<size_t>(target) * 4 + 2 * kind;
                         red_add_u64(d, static_cast<unsigned long long>(float_to_fix(w[q].x)));
@@ -770,10 +790,6 @@ constexpr size_t kLocalSmem = 4ull * kLocalWin * sizeof(int) + kLocalUnitRows * 
 
 __device__ __forceinline__ void red_add_shared_u32(const void* p, uint32_t v) {
     asm volatile("red.shared.add.u32 [%0], %1;" :: "r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))), "r"(v) : "memory");
-}
-__device__ __forceinline__ void red_add_f32x4(float4* addr, float4 v) {
-    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" :: "l"(addr), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
-                 : "memory");
 }
 
 // Spiking-row bitmap word wi of the population [p_lo, p_hi), bits outside masked off.
@@ -893,17 +909,19 @@ __device__ __forceinline__ void local_flush(const LocalWindow& W, int* acc) {
     float4* J = W.nv->J + W.lo;
     unsigned long long* dJf = FIX ? W.nv->dJf + 2ull * W.lo : nullptr;
     const uint32_t width = W.hi - W.lo;
+    const unsigned long long keep = l2_policy_keep();
     for (uint32_t i = threadIdx.x; i < width; i += blockDim.x) {
         const int4 v = make_int4(acc[i], acc[kLocalWin + i], acc[2 * kLocalWin + i], acc[3 * kLocalWin + i]);
         if (v.x | v.y | v.z | v.w) {
             if constexpr (FIX) {
                 const unsigned long long u0 = static_cast<uint32_t>(v.x), u1 = static_cast<uint32_t>(v.y);
                 const unsigned long long u2 = static_cast<uint32_t>(v.z), u3 = static_cast<uint32_t>(v.w);
-                if (u0 | u1) red_add_u64(dJf + 2ull * i, (u1 << 32) | u0);
-                if (u2 | u3) red_add_u64(dJf + 2ull * i + 1, (u3 << 32) | u2);
+                if (u0 | u1) red_add_u64_keep(dJf + 2ull * i, (u1 << 32) | u0, keep);
+                if (u2 | u3) red_add_u64_keep(dJf + 2ull * i + 1, (u3 << 32) | u2, keep);
             } else {
-                red_add_f32x4(J + i, make_float4(__fmul_rn(__int2float_rn(v.x), W.unscale), __fmul_rn(__int2float_rn(v.y), W.unscale),
-                                                 __fmul_rn(__int2float_rn(v.z), W.unscale), __fmul_rn(__int2float_rn(v.w), W.unscale)));
+                red_add_f32x4_keep(J + i, make_float4(__fmul_rn(__int2float_rn(v.x), W.unscale), __fmul_rn(__int2float_rn(v.y), W.unscale),
+                                                 __fmul_rn(__int2float_rn(v.z), W.unscale), __fmul_rn(__int2float_rn(v.w), W.unscale)),
+                                   keep);
             }
             acc[i] = 0;
             acc[kLocalWin + i] = 0;
@@ -1141,6 +1159,7 @@ push_tma_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ v
     __syncwarp();
     const uint32_t count = *sl.count;
     const uint32_t nw = gridDim.x * kTmaWarps;
+    const unsigned long long keep = l2_policy_keep();
     // producer cursor (lane-uniform): list index, remaining range of the row, its network
     uint32_t pr = blockIdx.x * kTmaWarps + warp;
     unsigned long long pc = 0, pe = 0;
@@ -1209,9 +1228,9 @@ push_tma_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ v
             const float2 w = smem_weight<WT>(sw, ow + e);
             const uint32_t target = c & kIndexMask, kind = c >> 31;
             if constexpr (ACC == ACC_FLOAT) {
-                red_add_f32x2(reinterpret_cast<float2*>(J + target) + kind, w);
+                red_add_f32x2_keep(reinterpret_cast<float2*>(J + target) + kind, w, keep);
             } else if constexpr (ACC == ACC_FIXED) {
-                red_add_u64(dJf + 2ull * target + kind, pack_fixed(w, fscale));
+                red_add_u64_keep(dJf + 2ull * target + kind, pack_fixed(w, fscale), keep);
             } else {
                 unsigned long long* d = reinterpret_cast<unsigned long long*>(dJ) + static_cast<size_t>(target) * 4 + 2 * kind;
                 red_add_u64(d, static_cast<unsigned long long>(float_to_fix(w.x)));
