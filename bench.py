@@ -54,11 +54,11 @@ CSR_COL_BYTES = 4
 ACC_BYTES = 8             # one logical accumulator update (a float pair) per event
 ROW_BYTES = 12            # rowptr pair + spike-list entry per spiking row
 PUSH_KINDS = ["reg", "tma", "local"]
-# DRAM bytes per delivered synaptic event of the concurrent population-local push (local:2008)
+# DRAM bytes per delivered synaptic event of the population-local push (measured on local:2008)
 # with FP32 weights on the 5M-neuron network: ncu's dram__bytes_read + dram__bytes_write of both
 # push kernels over 50 consecutive steps (one burst cycle, 5.0e9 events), caches flushed before
 # each launch (profiles/push_traffic_5m_50steps.md)
-LOCAL_PUSH_DRAM_BYTES_PER_EVENT_F32 = 18.4
+LOCAL_PUSH_DRAM_BYTES_PER_EVENT_F32 = 14.94
 PUSH_KERNELS = ["push_kernel", "push_tma_kernel", "push_kernel (cross-population) + push_local_kernel (windows)"]
 
 

@@ -446,10 +446,11 @@ def main():
     ap.add_argument("--serve", action="store_true",
                     help="one network per client connection, Runs batched on the GPU (continuous batching)")
     ap.add_argument("--hbm-cap-gb", type=float, default=150.0, help="HBM cap of the resident networks (--serve)")
+    ap.add_argument("--slice-steps", type=int, default=100, help="steps per continuous-batching slice (--serve)")
     args = ap.parse_args()
     syn = {"push": E.SYN_PUSH, "push_exact": E.SYN_PUSH_EXACT, "pull": E.SYN_PULL}[args.syn]
     server, port, svc = start(args.port, args.host, syn_mode=syn, device_weight=E.W_BF16 if args.bf16 else None,
-                              serve=args.serve, hbm_cap_gb=args.hbm_cap_gb)
+                              serve=args.serve, hbm_cap_gb=args.hbm_cap_gb, slice_steps=args.slice_steps)
     print(f"snn.Snn serving on {args.host}:{port}", flush=True)
     svc.stop_event.wait()
     server.stop(grace=2)

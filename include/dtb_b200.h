@@ -240,10 +240,12 @@ int32_t dtb_info(void* engine, dtb_engine_info* info);
  * up (keeping the best so far, or kind 0 param 8) after 400 reads of quiet steps. */
 int32_t dtb_set_push_variant(void* engine, int32_t kind, int32_t param);
 /* Window graphs of dtb_run (no reference counterpart): with enable != 0 (the
- * default) a chunk of push-mode steps is launched kernel by kernel the first time
- * its shape (steps, flags, modes, push variant) is seen, captured into a CUDA
- * graph the second time and replayed from then on; results are the same bits
- * either way.  enable = 0 launches every chunk kernel by kernel. */
+ * default) a chunk of push-mode steps is launched kernel by kernel the first two
+ * times its shape (steps, flags, modes, push variant) is seen in a row, captured
+ * into a CUDA graph the third time and replayed from then on -- when the eager
+ * chunk took under 0.2 ms of device time per step (launch-bound networks; larger
+ * ones stay eager, where a capture would cost more than replay saves).  Results
+ * are the same bits either way.  enable = 0 launches every chunk kernel by kernel. */
 int32_t dtb_set_graph(void* engine, int32_t enable);
 /* The autotuner's last measurement: on entry *n is the capacity of the arrays,
  * on return the number of variants timed (kind, param, push time in ms). */
