@@ -13,7 +13,7 @@ Contract (one JSON line on rank 0):
   back every step's spike counts and mean potentials;
 * roofline = the push kernel (the dominant kernel) against the measured HBM copy
   bandwidth; cpu_baseline = the C port of the reference CPU model on the bounded
-  CPU sample (20 x 75 simulated steps of a 50,000-neuron network of the same
+  CPU sample (20 x 90 simulated steps of a 50,000-neuron network of the same
   construction);
 * batched / served (single GPU, default configuration) = the metric's second half on
   reduced configurations: a 16-member BF16 ensemble batched vs the same members run
@@ -46,7 +46,7 @@ WINDOW = 500
 N_NEURONS, N_POPS, IN_DEGREE, SPEC_SEED = 5_000_000, 200, 1000, 1
 # the bounded CPU sample: the regional construction at 50,000 neurons (the 5M network needs
 # 200-280 GB of host memory as block_new's sparse tensors); one bench step = 75 simulated steps
-CPU_SAMPLE = dict(n=50_000, pops=20, in_degree=1000, seed=7, burn_in=400, per_step=75)
+CPU_SAMPLE = dict(n=50_000, pops=20, in_degree=1000, seed=7, burn_in=400, per_step=90)
 CPU_WORKLOAD = ("50,000-neuron regional LIF network, 20 populations, in-degree 1000, f32 weights, OU background "
                 "(the 5M-neuron network's construction at a size the host runs)")
 BYTES_STATE = 56          # V, J x4, i_ou, t_last read + written per neuron per step
@@ -444,9 +444,9 @@ def measure_ensemble(n_members, windows, W, warmup, batched_syn, seed=3):
     samples = [np.linspace(0, s.n - 1, 200).astype(np.uint32) for s in specs]
     g_ampa = E.PROP_IDS["CONDUCT_G_AMPA"]
 
-    def build(wt):
+    def build(wt, seed_base=100, members=None):
         t0 = time.perf_counter()
-        engs = [E.Engine.structured(s, weight_type=wt, seed=100 + i) for i, s in enumerate(specs)]
+        engs = [E.Engine.structured(s, weight_type=wt, seed=seed_base + i) for i, s in enumerate(specs[:members])]
         for e, smp in zip(engs, samples):
             e.set_samples(smp)
         torch.cuda.synchronize()
@@ -509,7 +509,25 @@ def measure_ensemble(n_members, windows, W, warmup, batched_syn, seed=3):
     rates_s, cv_s = summarise(acc)
     for e in engs:
         e.close()
+    # noise floor of the comparison: the first members again on the same FP32 path with other
+    # seeds (another realisation of the same network, untimed)
+    n_sp = min(8, len(specs))
+    engs, _ = build(E.W_F32, seed_base=5000, members=n_sp)
+    acc2 = [[np.zeros((0, s.n_pops), np.int32), np.zeros((0, 200), np.uint8)] for s in specs[:n_sp]]
+    for e in engs:
+        for _ in range(warmup):
+            e.run(W)
+    for w in range(windows):
+        for i, (e, s, f) in enumerate(zip(engs, specs, factors[w])):
+            e.update_prop_cols([g_ampa] * s.n_pops, np.arange(s.n_pops), f)
+            r = e.run(W, sample_spike=True)
+            acc2[i][0] = np.concatenate([acc2[i][0], r.freqs])
+            acc2[i][1] = np.concatenate([acc2[i][1], r.sample_spike])
+    for e in engs:
+        e.close()
+    rates_2, cv_2 = summarise(acc2)
     rate_rel = np.concatenate([np.abs(a - b) / np.maximum(b, 1e-9) for a, b in zip(rates_b, rates_s)])
+    rate_seed = np.concatenate([np.abs(a - b) / np.maximum(b, 1e-9) for a, b in zip(rates_2, rates_s)])
     member_steps = len(specs) * windows * W
     return {
         "workload": f"{len(specs)} ensemble members (N in [20k, 400k], in-degree in {{100, 200, 500}}, 10-50 "
@@ -533,6 +551,11 @@ def measure_ensemble(n_members, windows, W, warmup, batched_syn, seed=3):
             "population_rate_rel_diff_p95": float(np.percentile(rate_rel, 95)),
             "isi_cv_batched_mean": float(np.nanmean(cv_b)), "isi_cv_sequential_mean": float(np.nanmean(cv_s)),
             "isi_cv_rel_diff_median": float(np.nanmedian(np.abs(cv_b - cv_s) / cv_s)),
+            # the same statistics between two seeds of the sequential FP32 path (first members):
+            # what two realisations of one network differ by
+            "seed_spread_members": n_sp,
+            "population_rate_rel_diff_median_fp32_two_seeds": float(np.median(rate_seed)),
+            "isi_cv_rel_diff_median_fp32_two_seeds": float(np.nanmedian(np.abs(cv_2 - cv_s[:n_sp]) / cv_s[:n_sp])),
         },
         "clocks": clocks,
     }

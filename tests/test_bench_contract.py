@@ -18,5 +18,5 @@ def test_reference_arm_prints_its_line():
     assert line["higher_is_better"] is True
     # the line names the sample it times and counts the bench steps it timed
     assert line["steps"] == 1 and line["warmup"] == 3
-    assert "50,000-neuron" in line["config"]["workload"] and line["config"]["timed_sim_steps"] == 75
+    assert "50,000-neuron" in line["config"]["workload"] and line["config"]["timed_sim_steps"] == 90
     assert line["cpu_baseline"]["value"] == line["value"]
