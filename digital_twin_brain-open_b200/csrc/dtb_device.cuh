@@ -216,21 +216,14 @@ __device__ inline float u01(uint32_t r) {          // [0, 1)
     return static_cast<float>(r >> 8) * (1.0f / 16777216.0f);
 }
 
-#ifndef DTB_FAST_BM
-#define DTB_FAST_BM 0
-#endif
-// Box-Muller: two independent N(0,1) draws from two uniforms.
+// Box-Muller: two independent N(0,1) draws from two uniforms, on the SFU's
+// approximate log2 / rsqrt / sin / cos (the Philox draws are held to statistical
+// bars, never to bits; measured 2 % faster LIF than the IEEE-rounded functions).
 __device__ inline void box_muller(uint32_t a, uint32_t b, float& z0, float& z1) {
-#if DTB_FAST_BM
     const float x = -2.0f * __logf(u01_open(a));
     const float rad = x > 0.0f ? x * rsqrtf(x) : 0.0f;
     float s, c;
     __sincosf(6.28318530717958647692f * u01(b), &s, &c);
-#else
-    const float rad = sqrtf(-2.0f * logf(u01_open(a)));
-    float s, c;
-    sincospif(2.0f * u01(b), &s, &c);
-#endif
     z0 = rad * c;
     z1 = rad * s;
 }
