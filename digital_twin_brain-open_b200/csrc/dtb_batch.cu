@@ -23,7 +23,7 @@ namespace dtb {
 // Consecutive LIF tiles per CTA in a batch of several members (lif_kernel): a member
 // switch costs a chain of dependent loads that miss the L1, paid once per chunk.
 // Measured on the 64-member ensemble (batched device time of 6 windows): chunks of
-// 1 / 4 / 8 / 16 tiles -> ensemble 1.86x / 4.34 s / 4.60 s / 4.81 s.
+// 4 / 8 / 16 tiles -> 4.34 / 4.60 / 4.81 s; one tile per chunk ran ~7 % slower than four.
 constexpr uint32_t kBatchLifChunk = 4;
 
 Batch::~Batch() {
