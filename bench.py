@@ -406,7 +406,7 @@ def run_ours(args):
     if out is not None and world == 1 and not args.no_forms and args.net == "regional" and \
             args.neurons == N_NEURONS:
         # the metric's second half, batched/served vs plain at equal rate, on reduced configurations
-        out["batched"] = measure_ensemble(16, 4, 800, 1, args.batched_syn)
+        out["batched"] = measure_ensemble(16, 4, 800, 3, args.batched_syn)
         out["served"] = measure_serve(32, 60, 40.0, 800, 100, 150.0, args.batched_syn)
     return out
 
