@@ -81,13 +81,10 @@ int Batch::set_members(Engine* const* engines, uint32_t n) {
     if (n > cap_members) {
         if (d_views) cudaFree(d_views);
         if (d_prefix) cudaFree(d_prefix);
-        if (list_count) cudaFree(list_count);
         d_views = nullptr;
         d_prefix = nullptr;
-        list_count = nullptr;
         DTB_CU(cudaMalloc(reinterpret_cast<void**>(&d_views), sizeof(NetView) * n));
         DTB_CU(cudaMalloc(reinterpret_cast<void**>(&d_prefix), sizeof(uint32_t) * pre.size()));
-        DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_count), sizeof(uint32_t) * n));   // spiking rows per member
         cap_members = n;
     }
     if (total > cap_neurons) {
@@ -115,8 +112,11 @@ int Batch::set_members(Engine* const* engines, uint32_t n) {
     }
     // the prep kernel's block ticket sits after this membership's tables: start it at zero
     if (local_scratch) DTB_CU(cudaMemsetAsync(local_scratch, 0, sizeof(uint32_t) * (2ull * cap_windows + 3), stream));
-    if (!list_ticket) DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_ticket), sizeof(uint32_t)));
-    DTB_CU(cudaMemsetAsync(list_count, 0, sizeof(uint32_t) * n, stream));
+    if (!list_count) {
+        DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_count), sizeof(uint32_t)));
+        DTB_CU(cudaMalloc(reinterpret_cast<void**>(&list_ticket), sizeof(uint32_t)));
+    }
+    DTB_CU(cudaMemsetAsync(list_count, 0, sizeof(uint32_t), stream));
     DTB_CU(cudaMemsetAsync(list_ticket, 0, sizeof(uint32_t), stream));
     DTB_CU(cudaMemcpyAsync(d_prefix, pre.data(), sizeof(uint32_t) * pre.size(), cudaMemcpyHostToDevice, stream));
     lb.nets = d_views;

@@ -26,7 +26,7 @@ public:
     NetView* d_views = nullptr;
     uint32_t* d_prefix = nullptr;     // [lif n+1][pull n+1][vbase n+1][local windows n+1]
     uint32_t* list = nullptr;
-    uint32_t* list_count = nullptr;     // [cap_members] spiking rows per member
+    uint32_t* list_count = nullptr;
     uint32_t* list_ticket = nullptr;
     uint32_t cap_members = 0;         // capacity of d_views / d_prefix
     uint64_t cap_neurons = 0;         // capacity of the spike list

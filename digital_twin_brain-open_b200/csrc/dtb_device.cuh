@@ -163,14 +163,10 @@ struct NetView {
     float fix_scale, fix_unscale;  // 2^fix_shift, 2^-fix_shift
 };
 
-// Spike lists written by the LIF kernel and consumed by the push kernels: network
-// `net` of a launch keeps its spiking rows (network-local neuron ids) in
-// list[vbase[net] .. vbase[net] + counts[net]).  The push kernels walk the
-// networks' lists in network order, so the warps of a launch work on one or two
-// networks' accumulators at a time.
+// Batch-wide spike list written by the LIF kernel and consumed by the push kernel.
 struct SpikeList {
-    uint32_t* list;
-    uint32_t* counts;              // [n_nets]
+    uint32_t* list;                // virtual neuron ids: vbase[net] + neuron
+    uint32_t* count;
     uint32_t* ticket;              // last-CTA counter of the push kernel
     uint32_t capacity;
 };

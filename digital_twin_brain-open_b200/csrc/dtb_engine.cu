@@ -29,6 +29,7 @@ int cuda_fail(cudaError_t e, const char* what) {
 }
 
 __global__ void set_u64_kernel(unsigned long long* p, unsigned long long v) { *p = v; }
+__global__ void set_u32_kernel(uint32_t* p, uint32_t v) { *p = v; }
 
 static constexpr size_t kCsrPadWords = 16;   // 64 bytes after every CSR array
 static constexpr size_t kCsrPadBytes = 64;
@@ -1125,17 +1126,9 @@ static void pick_best(TuneResult& res) {
 // fastest.  `views` are the host copies of the launch's networks.
 int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int acc, int wtype, int sm_count,
                     cudaStream_t stream, cudaEvent_t ev[2], TuneResult& res) {
-    // the networks' spike counts: summed for the tuner, put back before every replay (the
-    // push's last CTA clears them)
-    std::vector<uint32_t> counts(views.size(), 0u);
-    DTB_CU(cudaMemcpyAsync(counts.data(), b.spikes.counts, sizeof(uint32_t) * counts.size(), cudaMemcpyDeviceToHost, stream));
+    uint32_t count = 0;
+    DTB_CU(cudaMemcpyAsync(&count, b.spikes.count, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     DTB_CU(cudaStreamSynchronize(stream));
-    uint64_t count_sum = 0;
-    for (uint32_t c : counts) count_sum += c;
-    const uint32_t count = static_cast<uint32_t>(std::min<uint64_t>(count_sum, 0xFFFFFFFFull));
-    auto restore_counts = [&]() {
-        return cudaMemcpyAsync(b.spikes.counts, counts.data(), sizeof(uint32_t) * counts.size(), cudaMemcpyHostToDevice, stream);
-    };
     uint64_t total_n = 0;
     for (const NetView& v : views) total_n += v.n_pad;
     res.sampled = false;
@@ -1179,7 +1172,7 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
             DTB_CU(push_prepare(acc, wtype, c, sm_count, &ctas));
             float ms_min = 1e30f;
             for (int rep = 0; rep < 3; ++rep) {
-                DTB_CU(restore_counts());
+                set_u32_kernel<<<1, 1, 0, stream>>>(b.spikes.count, count);
                 DTB_CU(cudaEventRecord(ev[0], stream));
                 DTB_CU(launch_push(tb, acc, wtype, c, ctas, stream));
                 DTB_CU(cudaEventRecord(ev[1], stream));
@@ -1190,7 +1183,7 @@ int tune_push_views(const LaunchBatch& b, const std::vector<NetView>& views, int
             }
             step.push_back({c, ms_min});
         }
-        DTB_CU(restore_counts());
+        set_u32_kernel<<<1, 1, 0, stream>>>(b.spikes.count, count);
         DTB_CU(cudaGetLastError());
         return DTB_OK;
     };

@@ -566,12 +566,13 @@ lif_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ tile_p
             }
             if ((flags & kFlagList) && wtotal) {
                 uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(sl.counts + net, wtotal);
-                base = __shfl_sync(0xffffffffu, base, 0) + __ldg(vbase + net);
+                if (lane == 0) base = atomicAdd(sl.count, wtotal);
+                base = __shfl_sync(0xffffffffu, base, 0);
                 const uint32_t below = (1u << lane) - 1u;
+                const uint32_t vb = __ldg(vbase + net) + i0;
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    if ((nib_prop >> k) & 1u) sl.list[base + __popc(wprop[k] & below)] = i0 + kSlotsPerTile * k;
+                    if ((nib_prop >> k) & 1u) sl.list[base + __popc(wprop[k] & below)] = vb + kSlotsPerTile * k;
                     base += __popc(wprop[k]);
                 }
             }
@@ -657,6 +658,7 @@ __device__ __forceinline__ void push_rows(const NetView* __restrict__ nets, cons
     // LPR lanes per row: 32 (a warp per row) or 16 / 8 (2 / 4 rows per warp, for short rows).
     // LOCAL: the own-population span of a row (own_seg) is left to push_local_kernel.
     constexpr uint32_t kGroups = 32 / LPR;
+    const uint32_t count = *sl.count;
     const uint32_t lane = (threadIdx.x & 31u) % LPR;
     const uint32_t gw = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * kGroups + (threadIdx.x & 31u) / LPR;
     const uint32_t nw = ((gridDim.x * blockDim.x) >> 5) * kGroups;
@@ -669,16 +671,12 @@ __device__ __forceinline__ void push_rows(const NetView* __restrict__ nets, cons
     float fscale = nets[0].fix_scale;
     const uint2* own = LOCAL ? nets[0].own_seg : nullptr;
     const unsigned long long keep = l2_policy_keep();
-    // global row r of the networks' lists laid end to end; this group takes r = gw (mod nw)
-    uint32_t k = 0, first = 0, cnt = sl.counts[0], lbase = 0;
-    for (uint32_t r = gw;; r += nw) {
-        if (r >= first + cnt) {
-            while (r >= first + cnt && ++k < n_nets) {
-                first += cnt;
-                cnt = sl.counts[k];
-            }
-            if (k >= n_nets) break;
-            lbase = __ldg(vbase + k);
+    uint32_t vb = 0;
+    for (uint32_t r = gw; r < count; r += nw) {
+        const uint32_t v = __ldg(sl.list + r);
+        if (n_nets > 1) {
+            const uint32_t k = find_net(vbase, n_nets, v);
+            vb = __ldg(vbase + k);
             ptr = nets[k].out_ptr;
             col = nets[k].out_col;
             wts = nets[k].out_w;
@@ -688,7 +686,7 @@ __device__ __forceinline__ void push_rows(const NetView* __restrict__ nets, cons
             fscale = nets[k].fix_scale;
             if constexpr (LOCAL) own = nets[k].own_seg;
         }
-        const uint32_t j = __ldg(sl.list + lbase + (r - first));
+        const uint32_t j = v - vb;
         const unsigned long long beg = __ldg(ptr + j), end = __ldg(ptr + j + 1);
         // virtual positions [0, len): [0, len1) -> beg + x, [len1, len) -> beg2 + (x - len1)
         unsigned long long len1 = end - beg, beg2 = end;
@@ -735,7 +733,7 @@ __device__ __forceinline__ void push_rows(const NetView* __restrict__ nets, cons
     if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(sl.ticket, 1u) == gridDim.x - 1) {
-            for (uint32_t q = 0; q < n_nets; ++q) sl.counts[q] = 0u;
+            *sl.count = 0u;
             *sl.ticket = 0u;
             __threadfence();
         }
@@ -1164,26 +1162,25 @@ push_tma_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ v
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncwarp();
+    const uint32_t count = *sl.count;
     const uint32_t nw = gridDim.x * kTmaWarps;
     const unsigned long long keep = l2_policy_keep();
-    // producer cursor (lane-uniform): global row of the networks' lists laid end to end,
-    // remaining range of the row, its network
+    // producer cursor (lane-uniform): list index, remaining range of the row, its network
     uint32_t pr = blockIdx.x * kTmaWarps + warp;
     unsigned long long pc = 0, pe = 0;
-    uint32_t pnet = 0, first = 0, cnt = sl.counts[0];
+    uint32_t pnet = 0;
     auto next_row = [&]() -> bool {
-        for (;; pr += nw) {
-            while (pr >= first + cnt) {
-                if (++pnet >= n_nets) return false;
-                first += cnt;
-                cnt = sl.counts[pnet];
-            }
-            const uint32_t j = __ldg(sl.list + __ldg(vbase + pnet) + (pr - first));
+        while (pr < count) {
+            const uint32_t v = __ldg(sl.list + pr);
+            pnet = n_nets > 1 ? find_net(vbase, n_nets, v) : 0u;
+            const uint32_t j = v - __ldg(vbase + pnet);
             const unsigned long long* ptr = nets[pnet].out_ptr;
             pc = __ldg(ptr + j);
             pe = __ldg(ptr + j + 1);
             if (pc < pe) return true;
+            pr += nw;
         }
+        return false;
     };
     bool have = next_row();
     uint32_t s_cnt[2] = {0, 0}, s_oc[2] = {0, 0}, s_ow[2] = {0, 0}, s_net[2] = {0, 0};
@@ -1258,7 +1255,7 @@ push_tma_kernel(const NetView* __restrict__ nets, const uint32_t* __restrict__ v
     if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(sl.ticket, 1u) == gridDim.x - 1) {
-            for (uint32_t q = 0; q < n_nets; ++q) sl.counts[q] = 0u;
+            *sl.count = 0u;
             *sl.ticket = 0u;
             __threadfence();
         }
