@@ -236,6 +236,8 @@ def run_ours(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.profile_steps and world > 1:
+        raise SystemExit("--profile-steps profiles one GPU; run it without torchrun")
     dist = None
     if world > 1:
         import datetime
