@@ -45,3 +45,24 @@ def test_consecutive_tiles_per_cta_bit_exact(gpu, block1m, syn):
         assert np.array_equal(eng.read_state(E.STATE_J), ref.J.T)
         assert np.array_equal(eng.read_state(E.STATE_I_OU), ref.i_bg)
     assert spiking_steps >= 10, "the network must burst"
+
+
+def test_window_push_at_scale_gives_the_same_bits(gpu):
+    """The population-window push at scale: a 1.2M-neuron regional network (24 populations of
+    ~50k neurons, in-degree 300, BF16) has ~4 windows per population, and a burst step hands each
+    window dozens of 1024-row work units.  With the fixed-point push the window form (local:2016,
+    its cross-population part on a second stream) and the register push must give the same bits:
+    per-step counts, events, V and J after 600 steps."""
+    spec = nw.structured_spec(1_200_000, 24, 300, seed=8)
+    results = []
+    for variant in [(E.PUSH_REG, 8), (E.PUSH_LOCAL, 2016)]:
+        with E.Engine.structured(spec, weight_type=E.W_BF16, seed=77, ou=OU) as eng:
+            eng.set_push_variant(*variant)
+            if variant[0] == E.PUSH_LOCAL:
+                assert eng.info().local_windows >= 48
+            r = eng.run(600, syn_mode=E.SYN_PUSH_FIXED)
+            results.append((r.freqs.copy(), r.events, eng.read_state(E.STATE_V), eng.read_state(E.STATE_J)))
+    (f0, e0, v0, j0), (f1, e1, v1, j1) = results
+    assert int((f0.sum(1) > spec.n // 100).sum()) >= 10, "the network must burst"
+    assert np.array_equal(f0, f1) and e0 == e1
+    assert np.array_equal(v0, v1) and np.array_equal(j0, j1)
