@@ -20,3 +20,13 @@ def test_reference_arm_prints_its_line():
     assert line["steps"] == 1 and line["warmup"] == 3
     assert "50,000-neuron" in line["config"]["workload"] and line["config"]["timed_sim_steps"] == 90
     assert line["cpu_baseline"]["value"] == line["value"]
+
+
+def test_profile_steps_refuses_multi_rank_launches():
+    """--profile-steps prints per-step events for an ncu capture of one GPU; under torchrun
+    (WORLD_SIZE > 1) it stops before touching a device."""
+    env = dict(os.environ, WORLD_SIZE="2", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--profile-steps", "3"],
+                       capture_output=True, text=True, timeout=600, cwd=ROOT, env=env)
+    assert r.returncode != 0
+    assert "--profile-steps profiles one GPU" in r.stderr
